@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: HPCG multigrid-preconditioned CG on B200.
+
+Default workload (one GPU): a 256^3 HPCG problem (16.8M rows, 449M nonzeros,
+4-level MG, generated b with exact solution 1, x0 = 0) solved to relative
+residual 1e-9 by the plain FP64 drop-in path.  One step = one full solve.
+`value` is HPCG GFLOP/s (src/ReportResults.cpp flop model x iterations /
+device time).  The same line carries:
+
+  e2e          the same solve through the C ABI from pinned HOST buffers
+               (b in, x out, copies inside the timed region)
+  roofline     the dominant kernel (level-0 full SymGS colour sweep) against
+               the measured HBM copy bandwidth
+  cpu_baseline the reference's own CPU path (CG_ref, OpenMP) on a bounded
+               sample, timed on this machine's host cores
+  mixed        FP64-outer / FP32 V-cycle solve at 320^3 with b ~ N(0,1)
+               (seed 0) vs the FP64 path on the same system, both verified
+               with an FP64 true residual
+
+`--impl reference` times the reference's CPU CG_ref on this machine instead.
+Under torchrun (N>1) every rank solves its own local problem (HPCG weak
+scaling with ExchangeHalo a single-rank no-op: replicas, no collective on the
+data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to rel. residual 1e-9 & HPCG GFLOP/s: mixed/learned vs FP64, 1 B200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--tol", type=float, default=1e-9)
+    ap.add_argument("--mixed-nx", type=int, default=320)
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def level_dims(n):
+    return [(n >> l, n >> l, n >> l) for l in range(4)]
+
+
+def stencil_nnz(d):
+    return (3 * d[0] - 2) * (3 * d[1] - 2) * (3 * d[2] - 2)
+
+
+def model(n):
+    from rochpcg_b200 import hpcg_model
+
+    dims = level_dims(n)
+    return hpcg_model(dims, [stencil_nnz(d) for d in dims])
+
+
+def generated_b_natural(nx, ny, nz):
+    """b_i = 26 - (nnz_i - 1) of the generated problem, natural order
+    (src/GenerateProblem.cpp:298-301)."""
+    def cnt(n):
+        c = np.full(n, 3, np.int8)
+        c[0] -= 1
+        c[-1] -= 1
+        return c
+    cz, cy, cx = cnt(nz), cnt(ny), cnt(nx)
+    nnz = (cz[:, None, None].astype(np.int32) * cy[None, :, None] * cx[None, None, :]).reshape(-1)
+    return 27.0 - nnz.astype(np.float64)
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- helpers
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(key: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary
+    (profiles/ncu_traffic.txt: lines `key bytes_per_launch`), else None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for ln in open(p):
+            parts = ln.split()
+            if len(parts) >= 2 and parts[0] == key:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline_sample(n: int, iters: int):
+    """The reference's CPU CG_ref (OpenMP, all host threads) on an n^3 sample."""
+    from oracle.oracle import RefProblem
+
+    R = RefProblem(n, n, n)
+    r = R.cg(iters, 0.0)
+    flops, _ = model(n)
+    gflops = flops * r["niters"] / r["seconds"] / 1e9
+    return gflops, r["seconds"], r["niters"]
+
+
+def host_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+# ------------------------------------------------------------ reference arm
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nx = int(os.environ.get("HPCG_BENCH_REF_SAMPLE", args.nx))
+    try:
+        from oracle.oracle import RefProblem, ref_lib
+
+        ref_lib()
+    except Exception as e:  # the reference library could not be built/loaded
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path not loadable: {e}"}))
+        return 0
+    t0 = time.perf_counter()
+    R = RefProblem(nx, nx, nx)
+    setup_s = time.perf_counter() - t0
+    flops_it, _ = model(nx)
+    # one step = one CG_ref iteration (preamble + 1 iteration) of the workload
+    for _ in range(args.warmup):
+        R.cg(1, 0.0)
+    times = []
+    for _ in range(args.steps):
+        r = R.cg(1, 0.0)
+        times.append(r["seconds"])
+    t = sum(times) / len(times)
+    gflops = flops_it / t / 1e9
+    cores = host_threads()
+    sample = f"CG_ref (src/CG_ref.cpp) on the {nx}^3 problem: 1 iteration + preamble per step, OMP threads={cores}"
+    line = {
+        "metric": METRIC, "value": gflops, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (HPCG generator)", "impl": "reference",
+        "config": {"workload": f"HPCG {nx}^3 FP64 MG-PCG (4 levels), generated b, x0=0", "grid": [nx, nx, nx],
+                   "mg_levels": 4, "parallelism": "replicas"},
+        "cpu_baseline": {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": gflops, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": setup_s,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args):
+    import torch
+    import rochpcg_b200 as R
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    nx = args.nx
+    P = R.Problem(nx)
+    flops_it, bytes_it = P.model()
+    m = P.rows[0]
+    stream = torch.cuda.ExternalStream(P.stream_handle)
+
+    # ---- device-timed solves (inputs resident in HBM)
+    for _ in range(args.warmup):
+        P.cg(1000, args.tol)
+    barrier()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    runs = []
+    for _ in range(args.steps):
+        runs.append(P.cg(1000, args.tol))
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    iters = runs[-1]["niters"]
+    ms_step = ms_total / args.steps
+    value = world * flops_it * iters / (ms_step * 1e-3) / 1e9
+    rel = runs[-1]["normr"] / runs[-1]["normr0"]
+    true_rel = P.true_residual()
+    kpi = P.kernels_per_iteration(R.MODE_FP64)
+    launches = args.steps * (iters * kpi + 2)
+
+    # ---- end to end through the C ABI from pinned host memory
+    b_host = torch.from_numpy(generated_b_natural(nx, nx, nx)).pin_memory()
+    x_host = torch.empty(m, dtype=torch.float64).pin_memory()
+    P.solve_host(b_host, x_host, 1000, args.tol)  # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        re = P.solve_host(b_host, x_host, 1000, args.tol)
+    barrier()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    e2e_val = world * flops_it * re["niters"] / e2e_s / 1e9
+    x_err = float(torch.max(torch.abs(x_host - 1.0)))
+
+    # ---- dominant kernel: level-0 full SymGS colour sweep
+    nb = P.nblocks[0]
+    sweep_ms = P.time_op("symgs_sweep", 20)
+    rows_c = m // nb
+    alg_bytes = rows_c * (27 * 12 + 3 * 8) + (m - rows_c) * 8
+    achieved = alg_bytes / (sweep_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic(f"symgs_sweep_{nx}")
+    roofline = {"kernel": "k_symgs_sweep (level-0 colour sweep, FP64 ELL)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": sweep_ms}
+    spmv_ms = P.time_op("spmv", 20)
+    spmv_bytes = m * (27 * 12 + 8 + 8)
+    extra_kernels = {"spmv_GBps": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "spmv_ms": spmv_ms,
+                     "mg_ms": P.time_op("mg", 5)}
+    P.close()
+    del P
+
+    # ---- mixed precision vs FP64 at 320^3, b ~ N(0,1) seed 0
+    mixed = None
+    if not args.no_mixed:
+        from rochpcg_b200.rhs import normal_rhs
+
+        n3 = args.mixed_nx
+        Q = R.Problem(n3)
+        Q.set_rhs(normal_rhs(Q.rows[0], 0))
+        f3, _ = Q.model()
+        res = {}
+        for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED)):
+            Q.cg(1000, args.tol, mode=mode)
+            barrier()
+            ts = []
+            for _ in range(2):
+                r3 = Q.cg(1000, args.tol, mode=mode)
+                ts.append(r3["seconds"])
+            res[name] = {"time_to_1e-9_s": min(ts), "iterations": r3["niters"],
+                         "rel_residual_recurrence": r3["normr"] / r3["normr0"],
+                         "rel_residual_fp64_true": Q.true_residual(),
+                         "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9}
+        res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
+        res["grid"] = [n3, n3, n3]
+        res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
+        mixed = res
+        Q.close()
+
+    # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            n_cpu, it_cpu = 128, 10
+            g, secs, its = cpu_baseline_sample(n_cpu, it_cpu)
+            cpu = {"value": g, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
+                   "sample": f"CG_ref (reference src/*_ref.cpp, OpenMP) on {n_cpu}^3, {its} iterations from x0=0, "
+                             f"{secs:.2f} s"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (HPCG problem generator, b for x*=1)",
+            "config": {"workload": f"HPCG {nx}^3 FP64 MG-PCG solve to rel. residual {args.tol:g}",
+                       "grid": [nx, nx, nx], "mg_levels": 4, "rhs": "generated (exact solution ones), x0=0",
+                       "l2": "inputs larger than L2 (level-0 ELL is %.1f GB)" % (27 * 12 * m / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "time_to_solution_s": ms_step * 1e-3, "iterations": iters, "rel_residual": rel,
+            "rel_residual_fp64_true": true_rel, "hpcg_model_bytes_per_iter": bytes_it,
+            "model_GBps": world * bytes_it * iters / (ms_step * 1e-3) / 1e9,
+            "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m,
+                    "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err},
+            "roofline": roofline, "kernels": extra_kernels, "cpu_baseline": cpu, "mixed": mixed,
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,252 @@
+/*
+ * hpcg_b200.h -- C ABI of libhpcgb200.so, the B200 (sm_100a) implementation of
+ * HPCG's multigrid-preconditioned conjugate-gradient hot path.
+ *
+ * Two layers are exported:
+ *
+ *  1. Kernel entry points (hpcgb200_spmv, hpcgb200_symgs, ...): plain device
+ *     pointers, sizes and a cudaStream_t passed as void*.  They replace the
+ *     device side of the reference operators named in each comment (paths are
+ *     relative to the rocHPCG source tree).  None of them allocates; scratch
+ *     space for reductions is passed in by the caller.
+ *  2. Problem entry points (hpcgb200_problem_*): an opaque handle that owns a
+ *     generated + optimized 4-level hierarchy and runs the reference's
+ *     protocol pieces (CG, TestCG, TestSymmetry) on it.  The C++ operator API
+ *     with the reference's signatures (CG, ComputeSPMV, ComputeMG, ...) is in
+ *     rochpcg_b200/host/hpcg.hpp and is what C++ callers link against.
+ *
+ * Index conventions: local_int_t is int32 (src/Geometry.hpp:29); ELL storage
+ * is column-major with slot p of row i at p*m + i (64-bit offset), width 27;
+ * pad slots hold column -1.  After optimization every vector is in the
+ * color-permuted order perm[] defines (new = perm[old]).
+ *
+ * Every function returns 0 on success or one of the HPCGB200_ERR_* codes; it
+ * never exits the process.  hpcgb200_last_error() describes the last failure.
+ */
+#ifndef HPCG_B200_H
+#define HPCG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPCGB200_OK 0
+#define HPCGB200_ERR_ARG 1            /* invalid argument / size */
+#define HPCGB200_ERR_CUDA 2           /* CUDA runtime error */
+#define HPCGB200_ERR_COLORING 3       /* multicoloring did not terminate */
+#define HPCGB200_ERR_WORKSPACE 4      /* workspace too small */
+#define HPCGB200_ERR_NOT_STENCIL 5    /* matrix is not the 27-point HPCG stencil (implicit paths) */
+#define HPCGB200_ERR_DEVICE_STATUS 6  /* a device-side check failed (status word set) */
+#define HPCGB200_ERR_NO_DEVICE 7      /* no CUDA device visible */
+
+#define HPCGB200_WIDTH 27
+#define HPCGB200_MAX_COLORS 128       /* src/utils.hpp:48 */
+
+/* ----------------------------------------------------------------- misc */
+
+/* Text of the last error recorded by this thread. */
+const char* hpcgb200_last_error(void);
+/* Library version string. */
+const char* hpcgb200_version(void);
+/* Bytes of caller-provided scratch the reduction entry points need. */
+size_t hpcgb200_reduction_workspace_bytes(void);
+/* The first n values rand() returns after srand(seed) with glibc's
+ * generator (n <= 4096); the colouring draws its colour pairs from this
+ * sequence with seed 0x586744 (src/MultiColoring.cpp:259,283-284). */
+int hpcgb200_rand_sequence(unsigned int seed, int n, int* out);
+
+/* ------------------------------------------------ problem construction
+ * src/GenerateProblem.cpp:98-303 (kernel_generate_problem) + src/SetupHalo.cpp:
+ * 107-131 (kernel_copy_indices, 1 rank).  Row-major 27 slots per row in
+ * (dz,dy,dx) order, boundary rows compacted.  mtx_ind gets LOCAL column ids
+ * (1 rank: global == local), pads -1; values pads 0.  l2g, hash, b may be NULL. */
+int hpcgb200_generate_problem(int nx, int ny, int nz, long long gnx, long long gny, long long gnz,
+                              long long gix0, long long giy0, long long giz0, int* mtx_ind, double* values,
+                              int8_t* nnz_in_row, int* diag_slot, long long* l2g, int* hash, double* b,
+                              void* stream);
+
+/* src/GenerateCoarseProblem.cpp:57-86 (kernel_f2c_operator); c2f (length nxf*nyf*nzf,
+ * -1 where no coarse point) may be NULL. */
+int hpcgb200_f2c_operator(int nxf, int nyf, int nzf, int* f2c, int* c2f, void* stream);
+
+/* src/MultiColoring.cpp:238-353 (JPLColoring): Jones-Plassmann-Luby rounds
+ * with (c1,c2) = rand()%8 after srand(0x586744) (glibc sequence, generated
+ * internally so the process's rand() state is untouched), then a stable
+ * counting sort by color (replacing rocPRIM radix_sort_pairs on
+ * [0, 32-clz(nblocks)) bits) and perm[sorted[i]] = i.
+ * Outputs: colors[m], perm[m] (device); *nblocks, round_sizes[nblocks] (the
+ * reference's per-round counts), sizes[] / offsets[] (host, by color value,
+ * HPCGB200_MAX_COLORS / +1 entries).  workspace: >= hpcgb200_coloring_workspace_bytes(m). */
+size_t hpcgb200_coloring_workspace_bytes(int m);
+int hpcgb200_jpl_coloring(int m, const int* hash, const int* mtx_ind, int* colors, int* perm, int* nblocks,
+                          int* round_sizes, int* sizes, int* offsets, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
+/* src/Permute.cpp:95-185 (PermuteColumns) + src/SparseMatrix.cpp:271-359
+ * (ConvertToELL) + src/Permute.cpp:187-218 (PermuteRows) in one pass:
+ * ell_col[p*m + perm[i]] = p-th smallest perm[col] of natural row i. */
+int hpcgb200_build_ell(int m, const int* mtx_ind, const double* values, const int* perm, int* ell_col,
+                       double* ell_val, void* stream);
+
+/* src/SparseMatrix.cpp:361-407 (ExtractDiagonal); diag (may be NULL) also gets a_ii. */
+int hpcgb200_extract_diagonal(int m, const int* ell_col, const double* ell_val, int* diag_idx, double* inv_diag,
+                              double* diag, void* stream);
+
+/* src/Permute.cpp:220-246 (PermuteVector): out[perm[i]] = in[i]. */
+int hpcgb200_permute_vector(int m, const int* perm, const double* in, double* out, void* stream);
+
+/* Inverse of the above: out[i] = in[perm[i]] (natural order from permuted). */
+int hpcgb200_unpermute_vector(int m, const int* perm, const double* in, double* out, void* stream);
+
+/* src/SparseMatrix.cpp:66-101 (HIPCopyMatrixDiagonal): diagonal[i] = a_ii. */
+int hpcgb200_copy_diagonal(int m, const int* ell_col, const double* ell_val, double* diagonal, void* stream);
+
+/* src/SparseMatrix.cpp:103-150 (HIPReplaceMatrixDiagonal): a_ii = diagonal[i],
+ * inv_diag = 1/a_ii; diag (may be NULL) mirrors a_ii. */
+int hpcgb200_replace_diagonal(int m, const double* diagonal, const int* ell_col, double* ell_val,
+                              double* inv_diag, double* diag, void* stream);
+
+/* Multigrid transfer indices: inj_f[ic] = perm_f[f2c[ic]], inj_c[ic] = perm_c[ic]
+ * (the two gathers src/ComputeRestriction.cpp:100-102 and
+ * src/ComputeProlongation.cpp:53-56 do per call, done once). */
+int hpcgb200_transfer_indices(int nc, const int* f2c, const int* perm_f, const int* perm_c, int* inj_f,
+                              int* inj_c, void* stream);
+
+/* ------------------------------------------------------- FP64 operators */
+
+/* src/ComputeSPMV.cpp:130-170,226-278 (kernel_spmv_ell): y = A x. */
+int hpcgb200_spmv(int m, const int* ell_col, const double* ell_val, const double* x, double* y, void* stream);
+
+/* src/ComputeSYMGS.cpp:113-151,369-404: one symmetric multicolor Gauss-Seidel
+ * step (colors 0..nblocks-1, then ublocks..0).  sizes/offsets are HOST arrays. */
+int hpcgb200_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
+                   const double* ell_val, const double* inv_diag, const double* r, double* x, void* stream);
+
+/* src/ComputeSYMGS.cpp:238-341,406-454 (ComputeSYMGSZeroGuess): the same step
+ * from x = 0 without reading x; diag/inv_diag are a_ii and 1/a_ii. */
+int hpcgb200_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets,
+                        const int* ell_col, const double* ell_val, const int* diag_idx, const double* diag,
+                        const double* inv_diag, const double* r, double* x, void* stream);
+
+/* src/ComputeRestriction.cpp:81-124,199-237 (ComputeFusedSpMVRestriction):
+ * rc[inj_c[i]] = rf[inj_f[i]] - (A xf)[inj_f[i]]. */
+int hpcgb200_restrict_fused(int nc, const int* inj_f, const int* inj_c, int mf, const int* ell_col,
+                            const double* ell_val, const double* rf, const double* xf, double* rc, void* stream);
+
+/* src/ComputeProlongation.cpp:39-86: xf[inj_f[i]] += xc[inj_c[i]]. */
+int hpcgb200_prolong(int nc, const int* inj_f, const int* inj_c, const double* xc, double* xf, void* stream);
+
+/* src/ComputeDotProduct.cpp:63-238: *result (DEVICE pointer) = sum x[i]*y[i].
+ * Deterministic fixed-shape two-level reduction in one launch; workspace >=
+ * hpcgb200_reduction_workspace_bytes(), its counter must start at zero (it is
+ * left at zero on return, so a zero-filled workspace can be reused). */
+int hpcgb200_dot(int n, const double* x, const double* y, double* result, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
+/* src/ComputeWAXPBY.cpp:63-135 (kernel_waxpby): w = alpha x + beta y with the
+ * reference's alpha==1 / beta==1 fma forms. */
+int hpcgb200_waxpby(int n, double alpha, const double* x, double beta, const double* y, double* w, void* stream);
+
+/* src/ComputeWAXPBY.cpp:137-240 (ComputeFusedWAXPBYDot): y += alpha x and
+ * *result (device) = ||y||^2; workspace as for hpcgb200_dot. */
+int hpcgb200_waxpby_dot(int n, double alpha, const double* x, double* y, double* result, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* src/ComputeResidual.cpp:77-152: *result (device) = max_i |v1[i] - v2[i]|. */
+int hpcgb200_residual_inf(int n, const double* v1, const double* v2, double* result, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------ problem handle
+ * A handle owns the device hierarchy built exactly as src/main.cpp:198-210 +
+ * src/OptimizeProblem.cpp:69-160 do (GenerateProblem, SetupHalo,
+ * 3x GenerateCoarseProblem, OptimizeProblem), on its own CUDA stream. */
+typedef struct hpcgb200_problem hpcgb200_problem;
+
+#define HPCGB200_MODE_FP64 0    /* plain FP64 drop-in (the reference's optimized path) */
+#define HPCGB200_MODE_MIXED 1   /* FP64 outer CG, FP32 V-cycle on the implicit stencil */
+
+int hpcgb200_problem_create(int nx, int ny, int nz, int nlevels, hpcgb200_problem** out);
+/* flags: HPCGB200_FLAG_KEEP_GENERATED keeps the row-major generated arrays
+ * (mtx_ind, values, hash ...) that OptimizeProblem otherwise frees. */
+#define HPCGB200_FLAG_KEEP_GENERATED 1
+int hpcgb200_problem_create_ex(int nx, int ny, int nz, int nlevels, int flags, hpcgb200_problem** out);
+int hpcgb200_problem_destroy(hpcgb200_problem* p);
+/* dims[3*level..], rows[level], nnz[level], nblocks[level] for every level (host arrays of nlevels). */
+int hpcgb200_problem_info(const hpcgb200_problem* p, int* nlevels, int* dims, int* rows, long long* nnz,
+                          int* nblocks);
+/* Seconds spent in generation (src/main.cpp:190-215) and in OptimizeProblem. */
+int hpcgb200_problem_setup_times(const hpcgb200_problem* p, double* setup_s, double* optimize_s);
+int hpcgb200_problem_stream(const hpcgb200_problem* p, void** stream);
+/* *ok = 1 when the level was verified to be the 27-point stencil in parity
+ * colouring (required by HPCGB200_MODE_MIXED). */
+int hpcgb200_problem_stencil_ok(const hpcgb200_problem* p, int level, int* ok);
+
+/* Field access for tests and tools: copy a device array of a level to host
+ * memory.  field: "perm","colors","ell_col","ell_val","diag_idx","inv_diag",
+ * "f2c","inj_f","inj_c","b","xexact","x","sizes","offsets","mtx_ind",
+ * "values","nnz_in_row","hash","round_sizes". */
+int hpcgb200_problem_copy_field(const hpcgb200_problem* p, int level, const char* field, void* host,
+                                size_t bytes);
+/* Size in bytes of a field (same names). */
+int hpcgb200_problem_field_bytes(const hpcgb200_problem* p, int level, const char* field, size_t* bytes);
+/* Device pointer of a field (same names) for zero-copy use. */
+int hpcgb200_problem_device_field(const hpcgb200_problem* p, int level, const char* field, void** dev);
+
+/* Right-hand side: b from HOST memory in natural order (it is permuted on
+ * upload); NULL restores the generated b (exact solution all ones). */
+int hpcgb200_problem_set_rhs(hpcgb200_problem* p, const double* host_b_natural);
+/* Current solution to HOST memory in natural order. */
+int hpcgb200_problem_get_x(hpcgb200_problem* p, double* host_x_natural);
+
+/* src/CG.cpp:104-200: CG from x = 0 on the problem's b.  mode: HPCGB200_MODE_*.
+ * normr_hist (host, may be NULL) gets max_iter+1 entries (normr after the
+ * preamble and after each iteration).  seconds: device-timed solve. */
+int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, double tol, int precond, int* niters,
+                        double* normr, double* normr0, double* normr_hist, double* seconds);
+
+/* Same, end to end from HOST memory: copies b_natural in, solves, copies x
+ * out (natural order); seconds covers the copies too. */
+int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const double* b_natural, double* x_natural,
+                                int max_iter, double tol, int* niters, double* normr, double* normr0,
+                                double* seconds);
+
+/* True residual of the current x, in FP64: *rel = ||b - A x|| / ||b||
+ * (independent of the CG recurrence's updated r). */
+int hpcgb200_problem_true_residual(hpcgb200_problem* p, double* rel);
+
+/* Number of kernel launches one CG iteration of the given mode issues (the
+ * kernel nodes of the captured iteration graph; available after a solve). */
+int hpcgb200_problem_kernels_per_iteration(hpcgb200_problem* p, int mode, int precond, int* kernels);
+
+/* src/TestCG.cpp:111-177.  out[0..3] = niters of unpreconditioned call 0,1
+ * and preconditioned call 0,1; *count_pass / *count_fail as the reference. */
+int hpcgb200_problem_test_cg(hpcgb200_problem* p, int mode, int* out_niters, int* count_pass, int* count_fail);
+
+/* src/TestSymmetry.cpp:88-166 with the reference's random vectors
+ * (rand()/RAND_MAX + 1 from the process rand() state): depsym_spmv,
+ * depsym_mg (mode selects the V-cycle precision), ||A xexact - b||_inf. */
+int hpcgb200_problem_test_symmetry(hpcgb200_problem* p, int mode, double* depsym_spmv, double* depsym_mg,
+                                   double* residual_inf);
+
+/* Per-operator calls on the handle's level data (vectors are DEVICE
+ * pointers in permuted order), used by the operator parity tests. */
+int hpcgb200_problem_spmv(hpcgb200_problem* p, int level, const double* x, double* y);
+int hpcgb200_problem_symgs(hpcgb200_problem* p, int level, const double* r, double* x);
+int hpcgb200_problem_symgs_zero(hpcgb200_problem* p, int level, const double* r, double* x);
+int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* r, double* x);
+int hpcgb200_problem_restrict(hpcgb200_problem* p, int level, const double* rf, const double* xf, double* rc);
+int hpcgb200_problem_prolong(hpcgb200_problem* p, int level, const double* xc, double* xf);
+
+/* Time n back-to-back launches of one level-0 operator with CUDA events on
+ * the problem's stream; *ms_per_launch = average.  op: "spmv","symgs_sweep"
+ * (one full-row color sweep, averaged over the 15 of a SymGS step),
+ * "symgs","symgs_zero","mg","mg_mixed". */
+int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPCG_B200_H */

@@ -1,0 +1,358 @@
+"""Python access to the two CPU oracles.  TEST INFRASTRUCTURE ONLY.
+
+* :class:`RefProblem` drives ``oracle/_ref/libhpcg_ref.so`` -- the reference's
+  own CPU path (``CG_ref``, ``ComputeMG_ref``, ``ComputeSYMGS_ref`` ...)
+  compiled unmodified from rocHPCG 0.8.9 ``src/*_ref.cpp`` by
+  ``oracle/Makefile``.
+* :class:`ColoredProblem` drives ``oracle/liboracle.so`` -- our C restatement
+  of the reference's *optimized* path (JPL multicoloring, permutation,
+  column-major ELL, colored SymGS; see ``oracle/colored.h`` for the per-kernel
+  citations).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libhpcg_ref.so")
+COLORED_SO = os.path.join(HERE, "liboracle.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle libraries (the reference one only where its source tree exists)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# --------------------------------------------------------------------------
+# reference CPU path
+
+
+_ref_lib = None
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(f"{REF_SO} missing: run `make -C oracle ref` where the reference tree exists")
+        L = ctypes.CDLL(REF_SO)
+        L.hpcgref_create.restype = ctypes.c_void_p
+        L.hpcgref_create.argtypes = [ctypes.c_int] * 4
+        L.hpcgref_destroy.argtypes = [ctypes.c_void_p]
+        L.hpcgref_num_levels.argtypes = [ctypes.c_void_p]
+        L.hpcgref_level_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _c_int_p,
+                                         ctypes.POINTER(ctypes.c_longlong)]
+        L.hpcgref_get_matrix.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 3
+        L.hpcgref_get_f2c.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.hpcgref_get_rhs.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.hpcgref_check_problem.argtypes = [ctypes.c_void_p]
+        L.hpcgref_cg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                 ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
+        for name in ("hpcgref_spmv", "hpcgref_symgs", "hpcgref_mg"):
+            getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.hpcgref_restriction.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 3
+        L.hpcgref_prolongation.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 2
+        L.hpcgref_dot.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _c_dbl_p]
+        L.hpcgref_waxpby.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_double,
+                                     ctypes.c_void_p, ctypes.c_void_p]
+        L.hpcgref_residual.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _c_dbl_p]
+        L.hpcgref_test_norms.argtypes = [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_int_p]
+        _ref_lib = L
+    return _ref_lib
+
+
+class RefProblem:
+    """The reference CPU problem (natural ordering): GenerateProblem_ref +
+    SetupHalo_ref + 3 coarse levels, solved by CG_ref."""
+
+    def __init__(self, nx: int, ny: int, nz: int, nlevels: int = 4):
+        self.L = ref_lib()
+        self.h = self.L.hpcgref_create(nx, ny, nz, nlevels)
+        if not self.h:
+            raise ValueError("hpcgref_create failed")
+        self.nlevels = self.L.hpcgref_num_levels(self.h)
+        self.dims, self.nrows, self.nnz = [], [], []
+        for l in range(self.nlevels):
+            d = np.zeros(3, np.int32)
+            m = ctypes.c_int()
+            nnz = ctypes.c_longlong()
+            self.L.hpcgref_level_info(self.h, l, _ptr(d), ctypes.byref(m), ctypes.byref(nnz))
+            self.dims.append(tuple(int(v) for v in d))
+            self.nrows.append(m.value)
+            self.nnz.append(nnz.value)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.hpcgref_destroy(self.h)
+            self.h = None
+
+    def matrix(self, level: int = 0):
+        m = self.nrows[level]
+        cols = np.empty((m, 27), np.int32)
+        vals = np.empty((m, 27), np.float64)
+        nnz = np.empty(m, np.int8)
+        self.L.hpcgref_get_matrix(self.h, level, _ptr(cols), _ptr(vals), _ptr(nnz))
+        return cols, vals, nnz
+
+    def f2c(self, level: int):
+        out = np.empty(self.nrows[level + 1], np.int32)
+        assert self.L.hpcgref_get_f2c(self.h, level, _ptr(out)) == 0
+        return out
+
+    def rhs(self):
+        b = np.empty(self.nrows[0])
+        xe = np.empty(self.nrows[0])
+        self.L.hpcgref_get_rhs(self.h, _ptr(b), _ptr(xe))
+        return b, xe
+
+    def check_problem(self):
+        self.L.hpcgref_check_problem(self.h)
+
+    def cg(self, max_iter: int, tol: float, b: np.ndarray | None = None, precond: bool = True):
+        x = np.empty(self.nrows[0])
+        it = ctypes.c_int()
+        nr, nr0, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        bb = None if b is None else np.ascontiguousarray(b, np.float64)
+        self.L.hpcgref_cg(self.h, max_iter, tol, None if bb is None else _ptr(bb), _ptr(x), int(precond),
+                          ctypes.byref(it), ctypes.byref(nr), ctypes.byref(nr0), ctypes.byref(t))
+        return dict(x=x, niters=it.value, normr=nr.value, normr0=nr0.value, seconds=t.value)
+
+    def spmv(self, level: int, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.nrows[level])
+        self.L.hpcgref_spmv(self.h, level, _ptr(x), _ptr(y))
+        return y
+
+    def symgs(self, level: int, r: np.ndarray, x: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.array(x, np.float64, copy=True)
+        self.L.hpcgref_symgs(self.h, level, _ptr(r), _ptr(x))
+        return x
+
+    def mg(self, r: np.ndarray, level: int = 0) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.zeros(self.nrows[level])
+        self.L.hpcgref_mg(self.h, level, _ptr(r), _ptr(x))
+        return x
+
+    def restriction(self, level: int, rf: np.ndarray, xf: np.ndarray) -> np.ndarray:
+        rf = np.ascontiguousarray(rf, np.float64)
+        xf = np.ascontiguousarray(xf, np.float64)
+        rc = np.empty(self.nrows[level + 1])
+        assert self.L.hpcgref_restriction(self.h, level, _ptr(rf), _ptr(xf), _ptr(rc)) == 0
+        return rc
+
+    def prolongation(self, level: int, xc: np.ndarray, xf: np.ndarray) -> np.ndarray:
+        xc = np.ascontiguousarray(xc, np.float64)
+        xf = np.array(xf, np.float64, copy=True)
+        assert self.L.hpcgref_prolongation(self.h, level, _ptr(xc), _ptr(xf)) == 0
+        return xf
+
+
+def ref_test_norms(values) -> dict:
+    v = np.ascontiguousarray(values, np.float64)
+    mean, var, ok = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    ref_lib().hpcgref_test_norms(_ptr(v), len(v), ctypes.byref(mean), ctypes.byref(var), ctypes.byref(ok))
+    return dict(mean=mean.value, variance=var.value, pass_=bool(ok.value))
+
+
+# --------------------------------------------------------------------------
+# colored (optimized-path) restatement
+
+
+class _OcLevel(ctypes.Structure):
+    _fields_ = [
+        ("m", ctypes.c_int), ("nblocks", ctypes.c_int), ("ublocks", ctypes.c_int),
+        ("sizes", ctypes.c_void_p), ("offsets", ctypes.c_void_p), ("ell_col", ctypes.c_void_p),
+        ("ell_val", ctypes.c_void_p), ("diag_idx", ctypes.c_void_p), ("inv_diag", ctypes.c_void_p),
+        ("nc", ctypes.c_int), ("f2c", ctypes.c_void_p), ("perm", ctypes.c_void_p), ("perm_c", ctypes.c_void_p),
+        ("rc", ctypes.c_void_p), ("xc", ctypes.c_void_p),
+    ]
+
+
+_oc_lib = None
+
+
+def colored_lib():
+    global _oc_lib
+    if _oc_lib is None:
+        if not os.path.exists(COLORED_SO):
+            build(ref=False)
+        L = ctypes.CDLL(COLORED_SO)
+        vp = ctypes.c_void_p
+        L.oc_generate.argtypes = [ctypes.c_int] * 3 + [vp] * 6
+        L.oc_f2c.argtypes = [ctypes.c_int] * 3 + [vp]
+        L.oc_jpl_coloring.argtypes = [ctypes.c_int] + [vp] * 6
+        L.oc_jpl_coloring.restype = ctypes.c_int
+        L.oc_color_perm.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, vp, vp]
+        L.oc_build_ell.argtypes = [ctypes.c_int] + [vp] * 7
+        L.oc_permute_vector.argtypes = [ctypes.c_int, vp, vp, vp]
+        L.oc_spmv.argtypes = [ctypes.c_int, vp, vp, vp, vp]
+        L.oc_symgs.argtypes = [ctypes.c_int] * 3 + [vp] * 7
+        L.oc_symgs_zero.argtypes = [ctypes.c_int] * 3 + [vp] * 7
+        L.oc_restrict_fused.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.oc_prolong.argtypes = [ctypes.c_int] + [vp] * 5
+        L.oc_dot.argtypes = [ctypes.c_int, vp, vp]
+        L.oc_dot.restype = ctypes.c_double
+        L.oc_mg.argtypes = [vp, ctypes.c_int, vp, vp]
+        L.oc_mg_f32.argtypes = [vp, ctypes.c_int, vp, vp]
+        L.oc_cg.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                            _c_int_p, _c_dbl_p, _c_dbl_p, vp]
+        _oc_lib = L
+    return _oc_lib
+
+
+class ColoredLevel:
+    """One level of the optimized data: natural-order generated matrix, JPL
+    colors, permutation, column-major ELL and diagonal data."""
+
+    def __init__(self, nx: int, ny: int, nz: int, with_rhs: bool = False):
+        L = colored_lib()
+        self.dims = (nx, ny, nz)
+        m = self.m = nx * ny * nz
+        self.cols = np.empty((m, 27), np.int32)
+        self.vals = np.empty((m, 27), np.float64)
+        self.nnz_in_row = np.empty(m, np.int8)
+        self.diag_slot = np.empty(m, np.int32)
+        self.hash = np.empty(m, np.int32)
+        self.b_nat = np.empty(m) if with_rhs else None
+        L.oc_generate(nx, ny, nz, _ptr(self.cols), _ptr(self.vals), _ptr(self.nnz_in_row), _ptr(self.diag_slot),
+                      _ptr(self.hash), None if self.b_nat is None else _ptr(self.b_nat))
+        self.colors = np.empty(m, np.int32)
+        self.round_colors = np.zeros(256, np.int32)
+        self.round_sizes = np.zeros(256, np.int32)
+        nb = L.oc_jpl_coloring(m, _ptr(self.cols), _ptr(self.nnz_in_row), _ptr(self.hash), _ptr(self.colors),
+                               _ptr(self.round_colors), _ptr(self.round_sizes))
+        if nb < 0:
+            raise RuntimeError("JPL coloring did not terminate")
+        self.nblocks = nb
+        self.ublocks = nb - 2  # MultiColoring.cpp:316,350-352 (non-reference build)
+        self.round_colors = self.round_colors[:nb].copy()
+        self.round_sizes = self.round_sizes[:nb].copy()
+        self.perm = np.empty(m, np.int32)
+        self.sizes = np.zeros(max(nb, int(self.colors.max()) + 1), np.int32)
+        self.offsets = np.zeros(len(self.sizes) + 1, np.int32)
+        L.oc_color_perm(m, _ptr(self.colors), len(self.sizes), _ptr(self.perm), _ptr(self.sizes), _ptr(self.offsets))
+        self.ell_col = np.empty((27, m), np.int32)
+        self.ell_val = np.empty((27, m), np.float64)
+        self.diag_idx = np.empty(m, np.int32)
+        self.inv_diag = np.empty(m, np.float64)
+        L.oc_build_ell(m, _ptr(self.cols), _ptr(self.vals), _ptr(self.perm), _ptr(self.ell_col), _ptr(self.ell_val),
+                       _ptr(self.diag_idx), _ptr(self.inv_diag))
+        self.f2c = None
+        self.nc = 0
+
+    def permute(self, v: np.ndarray) -> np.ndarray:
+        out = np.empty_like(v)
+        out[self.perm] = v
+        return out
+
+    def unpermute(self, v: np.ndarray) -> np.ndarray:
+        return v[self.perm]
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.m)
+        colored_lib().oc_spmv(self.m, _ptr(self.ell_col), _ptr(self.ell_val), _ptr(x), _ptr(y))
+        return y
+
+    def symgs(self, r, x):
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.array(x, np.float64, copy=True)
+        colored_lib().oc_symgs(self.m, self.nblocks, self.ublocks, _ptr(self.sizes), _ptr(self.offsets),
+                               _ptr(self.ell_col), _ptr(self.ell_val), _ptr(self.inv_diag), _ptr(r), _ptr(x))
+        return x
+
+    def symgs_zero(self, r):
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.zeros(self.m)
+        colored_lib().oc_symgs_zero(self.m, self.nblocks, self.ublocks, _ptr(self.sizes), _ptr(self.offsets),
+                                    _ptr(self.ell_col), _ptr(self.ell_val), _ptr(self.diag_idx), _ptr(r), _ptr(x))
+        return x
+
+
+class ColoredProblem:
+    """4-level optimized hierarchy (all vectors in color-permuted order)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, nlevels: int = 4):
+        self.levels = [ColoredLevel(nx, ny, nz, with_rhs=True)]
+        for l in range(1, nlevels):
+            f = self.levels[-1]
+            fx, fy, fz = f.dims
+            f.f2c = np.empty((fx // 2) * (fy // 2) * (fz // 2), np.int32)
+            colored_lib().oc_f2c(fx, fy, fz, _ptr(f.f2c))
+            f.nc = len(f.f2c)
+            self.levels.append(ColoredLevel(fx // 2, fy // 2, fz // 2))
+        self.nlevels = nlevels
+        L0 = self.levels[0]
+        self.b = L0.permute(L0.b_nat)
+        self.xexact = np.ones(L0.m)
+        self._bufs = []
+        self._struct = (_OcLevel * nlevels)()
+        for l, lev in enumerate(self.levels):
+            s = self._struct[l]
+            s.m, s.nblocks, s.ublocks = lev.m, lev.nblocks, lev.ublocks
+            s.sizes, s.offsets = _ptr(lev.sizes).value, _ptr(lev.offsets).value
+            s.ell_col, s.ell_val = _ptr(lev.ell_col).value, _ptr(lev.ell_val).value
+            s.diag_idx, s.inv_diag = _ptr(lev.diag_idx).value, _ptr(lev.inv_diag).value
+            s.perm = _ptr(lev.perm).value
+            if l + 1 < nlevels:
+                rc, xc = np.zeros(lev.nc), np.zeros(lev.nc)
+                self._bufs += [rc, xc]
+                s.nc, s.f2c = lev.nc, _ptr(lev.f2c).value
+                s.perm_c = _ptr(self.levels[l + 1].perm).value
+                s.rc, s.xc = _ptr(rc).value, _ptr(xc).value
+
+    def restrict_fused(self, level: int, rf, xf):
+        A, C = self.levels[level], self.levels[level + 1]
+        rf = np.ascontiguousarray(rf, np.float64)
+        xf = np.ascontiguousarray(xf, np.float64)
+        rc = np.empty(C.m)
+        colored_lib().oc_restrict_fused(A.nc, _ptr(A.f2c), _ptr(A.perm), _ptr(C.perm), A.m, _ptr(A.ell_col),
+                                        _ptr(A.ell_val), _ptr(rf), _ptr(xf), _ptr(rc))
+        return rc
+
+    def prolong(self, level: int, xc, xf):
+        A, C = self.levels[level], self.levels[level + 1]
+        xc = np.ascontiguousarray(xc, np.float64)
+        xf = np.array(xf, np.float64, copy=True)
+        colored_lib().oc_prolong(A.nc, _ptr(A.f2c), _ptr(A.perm), _ptr(C.perm), _ptr(xc), _ptr(xf))
+        return xf
+
+    def mg(self, r):
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.zeros(self.levels[0].m)
+        colored_lib().oc_mg(ctypes.cast(self._struct, ctypes.c_void_p), self.nlevels, _ptr(r), _ptr(x))
+        return x
+
+    def mg_f32(self, r):
+        r = np.ascontiguousarray(r, np.float32)
+        x = np.zeros(self.levels[0].m, np.float32)
+        colored_lib().oc_mg_f32(ctypes.cast(self._struct, ctypes.c_void_p), self.nlevels, _ptr(r), _ptr(x))
+        return x
+
+    def cg(self, max_iter: int, tol: float, b=None, precond: bool = True):
+        b = self.b if b is None else np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.levels[0].m)
+        hist = np.zeros(max_iter + 1)
+        it = ctypes.c_int()
+        nr, nr0 = ctypes.c_double(), ctypes.c_double()
+        colored_lib().oc_cg(ctypes.cast(self._struct, ctypes.c_void_p), self.nlevels, _ptr(b), _ptr(x), max_iter, tol,
+                            int(precond), ctypes.byref(it), ctypes.byref(nr), ctypes.byref(nr0), _ptr(hist))
+        return dict(x=x, niters=it.value, normr=nr.value, normr0=nr0.value, hist=hist[: it.value + 1])

@@ -1,0 +1,236 @@
+// Device-resident CG recurrence of src/CG.cpp:104-200.  The reference
+// pays 12 device synchronisations and 3 blocking scalar read-backs per
+// iteration; here every scalar (rtz, pAp, alpha, beta, normr) is produced by
+// the last block of the reduction that needs it, and the loop condition is
+// written to a CUDA-graph conditional handle, so a whole solve runs as one
+// graph launch.  Vector arithmetic keeps the reference's fma forms.
+#include "cg.cuh"
+
+namespace hb {
+
+__global__ void __launch_bounds__(kReduceThreads) k_cg_residual0(int n, const double* __restrict__ b,
+                                                                 const double* __restrict__ Ap,
+                                                                 double* __restrict__ r, CGState* st,
+                                                                 ReduceScratch* ws)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    {
+        const double v = fma(-1.0, Ap[i], b[i]);  // WAXPBY(1, b, -1, Ap): alpha == 1 form
+        r[i] = v;
+        s = fma(v, v, s);
+    }
+    s = block_sum(s, red);
+    double total;
+    if(grid_reduce(s, ws, kReduceBlocks, &total))
+    {
+        const double nr = sqrt(total);
+        st->normr = nr;
+        st->normr0 = nr;
+        st->hist[0] = nr;
+        st->k = 1;
+        st->niters = 0;
+        st->rtz = 0.0;
+        st->oldrtz = 0.0;
+        st->rtz_flex = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_cg_rtz(int n, const double* __restrict__ r,
+                                                           const double* __restrict__ z, CGState* st,
+                                                           ReduceScratch* ws)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+        s = fma(z[i], r[i], s);
+    s = block_sum(s, red);
+    double total;
+    if(grid_reduce(s, ws, kReduceBlocks, &total))
+    {
+        if(st->k == 1)
+        {
+            st->rtz = total;
+            st->beta = 0.0;
+        }
+        else
+        {
+            st->oldrtz = st->rtz;
+            st->rtz = total;
+            // Fletcher-Reeves (the reference) or Polak-Ribiere for flexible CG:
+            // beta = r_k.(z_k - z_{k-1}) / r_{k-1}.z_{k-1}
+            const double num = st->flexible ? total - st->rtz_flex : total;
+            st->beta = num / st->oldrtz;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const double* __restrict__ z, double* __restrict__ p,
+                                                     const CGState* __restrict__ st)
+{
+    const int i = blockIdx.x * kBS + threadIdx.x;
+    if(i >= n) return;
+    if(st->k == 1) p[i] = fma(0.0, z[i], z[i]);     // WAXPBY(1, z, 0, z)
+    else p[i] = fma(st->beta, p[i], z[i]);          // WAXPBY(1, z, beta, p)
+}
+
+// Ap = A p (interleaved colour map as k_spmv) and pAp; alpha = rtz / pAp.
+__global__ void __launch_bounds__(kReduceThreads) k_cg_spmv_pap(int m, ColorChunks cc,
+                                                                const int* __restrict__ ell_col,
+                                                                const double* __restrict__ ell_val,
+                                                                const double* __restrict__ p,
+                                                                double* __restrict__ Ap, CGState* st,
+                                                                ReduceScratch* ws)
+{
+    static_assert(kReduceThreads == kBS, "chunk map assumes kBS threads");
+    __shared__ double red[32];
+    double s = 0.0;
+    const int nch = cc.nchunks();
+    for(int ch = blockIdx.x; ch < nch; ch += gridDim.x)
+    {
+        int row;
+        if(!cc.row_of(ch, threadIdx.x, row)) continue;
+        double sum = 0.0;
+#pragma unroll
+        for(int q = 0; q < kWidth; ++q)
+        {
+            const size_t idx = (size_t)q * m + row;
+            const int col = ld_stream(ell_col + idx);
+            const double v = ld_stream(ell_val + idx);
+            if(col >= 0 && col < m) sum = fma(v, __ldg(p + col), sum);
+        }
+        Ap[row] = sum;
+        s = fma(sum, p[row], s);
+    }
+    s = block_sum(s, red);
+    double total;
+    if(grid_reduce(s, ws, gridDim.x, &total))
+    {
+        st->pAp = total;
+        st->alpha = st->rtz / total;
+    }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const double* __restrict__ p,
+                                                                 const double* __restrict__ Ap,
+                                                                 double* __restrict__ r, double* __restrict__ x,
+                                                                 const double* __restrict__ z, CGState* st,
+                                                                 ReduceScratch* ws)
+{
+    __shared__ double red[32];
+    const double alpha = st->alpha;
+    const bool flex = st->flexible != 0;
+    double s = 0.0, sf = 0.0;
+    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    {
+        const double v = fma(-alpha, Ap[i], r[i]);   // ComputeFusedWAXPBYDot(-alpha, Ap, r)
+        r[i] = v;
+        s = fma(v, v, s);
+        x[i] = fma(alpha, p[i], x[i]);               // WAXPBY(1, x, alpha, p)
+        if(flex) sf = fma(z[i], v, sf);
+    }
+    double t1, t2;
+    bool last;
+    if(flex)
+    {
+        s = block_sum(s, red);
+        sf = block_sum(sf, red);
+        last = grid_reduce2(s, sf, ws, kReduceBlocks, &t1, &t2);
+    }
+    else
+    {
+        s = block_sum(s, red);
+        last = grid_reduce(s, ws, kReduceBlocks, &t1);
+        t2 = 0.0;
+    }
+    if(last)
+    {
+        const double nr = sqrt(t1);
+        st->normr = nr;
+        st->rtz_flex = t2;
+        st->hist[st->k] = nr;
+    }
+}
+
+// Loop control of the device-resident CG, one thread: always advances k, so
+// the WHILE node ends after at most max_iter iterations whatever the
+// reductions produced.  src/CG.cpp:148: continue while k <= max_iter &&
+// normr/normr0 > tol (a NaN residual compares false and ends the loop).
+__global__ void k_cg_loop_control(CGState* st, unsigned long long cond)
+{
+    const int k = st->k;
+    st->niters = k;
+    st->k = k + 1;
+    const unsigned go = (k + 1 <= st->max_iter) && (st->normr / st->normr0 > st->tol);
+    if(cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, go);
+}
+
+__global__ void k_cast_d2f(int n, const double* __restrict__ in, float* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) out[i] = (float)in[i];
+}
+
+__global__ void k_cast_f2d(int n, const float* __restrict__ in, double* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) out[i] = (double)in[i];
+}
+
+int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGState* st, ReduceScratch* ws,
+                        cudaStream_t s)
+{
+    k_cg_residual0<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, Ap, r, st, ws);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s)
+{
+    k_cg_rtz<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, st, ws);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s)
+{
+    k_cg_update_p<<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
+                       double* Ap, CGState* st, ReduceScratch* ws, cudaStream_t s)
+{
+    const int grid = cc.nchunks() < kReduceBlocks ? cc.nchunks() : kReduceBlocks;
+    k_cg_spmv_pap<<<grid, kReduceThreads, 0, s>>>(m, cc, ell_col, ell_val, p, Ap, st, ws);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, cudaStream_t s)
+{
+    k_cg_update_xr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
+    HB_LAUNCHED();
+    k_cg_loop_control<<<1, 1, 0, s>>>(st, cond);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cast_d2f(int n, const double* in, float* out, cudaStream_t s)
+{
+    k_cast_d2f<<<(n + 255) / 256, 256, 0, s>>>(n, in, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cast_f2d(int n, const float* in, double* out, cudaStream_t s)
+{
+    k_cast_f2d<<<(n + 255) / 256, 256, 0, s>>>(n, in, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+}  // namespace hb

@@ -1,0 +1,49 @@
+// Device-resident CG recurrence (src/CG.cpp:104-200) for libhpcgb200.
+#pragma once
+
+#include "common.cuh"
+#include "ops64.cuh"
+
+namespace hb {
+
+// Scalars of one CG solve, kept in device memory so that an iteration needs
+// no host round trip: alpha/beta are formed by the last block of the
+// reduction that produces their denominator.
+struct CGState
+{
+    double rtz, oldrtz, alpha, beta, pAp;
+    double normr, normr0, tol;
+    double rtz_flex;      // r_new . z_old (flexible-CG beta numerator term)
+    int k;                // iteration about to run (1-based)
+    int max_iter;
+    int niters;
+    int flexible;         // 1: Polak-Ribiere beta (flexible CG); 0: Fletcher-Reeves as the reference
+    int status;           // nonzero: a device-side check failed
+    int pad[3];
+    double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
+};
+
+inline size_t cg_state_bytes(int max_iter) { return sizeof(CGState) + sizeof(double) * (size_t)(max_iter + 1); }
+
+// Preamble: r = b - Ap (WAXPBY(1,b,-1,Ap)), normr = ||r||, normr0 = normr,
+// k = 1; returns whether iterations are needed through state.
+int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGState* st, ReduceScratch* ws,
+                        cudaStream_t s);
+// rtz = r.z, beta = rtz/oldrtz (k>1), oldrtz kept.
+int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
+// p = z (k == 1) or p = z + beta p.
+int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s);
+// Ap = A p and alpha = rtz / (p.Ap).
+int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
+                       double* Ap, CGState* st, ReduceScratch* ws, cudaStream_t s);
+// r -= alpha Ap, normr = ||r||, x += alpha p, history; then (own 1-thread
+// kernel) k++ and the loop condition (k <= max_iter && normr/normr0 > tol)
+// written to `cond` (a graph conditional handle; 0 = none).
+int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, cudaStream_t s);
+
+// Mixed precision glue: r32 = (float) r and z = (double) z32.
+int launch_cast_d2f(int n, const double* in, float* out, cudaStream_t s);
+int launch_cast_f2d(int n, const float* in, double* out, cudaStream_t s);
+
+}  // namespace hb

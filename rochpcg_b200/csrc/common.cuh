@@ -1,0 +1,180 @@
+// Shared definitions for the sm_100a kernels of libhpcgb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hpcg_b200.h"
+
+namespace hb {
+
+constexpr int kWidth = HPCGB200_WIDTH;  // ELL width of the 27-point stencil
+
+// Fixed reduction shape: results do not depend on the device or on timing,
+// so every dot product is bit-reproducible run to run.
+constexpr int kReduceBlocks = 1184;  // 8 x 148 SMs
+constexpr int kReduceThreads = 256;
+
+// Reduction scratch: partial sums then one ticket counter.
+struct ReduceScratch
+{
+    double partial[kReduceBlocks];
+    double partial2[kReduceBlocks];  // second sum of two-value reductions
+    unsigned int ticket;
+    unsigned int pad[3];
+};
+
+int record_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace hb
+
+#define HB_CUDA(call)                                                           \
+    do                                                                          \
+    {                                                                           \
+        cudaError_t hb_e_ = (call);                                             \
+        if(hb_e_ != cudaSuccess) return hb::cuda_error(hb_e_, #call, __FILE__, __LINE__); \
+    } while(0)
+
+#define HB_LAUNCHED() HB_CUDA(cudaGetLastError())
+
+#define HB_CHECK_ARG(cond, msg)                                                 \
+    do                                                                          \
+    {                                                                           \
+        if(!(cond)) return hb::record_error(HPCGB200_ERR_ARG, "%s: %s", __func__, msg); \
+    } while(0)
+
+#define HB_RETURN_IF(err)       \
+    do                          \
+    {                           \
+        int hb_r_ = (err);      \
+        if(hb_r_ != 0) return hb_r_; \
+    } while(0)
+
+// ---------------------------------------------------------------- device helpers
+
+namespace hb {
+
+// Streaming (read-once) loads for matrix data: evict-first in L2 so that the
+// vectors gathered by the stencil stay resident.
+__device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum (blockDim.x multiple of 32, <= 1024); result valid in thread 0.
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* smem /* >= 32 */)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if(lane == 0) smem[warp] = v;
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    T r = (threadIdx.x < nw) ? smem[threadIdx.x] : T(0);
+    if(warp == 0) r = warp_sum(r);
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_max(T v, T* smem)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_max(v);
+    if(lane == 0) smem[warp] = v;
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    T r = (threadIdx.x < nw) ? smem[threadIdx.x] : T(0);
+    if(warp == 0) r = warp_max(r);
+    __syncthreads();
+    return r;
+}
+
+// Two-level deterministic reduction epilogue.  Every block of a kernel with
+// gridDim.x == nblocks calls this with its block's partial (valid in thread
+// 0).  Returns true in thread 0 of the LAST block to arrive, which then holds
+// the total in *total (summed over partials in index order).  The ticket is
+// reset for the next launch.
+template <bool kMax = false>
+__device__ __forceinline__ bool grid_reduce(double block_partial, ReduceScratch* ws, int nblocks, double* total)
+{
+    __shared__ bool last;
+    __shared__ double red[32];
+    if(threadIdx.x == 0)
+    {
+        ws->partial[blockIdx.x] = block_partial;
+        __threadfence();
+        const unsigned int t = atomicAdd(&ws->ticket, 1u);
+        last = (t == (unsigned)nblocks - 1);
+    }
+    __syncthreads();
+    if(!last) return false;
+    __threadfence();
+    double acc = kMax ? 0.0 : 0.0;
+    for(int i = threadIdx.x; i < nblocks; i += blockDim.x)
+    {
+        const double v = __ldcg(&ws->partial[i]);
+        acc = kMax ? fmax(acc, v) : acc + v;
+    }
+    acc = kMax ? block_max(acc, red) : block_sum(acc, red);
+    if(threadIdx.x == 0)
+    {
+        ws->ticket = 0;
+        *total = acc;
+    }
+    return threadIdx.x == 0;
+}
+
+// Two sums at once (same protocol as grid_reduce).
+__device__ __forceinline__ bool grid_reduce2(double a, double b, ReduceScratch* ws, int nblocks, double* ta,
+                                             double* tb)
+{
+    __shared__ bool last;
+    __shared__ double red[32];
+    if(threadIdx.x == 0)
+    {
+        ws->partial[blockIdx.x] = a;
+        ws->partial2[blockIdx.x] = b;
+        __threadfence();
+        const unsigned int t = atomicAdd(&ws->ticket, 1u);
+        last = (t == (unsigned)nblocks - 1);
+    }
+    __syncthreads();
+    if(!last) return false;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for(int i = threadIdx.x; i < nblocks; i += blockDim.x)
+    {
+        sa += __ldcg(&ws->partial[i]);
+        sb += __ldcg(&ws->partial2[i]);
+    }
+    sa = block_sum(sa, red);
+    sb = block_sum(sb, red);
+    if(threadIdx.x == 0)
+    {
+        ws->ticket = 0;
+        *ta = sa;
+        *tb = sb;
+    }
+    return threadIdx.x == 0;
+}
+
+}  // namespace hb

@@ -1,0 +1,63 @@
+// FP32 V-cycle on the implicit 27-point stencil (mixed-precision path).
+//
+// After the reference's JPL multicoloring of the HPCG grid every colour is
+// one parity class (ix&1, iy&1, iz&1) and, because the colour sort is
+// stable, the rows of a colour are that class in natural (z,y,x) order: a
+// dense brick.  A row's neighbours are therefore computable from its
+// position, and their ELL slot order (ascending permuted column) is fixed per
+// colour: by neighbour colour, then by (dz,dy,dx).  The kernels walk that
+// order, so their float sums round exactly like an ELL sweep with float
+// values -- without reading any matrix data.  Off-diagonal values are the
+// stencil's -1 (verified on the device before this path is enabled); the
+// diagonal stays an explicit array because TestCG rescales it.
+#pragma once
+
+#include "common.cuh"
+
+namespace hb {
+
+constexpr int kMaxStencilColors = 8;
+
+struct StencilLevel
+{
+    int nx, ny, nz, m;
+    int ncolors;
+    int offsets[kMaxStencilColors + 1];
+    int bx[kMaxStencilColors], by[kMaxStencilColors];
+    int par[kMaxStencilColors];           // parity bits (ix&1)<<2 | (iy&1)<<1 | (iz&1) of colour v
+    int color_of_par[8];
+    // Per colour: the 27 stencil offsets in ELL slot order, packed as
+    // (dx+1) | (dy+1)<<2 | (dz+1)<<4 | (neighbour colour)<<8.
+    unsigned short nb[kMaxStencilColors][27];
+    unsigned char diag_pos[kMaxStencilColors];
+};
+
+// Builds the level description from the grid and the colour of each parity
+// class; returns false when some parity class is empty or the colours are not
+// a permutation of 0..7.
+bool make_stencil_level(int nx, int ny, int nz, const int* offsets, const int color_of_par[8], StencilLevel* out);
+
+// Counts (into *bad, device) rows where perm/ELL differ from the implicit
+// stencil: permuted position, column order, off-diagonal value -1.
+int launch_stencil_check(const StencilLevel& L, const int* perm, const int* ell_col, const double* ell_val, int* bad,
+                         cudaStream_t s);
+
+// diag32 = (float) a_ii, inv_diag32 = 1.0f / diag32.
+int launch_diag32(int m, const double* diag, float* diag32, float* inv_diag32, cudaStream_t s);
+
+// Zero-guess symmetric GS (forward colours 0..n-1, backward n-2..0).  When
+// r64 is non-null the forward sweeps read the FP64 residual and also store
+// its float value into r32 (fusing the down-conversion).
+int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float* inv_diag32, const double* r64,
+                        float* r32, float* x, cudaStream_t s);
+// Full symmetric GS step.  When z64 is non-null every row's final value is
+// also stored as double there (fusing the up-conversion).
+int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* r, float* x, double* z64,
+                   cudaStream_t s);
+// rc[inj_c[i]] = rf[inj_f[i]] - (A xf)[inj_f[i]].
+int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* diag32,
+                      const float* rf, const float* xf, float* rc, cudaStream_t s);
+// xf[inj_f[i]] += xc[inj_c[i]].
+int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf, cudaStream_t s);
+
+}  // namespace hb

@@ -1,0 +1,254 @@
+// CG (src/CG.cpp:104-200) as a device-resident loop.
+//
+// The preamble (p = x, Ap = A p, r = b - Ap, normr0) runs as plain launches
+// followed by one read-back.  The iterations are one CUDA graph: a
+// conditional WHILE node whose body is MG (or z = r), rtz, p update, SpMV+pAp,
+// r/x update; the last kernel of the body evaluates the reference's loop
+// condition (k <= max_iter && normr/normr0 > tol) on the device and feeds it
+// to the WHILE node.  A solve therefore costs one graph launch and two
+// read-backs instead of the reference's 12 device syncs + 3 blocking copies
+// per iteration.  Where conditional nodes are unavailable the same body runs
+// as a per-iteration graph with a host-side check.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "hpcg_b200.h"
+#include "internal.hpp"
+
+using namespace hpcg_b200;
+
+namespace hpcg_b200 {
+
+static void ensure_state(LevelOpt* o, int max_iter)
+{
+    if(o->cg_state && o->cg_state_iters >= max_iter) return;
+    const int cap = max_iter < 1024 ? 1024 : max_iter;
+    dfree(o->cg_state);
+    o->cg_state = reinterpret_cast<hb::CGState*>(dalloc<char>(hb::cg_state_bytes(cap)));
+    o->cg_state_iters = cap;
+    // graphs captured the old state pointer
+    for(auto& g : o->graphs)
+    {
+        if(g->exec) cudaGraphExecDestroy(g->exec);
+        if(g->graph) cudaGraphDestroy(g->graph);
+    }
+    o->graphs.clear();
+}
+
+static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool precond, MGPrecision prec,
+                        hb::CGState* st, unsigned long long cond, cudaStream_t s)
+{
+    const int n = A.localNumberOfRows;
+    if(precond)
+    {
+        HB_RETURN_IF(prec == MGPrecision::FP64 ? ComputeMG(A, data.r, data.z) : ComputeMG_Mixed(A, data.r, data.z));
+    }
+    else
+    {
+        const cudaError_t e =
+            cudaMemcpyAsync(data.z.d_values, data.r.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        if(e != cudaSuccess) return hb::cuda_error(e, "copy r to z", __FILE__, __LINE__);
+    }
+    HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
+    HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
+    HB_RETURN_IF(hb::launch_cg_spmv_pap(n, opt(A)->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, st,
+                                        rt().ws, s));
+    HB_RETURN_IF(hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
+                                         data.z.d_values, st, rt().ws, cond, s));
+    return 0;
+}
+
+static int count_kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if(cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if(cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    int k = 0;
+    for(auto nd : nodes)
+    {
+        cudaGraphNodeType t;
+        if(cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
+
+static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, bool precond,
+                          MGPrecision prec, bool flexible)
+{
+    LevelOpt* o = opt(A);
+    const double* key[6] = {data.r.d_values, data.z.d_values, data.p.d_values, data.Ap.d_values, b.d_values,
+                            x.d_values};
+    for(auto& g : o->graphs)
+        if(!std::memcmp(g->key, key, sizeof(key)) && g->mode == (int)prec && g->precond == precond &&
+           g->flexible == flexible)
+            return g.get();
+
+    auto G = std::make_unique<CGGraph>();
+    std::memcpy(G->key, key, sizeof(key));
+    G->mode = (int)prec;
+    G->precond = precond;
+    G->flexible = flexible;
+    cudaStream_t s = rt().stream;
+
+    // Preferred: WHILE conditional node around the iteration body.
+    bool built = false;
+    {
+        cudaGraph_t g = nullptr;
+        cudaGraphConditionalHandle h = 0;
+        cudaGraphNode_t node;
+        cudaGraphNodeParams cp{};
+        if(cudaGraphCreate(&g, 0) == cudaSuccess &&
+           cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess)
+        {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            if(cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess)
+            {
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                if(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                   cudaSuccess)
+                {
+                    const int rc = capture_body(A, data, x, precond, prec, o->cg_state, (unsigned long long)h, s);
+                    cudaGraph_t out = nullptr;
+                    const cudaError_t e = cudaStreamEndCapture(s, &out);
+                    if(rc == 0 && e == cudaSuccess && cudaGraphInstantiate(&G->exec, g, 0) == cudaSuccess)
+                    {
+                        G->kernels_per_iteration = count_kernel_nodes(body);
+                        G->graph = g;
+                        G->conditional = true;
+                        built = true;
+                    }
+                }
+            }
+        }
+        if(!built)
+        {
+            cudaGetLastError();
+            if(g) cudaGraphDestroy(g);
+        }
+    }
+    if(!built)
+    {
+        // Fallback: one iteration per launch, host checks the condition.
+        cudaGraph_t g = nullptr;
+        HB_HOST_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int rc = capture_body(A, data, x, precond, prec, o->cg_state, 0ULL, s);
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if(rc) throw_last(rc);
+        HB_HOST_CUDA(e);
+        HB_HOST_CUDA(cudaGraphInstantiate(&G->exec, g, 0));
+        G->kernels_per_iteration = count_kernel_nodes(g);
+        G->graph = g;
+        G->conditional = false;
+    }
+    o->graphs.push_back(std::move(G));
+    return o->graphs.back().get();
+}
+
+int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,
+           double& normr, double& normr0, bool precond, MGPrecision prec, bool flexible, double* hist,
+           double* seconds)
+{
+    try
+    {
+        ensure_runtime();
+        if(max_iter < 0 || max_iter > 1000000) return hb::record_error(HPCGB200_ERR_ARG, "CG: max_iter out of range");
+        LevelOpt* o = opt(A);
+        if(!o) return hb::record_error(HPCGB200_ERR_ARG, "CG: OptimizeProblem has not run");
+        cudaStream_t s = rt().stream;
+        const int n = A.localNumberOfRows;
+        ensure_state(o, max_iter);
+        hb::CGState* st = o->cg_state;
+
+        hb::CGState h{};
+        h.tol = tol;
+        h.max_iter = max_iter;
+        h.flexible = flexible ? 1 : 0;
+        cudaEvent_t e0, e1;
+        HB_HOST_CUDA(cudaEventCreate(&e0));
+        HB_HOST_CUDA(cudaEventCreate(&e1));
+        HB_HOST_CUDA(cudaEventRecord(e0, s));
+        HB_HOST_CUDA(cudaMemcpyAsync(st, &h, offsetof(hb::CGState, hist), cudaMemcpyHostToDevice, s));
+        // a fresh reduction ticket for every solve
+        HB_HOST_CUDA(cudaMemsetAsync(&rt().ws->ticket, 0, sizeof(unsigned int), s));
+
+        // preamble: p = x; Ap = A p; r = b - Ap; normr = ||r||
+        HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        check(hb::launch_spmv(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, s));
+        check(hb::launch_cg_residual0(n, b.d_values, data.Ap.d_values, data.r.d_values, st, rt().ws, s));
+        HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+        HB_HOST_CUDA(cudaStreamSynchronize(s));
+
+        const bool iterate = max_iter >= 1 && (h.normr / h.normr0 > tol);
+        if(iterate)
+        {
+            CGGraph* G = get_graph(A, data, b, x, precond, prec, flexible);
+            if(G->conditional)
+            {
+                HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
+            }
+            else
+            {
+                for(int k = 1; k <= max_iter; ++k)
+                {
+                    HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
+                    HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+                    HB_HOST_CUDA(cudaStreamSynchronize(s));
+                    if(!(h.normr / h.normr0 > tol)) break;
+                }
+            }
+        }
+        HB_HOST_CUDA(cudaEventRecord(e1, s));
+        HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+        HB_HOST_CUDA(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        HB_HOST_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if(hist)
+        {
+            HB_HOST_CUDA(cudaMemcpy(hist, st->hist, sizeof(double) * (h.niters + 1), cudaMemcpyDeviceToHost));
+            for(int k = h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
+        }
+        niters = h.niters;
+        normr = h.normr;
+        normr0 = h.normr0;
+        if(seconds) *seconds = ms * 1e-3;
+        return 0;
+    }
+    catch(const Error& e)
+    {
+        return report(e);
+    }
+}
+
+}  // namespace hpcg_b200
+
+int CG_B200(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tolerance,
+            int& niters, double& normr, double& normr0, double* times, bool doPreconditioning, MGPrecision prec,
+            bool flexible, double* normr_hist)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = run_cg(A, data, b, x, max_iter, tolerance, niters, normr, normr0, doPreconditioning, prec, flexible,
+                          normr_hist, nullptr);
+    if(times) times[0] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+int CG(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const int max_iter, const double tolerance,
+       int& niters, double& normr, double& normr0, double* times, bool doPreconditioning, bool verbose)
+{
+    std::vector<double> hist(verbose ? max_iter + 1 : 0);
+    const int rc = CG_B200(A, data, b, x, max_iter, tolerance, niters, normr, normr0, times, doPreconditioning,
+                           MGPrecision::FP64, false, verbose ? hist.data() : nullptr);
+    if(rc == 0 && verbose)
+    {
+        printf("B200 Initial Residual = %le\n", normr0);
+        for(int k = 1; k <= niters; ++k) printf("B200 Iteration = %d   Scaled Residual = %le\n", k, hist[k] / normr0);
+    }
+    return rc;
+}

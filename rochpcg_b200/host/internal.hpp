@@ -1,0 +1,114 @@
+// Implementation state of the host layer (not part of the public API).
+#pragma once
+
+#include <cstdio>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../csrc/cg.cuh"
+#include "../csrc/mixed.cuh"
+#include "../csrc/ops64.cuh"
+#include "hpcg.hpp"
+
+namespace hpcg_b200 {
+
+// Errors from CUDA or from the C ABI inside the void-returning reference
+// signatures surface as this exception; the C ABI converts it back to a code.
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_last(int code);
+// Records the exception text as the C ABI's last error and returns its code.
+inline int report(const Error& e) { return hb::record_error(e.code, "%s", e.what()); }
+void check_cuda(cudaError_t e, const char* what);
+inline void check(int rc)
+{
+    if(rc != 0) throw_last(rc);
+}
+#define HB_HOST_CUDA(call) ::hpcg_b200::check_cuda((call), #call)
+
+struct Runtime
+{
+    bool initialized = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    hb::ReduceScratch* ws = nullptr;   // reduction scratch (ticket left at zero)
+    double* d_scalar = nullptr;        // device result slots
+    double* h_scalar = nullptr;        // pinned mirror
+};
+Runtime& rt();
+void ensure_runtime();
+
+template <typename T>
+T* dalloc(size_t n)
+{
+    void* p = nullptr;
+    if(n == 0) n = 1;
+    HB_HOST_CUDA(cudaMalloc(&p, n * sizeof(T)));
+    return static_cast<T*>(p);
+}
+void dfree(void* p);
+
+// Cached solve graph (one per CG vector set / mode).
+struct CGGraph
+{
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    bool conditional = false;          // WHILE node available
+    const double* key[6] = {};
+    int mode = -1;
+    bool precond = true;
+    bool flexible = false;
+    int kernels_per_iteration = 0;     // kernel nodes of one iteration body
+};
+
+// Per-level implementation data (SparseMatrix::optimizationData).
+struct LevelOpt
+{
+    double* diag = nullptr;            // a_ii, read coalesced by the zero-guess backward sweep
+    int* colors = nullptr;
+    int jpl_blocks = 0;                // the reference's nblocks (2 per JPL round)
+    std::vector<int> round_sizes;      // the reference's per-round sizes[]
+    hb::ColorChunks cc{};              // colour-interleaved SpMV map
+
+    // FP32 / implicit-stencil data
+    bool stencil_ok = false;
+    hb::StencilLevel st{};
+    float* diag32 = nullptr;
+    float* inv_diag32 = nullptr;
+
+    // level-0 solver state
+    hb::CGState* cg_state = nullptr;
+    int cg_state_iters = 0;
+    std::vector<std::unique_ptr<CGGraph>> graphs;
+    float* r32 = nullptr;              // FP32 right-hand side of the V-cycle (level 0)
+    float* z32 = nullptr;              // FP32 V-cycle result (level 0)
+    double* vec_scratch = nullptr;     // one FP64 vector of length m (TestCG / TestSymmetry)
+};
+
+// Per-level transfer data (MGData::optimizationData).
+struct MGOpt
+{
+    int* inj_f = nullptr;              // permuted fine row of coarse point i
+    int* inj_c = nullptr;              // permuted coarse row of coarse point i
+    float* rc32 = nullptr;
+    float* xc32 = nullptr;
+};
+
+inline LevelOpt* opt(const SparseMatrix& A) { return static_cast<LevelOpt*>(A.optimizationData); }
+inline MGOpt* mgopt(const SparseMatrix& A) { return A.mgData ? static_cast<MGOpt*>(A.mgData->optimizationData) : nullptr; }
+
+// Operators on raw FP32 level data (mixed V-cycle), defined in operators.cpp.
+int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s);
+
+// Graph-cached solve, defined in cg.cpp.
+int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,
+           double& normr, double& normr0, bool precond, MGPrecision prec, bool flexible, double* hist,
+           double* seconds);
+
+}  // namespace hpcg_b200

@@ -1,0 +1,207 @@
+// The reference's operator API on B200 kernels.  Each function keeps the
+// signature and semantics of its rocHPCG counterpart (cited per function)
+// and launches on the runtime stream; scalar-returning ones block for the
+// result exactly like the reference (which syncs after every dot product).
+#include "hpcg_b200.h"
+#include "internal.hpp"
+
+using namespace hpcg_b200;
+
+namespace {
+
+template <typename F>
+int guarded(F&& f)
+{
+    try
+    {
+        ensure_runtime();
+        return f();
+    }
+    catch(const Error& e)
+    {
+        return report(e);
+    }
+}
+
+double read_scalar(int slot)
+{
+    Runtime& R = rt();
+    HB_HOST_CUDA(cudaMemcpyAsync(R.h_scalar + slot, R.d_scalar + slot, sizeof(double), cudaMemcpyDeviceToHost,
+                                 R.stream));
+    HB_HOST_CUDA(cudaStreamSynchronize(R.stream));
+    return R.h_scalar[slot];
+}
+
+}  // namespace
+
+// src/ComputeSPMV.cpp:226-278.  (The reference computes only the rows the
+// restriction needs when y is mgData->Axf; the full product is a superset.)
+int ComputeSPMV(const SparseMatrix& A, Vector& x, Vector& y)
+{
+    return guarded([&] {
+        ExchangeHalo(A, x);
+        if(A.mgData && &y == A.mgData->Axf && !y.d_values) CudaInitializeVector(y, A.localNumberOfColumns);
+        const LevelOpt* o = opt(A);
+        return hb::launch_spmv(A.localNumberOfRows, o ? o->cc : hb::make_chunks(A.localNumberOfRows, 0, nullptr),
+                               A.ell_col_ind, A.ell_val, x.d_values, y.d_values, rt().stream);
+    });
+}
+
+// src/ComputeSYMGS.cpp:369-404.
+int ComputeSYMGS(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] {
+        ExchangeHalo(A, x);
+        return hb::launch_symgs(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind,
+                                A.ell_val, A.inv_diag, r.d_values, x.d_values, rt().stream);
+    });
+}
+
+// src/ComputeSYMGS.cpp:406-454.
+int ComputeSYMGSZeroGuess(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] {
+        return hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind,
+                                     A.ell_val, A.diag_idx, opt(A)->diag, A.inv_diag, r.d_values, x.d_values,
+                                     rt().stream);
+    });
+}
+
+// src/ComputeRestriction.cpp:199-237.
+int ComputeFusedSpMVRestriction(const SparseMatrix& A, const Vector& rf, Vector& xf)
+{
+    return guarded([&] {
+        ExchangeHalo(A, xf);
+        const MGOpt* mo = mgopt(A);
+        return hb::launch_restrict(A.mgData->rc->localLength, mo->inj_f, mo->inj_c, A.localNumberOfRows,
+                                   A.ell_col_ind, A.ell_val, rf.d_values, xf.d_values, A.mgData->rc->d_values,
+                                   rt().stream);
+    });
+}
+
+// src/ComputeRestriction.cpp:182-197 (uses mgData->Axf = A xf from ComputeSPMV).
+int ComputeRestriction(const SparseMatrix& A, const Vector& rf)
+{
+    return guarded([&] {
+        const MGOpt* mo = mgopt(A);
+        if(!A.mgData->Axf->d_values) return hb::record_error(HPCGB200_ERR_ARG, "ComputeRestriction: Axf not computed");
+        return hb::launch_restrict_axf(A.mgData->rc->localLength, mo->inj_f, mo->inj_c, rf.d_values,
+                                       A.mgData->Axf->d_values, A.mgData->rc->d_values, rt().stream);
+    });
+}
+
+// src/ComputeProlongation.cpp:72-86.
+int ComputeProlongation(const SparseMatrix& Af, Vector& xf)
+{
+    return guarded([&] {
+        const MGOpt* mo = mgopt(Af);
+        return hb::launch_prolong(Af.mgData->rc->localLength, mo->inj_f, mo->inj_c, Af.mgData->xc->d_values,
+                                  xf.d_values, rt().stream);
+    });
+}
+
+// src/ComputeMG.cpp:64-102.
+int ComputeMG(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    if(A.mgData)
+    {
+        int ierr = ComputeSYMGSZeroGuess(A, r, x);
+        if(ierr) return ierr;
+        for(int i = 1; i < A.mgData->numberOfPresmootherSteps; ++i)
+            if((ierr = ComputeSYMGS(A, r, x))) return ierr;
+        if((ierr = ComputeFusedSpMVRestriction(A, r, x))) return ierr;
+        if((ierr = ComputeMG(*A.Ac, *A.mgData->rc, *A.mgData->xc))) return ierr;
+        if((ierr = ComputeProlongation(A, x))) return ierr;
+        for(int i = 0; i < A.mgData->numberOfPostsmootherSteps; ++i)
+            if((ierr = ComputeSYMGS(A, r, x))) return ierr;
+        return 0;
+    }
+    return ComputeSYMGSZeroGuess(A, r, x);
+}
+
+namespace hpcg_b200 {
+
+// FP32 V-cycle on level data, same recursion as ComputeMG.
+int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s)
+{
+    const LevelOpt* o = opt(A);
+    HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s));
+    if(!A.mgData) return 0;
+    const MGOpt* mo = mgopt(A);
+    const int nc = A.Ac->localNumberOfRows;
+    HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
+    HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
+    HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
+    return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
+}
+
+}  // namespace hpcg_b200
+
+// FP32 V-cycle preconditioner for FP64 vectors: the level-0 zero-guess sweep
+// reads r in FP64 (storing its float copy), the post-smoother writes z in FP64.
+int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] {
+        const LevelOpt* o = opt(A);
+        for(const SparseMatrix* M = &A; M; M = M->Ac)
+            if(!opt(*M) || !opt(*M)->stencil_ok)
+                return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
+                                        "mixed V-cycle needs the 27-point stencil in parity colouring on every level");
+        cudaStream_t s = rt().stream;
+        const int m = A.localNumberOfRows;
+        HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r.d_values, o->r32, o->z32, s));
+        if(!A.mgData) return hb::launch_cast_f2d(m, o->z32, x.d_values, s);
+        const MGOpt* mo = mgopt(A);
+        const int nc = A.Ac->localNumberOfRows;
+        HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
+        HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
+        HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
+        return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
+    });
+}
+
+// src/ComputeDotProduct.cpp:189-238 (blocking, like the reference).
+int ComputeDotProduct(local_int_t n, const Vector& x, const Vector& y, double& result, double& time_allreduce,
+                      bool& isOptimized)
+{
+    (void)time_allreduce;  // one rank: no allreduce
+    (void)isOptimized;
+    return guarded([&] {
+        HB_RETURN_IF(hb::launch_dot(n, x.d_values, y.d_values, rt().ws, rt().d_scalar, rt().stream));
+        result = read_scalar(0);
+        return 0;
+    });
+}
+
+// src/ComputeWAXPBY.cpp:111-135.
+int ComputeWAXPBY(local_int_t n, double alpha, const Vector& x, double beta, const Vector& y, Vector& w,
+                  bool& isOptimized)
+{
+    (void)isOptimized;
+    return guarded([&] {
+        if(n == 0) return 0;
+        return hb::launch_waxpby(n, alpha, x.d_values, beta, y.d_values, w.d_values, rt().stream);
+    });
+}
+
+// src/ComputeWAXPBY.cpp:198-240.
+int ComputeFusedWAXPBYDot(local_int_t n, double alpha, const Vector& x, Vector& y, double& result,
+                          double& time_allreduce)
+{
+    (void)time_allreduce;
+    return guarded([&] {
+        HB_RETURN_IF(hb::launch_waxpby_dot(n, alpha, x.d_values, y.d_values, rt().ws, rt().d_scalar, rt().stream));
+        result = read_scalar(0);
+        return 0;
+    });
+}
+
+// src/ComputeResidual.cpp:121-152.
+int ComputeResidual(local_int_t n, const Vector& v1, const Vector& v2, double& residual)
+{
+    return guarded([&] {
+        HB_RETURN_IF(hb::launch_residual_inf(n, v1.d_values, v2.d_values, rt().ws, rt().d_scalar, rt().stream));
+        residual = read_scalar(0);
+        return 0;
+    });
+}

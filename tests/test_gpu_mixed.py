@@ -1,0 +1,58 @@
+"""Mixed precision: FP64 outer CG with the FP32 V-cycle on the implicit
+stencil.  The V-cycle must equal the CPU FP32 restatement of the ELL kernels
+bit for bit; the solve must reach 1e-9 verified by an FP64 true residual."""
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import host, problems, sync, to_dev
+
+pytestmark = pytest.mark.gpu
+
+FLT_OVER_DBL = np.finfo(np.float32).eps / np.finfo(np.float64).eps
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32)])
+def test_mixed_vcycle_bitwise(dims):
+    import rochpcg_b200 as R
+
+    P, O = problems(*dims)
+    r = np.random.default_rng(3).normal(size=O.levels[0].m)
+    rd, zd = to_dev(r), torch.empty(O.levels[0].m, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    P.mg(rd.data_ptr(), zd.data_ptr(), mode=R.MODE_MIXED)
+    sync(P)
+    z_oracle = O.mg_f32(r.astype(np.float32)).astype(np.float64)
+    assert np.array_equal(host(zd), z_oracle)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_mixed_cg_converges_fp64_verified(n):
+    import rochpcg_b200 as R
+    from rochpcg_b200.rhs import normal_rhs
+
+    P = R.Problem(n)
+    fp = P.cg(1000, 1e-9)
+    mx = P.cg(1000, 1e-9, mode=R.MODE_MIXED)
+    assert mx["normr"] / mx["normr0"] <= 1e-9
+    assert P.true_residual() <= 2e-9
+    assert mx["niters"] <= fp["niters"] + 3
+    P.set_rhs(normal_rhs(P.rows[0], 0))
+    fp = P.cg(1000, 1e-9)
+    mx = P.cg(1000, 1e-9, mode=R.MODE_MIXED)
+    assert P.true_residual() <= 2e-9
+    assert mx["niters"] <= fp["niters"] + 3
+    P.close()
+
+
+def test_mixed_test_symmetry_and_test_cg():
+    import rochpcg_b200 as R
+
+    P, _ = problems(32, 32, 32)
+    s = P.test_symmetry(mode=R.MODE_MIXED)
+    assert s["depsym_spmv"] <= 1.0
+    # the FP32 V-cycle is symmetric to single-precision rounding: the
+    # reference's DBL_EPSILON-scaled departure, rescaled to FLT_EPSILON
+    assert s["depsym_mg"] / FLT_OVER_DBL <= 1.0
+    t = P.test_cg(mode=R.MODE_MIXED)
+    assert t["count_fail"] == 0, t
