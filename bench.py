@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--mixed-nx", type=int, default=320)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-iter", type=int, default=1000,
+                    help="iteration cap per solve (profiling runs use a few iterations)")
+    ap.add_argument("--lite", action="store_true",
+                    help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
+    ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
     return ap.parse_args()
 
 
@@ -260,6 +265,9 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.mixed_only:
+        return run_mixed_only(args, R, barrier)
+
     nx = args.nx
     P = R.Problem(nx)
     flops_it, bytes_it = P.model()
@@ -268,7 +276,7 @@ def run_ours(args):
 
     # ---- device-timed solves (inputs resident in HBM)
     for _ in range(args.warmup):
-        P.cg(1000, args.tol)
+        P.cg(args.max_iter, args.tol)
     barrier()
     sampler = ClockSampler(dev)
     sampler.start()
@@ -276,7 +284,7 @@ def run_ours(args):
     e0.record(stream)
     runs = []
     for _ in range(args.steps):
-        runs.append(P.cg(1000, args.tol))
+        runs.append(P.cg(args.max_iter, args.tol))
     e1.record(stream)
     e1.synchronize()
     barrier()
@@ -289,6 +297,15 @@ def run_ours(args):
     true_rel = P.true_residual()
     kpi = P.kernels_per_iteration(R.MODE_FP64)
     launches = args.steps * (iters * kpi + 2)
+
+    if args.lite:
+        if rank == 0:
+            print(json.dumps({"lite": True, "metric": METRIC, "value": value, "unit": "GFLOP/s", "iterations": iters,
+                              "ms_per_step": ms_step, "gpu_launches": launches}))
+        P.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     # ---- end to end through the C ABI from pinned host memory
     b_host = torch.from_numpy(generated_b_natural(nx, nx, nx)).pin_memory()
@@ -324,29 +341,7 @@ def run_ours(args):
     # ---- mixed precision vs FP64 at 320^3, b ~ N(0,1) seed 0
     mixed = None
     if not args.no_mixed:
-        from rochpcg_b200.rhs import normal_rhs
-
-        n3 = args.mixed_nx
-        Q = R.Problem(n3)
-        Q.set_rhs(normal_rhs(Q.rows[0], 0))
-        f3, _ = Q.model()
-        res = {}
-        for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED)):
-            Q.cg(1000, args.tol, mode=mode)
-            barrier()
-            ts = []
-            for _ in range(2):
-                r3 = Q.cg(1000, args.tol, mode=mode)
-                ts.append(r3["seconds"])
-            res[name] = {"time_to_1e-9_s": min(ts), "iterations": r3["niters"],
-                         "rel_residual_recurrence": r3["normr"] / r3["normr0"],
-                         "rel_residual_fp64_true": Q.true_residual(),
-                         "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9}
-        res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
-        res["grid"] = [n3, n3, n3]
-        res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
-        mixed = res
-        Q.close()
+        mixed = mixed_comparison(args, R, barrier)
 
     # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1)
     cpu = None
@@ -381,6 +376,44 @@ def run_ours(args):
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def mixed_comparison(args, R, barrier, steps=2, warmup=1):
+    """FP64-outer / FP32 V-cycle vs plain FP64 on the same n^3
+    system with b ~ N(0,1) (seed 0), both to args.tol, both verified with an
+    FP64 true residual."""
+    from rochpcg_b200.rhs import normal_rhs
+
+    n3 = args.mixed_nx
+    Q = R.Problem(n3)
+    Q.set_rhs(normal_rhs(Q.rows[0], 0))
+    f3, _ = Q.model()
+    res = {}
+    for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED)):
+        for _ in range(warmup):
+            Q.cg(args.max_iter, args.tol, mode=mode)
+        barrier()
+        ts = []
+        for _ in range(steps):
+            r3 = Q.cg(args.max_iter, args.tol, mode=mode)
+            ts.append(r3["seconds"])
+        res[name] = {"time_to_1e-9_s": min(ts), "iterations": r3["niters"],
+                     "rel_residual_recurrence": r3["normr"] / r3["normr0"],
+                     "rel_residual_fp64_true": Q.true_residual(),
+                     "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9,
+                     "kernels_per_iteration": Q.kernels_per_iteration(mode)}
+    res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
+    res["grid"] = [n3, n3, n3]
+    res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
+    Q.close()
+    return res
+
+
+def run_mixed_only(args, R, barrier):
+    res = mixed_comparison(args, R, barrier, steps=args.steps, warmup=args.warmup)
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps({"mixed_only": True, "metric": METRIC, "mixed": res}))
     return 0
 
 

@@ -11,6 +11,7 @@
 // as a per-iteration graph with a host-side check.
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "hpcg_b200.h"
@@ -149,6 +150,15 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
     return o->graphs.back().get();
 }
 
+// HPCGB200_GRAPH=0 runs the iteration body as direct launches with a host
+// check per iteration (for profilers that cannot look inside graphs with
+// conditional nodes); the kernels and their order are the same.
+static bool graphs_enabled()
+{
+    const char* e = std::getenv("HPCGB200_GRAPH");
+    return !(e && e[0] == '0');
+}
+
 int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,
            double& normr, double& normr0, bool precond, MGPrecision prec, bool flexible, double* hist,
            double* seconds)
@@ -184,7 +194,17 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaStreamSynchronize(s));
 
         const bool iterate = max_iter >= 1 && (h.normr / h.normr0 > tol);
-        if(iterate)
+        if(iterate && !graphs_enabled())
+        {
+            for(int k = 1; k <= max_iter; ++k)
+            {
+                check(capture_body(A, data, x, precond, prec, st, 0ULL, s));
+                HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+                HB_HOST_CUDA(cudaStreamSynchronize(s));
+                if(!(h.normr / h.normr0 > tol)) break;
+            }
+        }
+        else if(iterate)
         {
             CGGraph* G = get_graph(A, data, b, x, precond, prec, flexible);
             if(G->conditional)
