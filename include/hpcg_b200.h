@@ -146,6 +146,20 @@ int hpcgb200_prolong(int nc, const int* inj_f, const int* inj_c, const double* x
 int hpcgb200_dot(int n, const double* x, const double* y, double* result, void* workspace, size_t workspace_bytes,
                  void* stream);
 
+/* No counterpart in the reference.  The dot product for callers that cannot
+ * allocate device memory: applications whose device memory belongs to their
+ * own pool (a framework's caching allocator, a plugin with a fixed budget)
+ * and latency-critical callers for which cudaMalloc -- which can synchronize
+ * the device -- is not allowed.  *result (DEVICE pointer) = sum x[i]*y[i],
+ * with no workspace argument: the scratch is a 32 KB array inside the library
+ * that every GPU loading the library keeps until the process exits.
+ * n <= 16,777,216 (4096 partial sums of 4096-element tiles); larger n returns
+ * HPCGB200_ERR_ARG.  All calls share that array: calls that overlap on the
+ * GPU race, so serialize them.  The first call on a device looks up the
+ * array's address (once per device); make it before any stream capture.
+ * Allocates nothing.  Same value as hpcgb200_dot up to summation order. */
+int hpcgb200_dot_noalloc(long long n, const double* x, const double* y, double* result, void* stream);
+
 /* src/ComputeWAXPBY.cpp:63-135 (kernel_waxpby): w = alpha x + beta y with the
  * reference's alpha==1 / beta==1 fma forms. */
 int hpcgb200_waxpby(int n, double alpha, const double* x, double beta, const double* y, double* w, void* stream);
