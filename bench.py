@@ -404,6 +404,17 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
                      "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9,
                      "kernels_per_iteration": Q.kernels_per_iteration(mode)}
     res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
+    # level-0 kernels of the mixed path, timed alone (CUDA events)
+    m3 = Q.rows[0]
+    rows_c = m3 // 8
+    sw = Q.time_op("symgs32_sweep", 10)
+    sw_bytes = rows_c * (4 + 4 + 4) + (m3 - rows_c) * 4
+    sp = Q.time_op("spmv_stencil", 10)
+    sp_bytes = m3 * (8 + 8 + 8)
+    res["kernels"] = {"k32_sweep_ms": sw, "k32_sweep_GBps": sw_bytes / (sw * 1e-3) / 1e9,
+                      "k32_sweep_algorithmic_bytes": sw_bytes,
+                      "k64_spmv_stencil_ms": sp, "k64_spmv_stencil_GBps": sp_bytes / (sp * 1e-3) / 1e9,
+                      "mg_mixed_ms": Q.time_op("mg_mixed", 5), "mg_fp64_ms": Q.time_op("mg", 3)}
     res["grid"] = [n3, n3, n3]
     res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
     Q.close()

@@ -232,7 +232,7 @@ int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const double* b_n
 int hpcgb200_problem_true_residual(hpcgb200_problem* p, double* rel);
 
 /* Number of kernel launches one CG iteration of the given mode issues (the
- * kernel nodes of the captured iteration graph; available after a solve). */
+ * kernel nodes of its iteration graph, captured here if needed). */
 int hpcgb200_problem_kernels_per_iteration(hpcgb200_problem* p, int mode, int precond, int* kernels);
 
 /* src/TestCG.cpp:111-177.  out[0..3] = niters of unpreconditioned call 0,1
@@ -248,6 +248,9 @@ int hpcgb200_problem_test_symmetry(hpcgb200_problem* p, int mode, double* depsym
 /* Per-operator calls on the handle's level data (vectors are DEVICE
  * pointers in permuted order), used by the operator parity tests. */
 int hpcgb200_problem_spmv(hpcgb200_problem* p, int level, const double* x, double* y);
+/* y = A x on the implicit stencil (the mixed path's FP64 operator); no
+ * reference counterpart; bitwise equal to hpcgb200_problem_spmv. */
+int hpcgb200_problem_spmv_stencil(hpcgb200_problem* p, int level, const double* x, double* y);
 int hpcgb200_problem_symgs(hpcgb200_problem* p, int level, const double* r, double* x);
 int hpcgb200_problem_symgs_zero(hpcgb200_problem* p, int level, const double* r, double* x);
 int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* r, double* x);
@@ -257,7 +260,8 @@ int hpcgb200_problem_prolong(hpcgb200_problem* p, int level, const double* xc, d
 /* Time n back-to-back launches of one level-0 operator with CUDA events on
  * the problem's stream; *ms_per_launch = average.  op: "spmv","symgs_sweep"
  * (one full-row color sweep, averaged over the 15 of a SymGS step),
- * "symgs","symgs_zero","mg","mg_mixed". */
+ * "symgs","symgs_zero","mg","mg_mixed", "symgs32_sweep" (one FP32 implicit
+ * colour sweep, averaged over a SymGS step), "spmv_stencil". */
 int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
 
 #ifdef __cplusplus

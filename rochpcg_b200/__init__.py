@@ -187,6 +187,10 @@ class Problem:
     def spmv(self, level: int, x_ptr: int, y_ptr: int):
         check(self.L, self.L.hpcgb200_problem_spmv(self.h, level, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr)))
 
+    def spmv_stencil(self, level: int, x_ptr: int, y_ptr: int):
+        check(self.L, self.L.hpcgb200_problem_spmv_stencil(self.h, level, ctypes.c_void_p(x_ptr),
+                                                           ctypes.c_void_p(y_ptr)))
+
     def symgs(self, level: int, r_ptr: int, x_ptr: int):
         check(self.L, self.L.hpcgb200_problem_symgs(self.h, level, ctypes.c_void_p(r_ptr), ctypes.c_void_p(x_ptr)))
 

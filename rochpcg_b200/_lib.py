@@ -60,6 +60,7 @@ SIGNATURES = {
     "hpcgb200_problem_test_cg": (_i, [_vp, _i, _vp, _vp, _vp]),
     "hpcgb200_problem_test_symmetry": (_i, [_vp, _i, _vp, _vp, _vp]),
     "hpcgb200_problem_spmv": (_i, [_vp, _i, _vp, _vp]),
+    "hpcgb200_problem_spmv_stencil": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_symgs": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_symgs_zero": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_mg": (_i, [_vp, _i, _vp, _vp]),

@@ -75,22 +75,20 @@ __global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const double* __rest
     else p[i] = fma(st->beta, p[i], z[i]);          // WAXPBY(1, z, beta, p)
 }
 
-// Ap = A p (interleaved colour map as k_spmv) and pAp; alpha = rtz / pAp.
-__global__ void __launch_bounds__(kReduceThreads) k_cg_spmv_pap(int m, ColorChunks cc,
-                                                                const int* __restrict__ ell_col,
-                                                                const double* __restrict__ ell_val,
-                                                                const double* __restrict__ p,
-                                                                double* __restrict__ Ap, CGState* st,
-                                                                ReduceScratch* ws)
+// Ap = A p (one row per thread, colour-interleaved blocks as k_spmv) and
+// pAp: one partial per block, summed in block order by the last block, which
+// forms alpha = rtz / pAp.
+__global__ void __launch_bounds__(kBS) k_cg_spmv_pap(int m, ColorChunks cc, const int* __restrict__ ell_col,
+                                                     const double* __restrict__ ell_val,
+                                                     const double* __restrict__ p, double* __restrict__ Ap,
+                                                     CGState* st, double* partial, unsigned int* ticket)
 {
-    static_assert(kReduceThreads == kBS, "chunk map assumes kBS threads");
     __shared__ double red[32];
+    __shared__ bool last;
     double s = 0.0;
-    const int nch = cc.nchunks();
-    for(int ch = blockIdx.x; ch < nch; ch += gridDim.x)
+    int row;
+    if(cc.row_of(blockIdx.x, threadIdx.x, row))
     {
-        int row;
-        if(!cc.row_of(ch, threadIdx.x, row)) continue;
         double sum = 0.0;
 #pragma unroll
         for(int q = 0; q < kWidth; ++q)
@@ -101,14 +99,26 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_spmv_pap(int m, ColorChun
             if(col >= 0 && col < m) sum = fma(v, __ldg(p + col), sum);
         }
         Ap[row] = sum;
-        s = fma(sum, p[row], s);
+        s = sum * p[row];
     }
     s = block_sum(s, red);
-    double total;
-    if(grid_reduce(s, ws, gridDim.x, &total))
+    if(threadIdx.x == 0)
     {
-        st->pAp = total;
-        st->alpha = st->rtz / total;
+        partial[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(unsigned i = threadIdx.x; i < gridDim.x; i += kBS) acc += __ldcg(&partial[i]);
+    acc = block_sum(acc, red);
+    if(threadIdx.x == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
     }
 }
 
@@ -201,10 +211,9 @@ int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cud
 }
 
 int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
-                       double* Ap, CGState* st, ReduceScratch* ws, cudaStream_t s)
+                       double* Ap, CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
-    const int grid = cc.nchunks() < kReduceBlocks ? cc.nchunks() : kReduceBlocks;
-    k_cg_spmv_pap<<<grid, kReduceThreads, 0, s>>>(m, cc, ell_col, ell_val, p, Ap, st, ws);
+    k_cg_spmv_pap<<<cc.nchunks(), kBS, 0, s>>>(m, cc, ell_col, ell_val, p, Ap, st, partial, ticket);
     HB_LAUNCHED();
     return 0;
 }

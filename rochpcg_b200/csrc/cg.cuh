@@ -33,9 +33,10 @@ int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGS
 int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
 // p = z (k == 1) or p = z + beta p.
 int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s);
-// Ap = A p and alpha = rtz / (p.Ap).
+// Ap = A p and alpha = rtz / (p.Ap); `partial` holds cc.nchunks() per-block
+// sums, `ticket` must start at zero and is left at zero.
 int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
-                       double* Ap, CGState* st, ReduceScratch* ws, cudaStream_t s);
+                       double* Ap, CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
 // r -= alpha Ap, normr = ||r||, x += alpha p, history; then (own 1-thread
 // kernel) k++ and the loop condition (k <= max_iter && normr/normr0 > tol)
 // written to `cond` (a graph conditional handle; 0 = none).

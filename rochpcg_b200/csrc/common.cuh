@@ -79,16 +79,25 @@ __device__ __forceinline__ T warp_max(T v)
     return v;
 }
 
-// Block-wide sum (blockDim.x multiple of 32, <= 1024); result valid in thread 0.
+// Linear thread index and size of the block (1-D, 2-D and 3-D blocks).
+__device__ __forceinline__ int block_tid()
+{
+    return (int)(threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
+}
+__device__ __forceinline__ int block_threads() { return (int)(blockDim.x * blockDim.y * blockDim.z); }
+
+// Block-wide sum (block size a multiple of 32, <= 1024); result valid in the
+// thread with block_tid() == 0.
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* smem /* >= 32 */)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = block_tid();
+    const int lane = tid & 31, warp = tid >> 5;
     v = warp_sum(v);
     if(lane == 0) smem[warp] = v;
     __syncthreads();
-    const int nw = blockDim.x >> 5;
-    T r = (threadIdx.x < nw) ? smem[threadIdx.x] : T(0);
+    const int nw = block_threads() >> 5;
+    T r = (tid < nw) ? smem[tid] : T(0);
     if(warp == 0) r = warp_sum(r);
     __syncthreads();
     return r;
@@ -97,12 +106,13 @@ __device__ __forceinline__ T block_sum(T v, T* smem /* >= 32 */)
 template <typename T>
 __device__ __forceinline__ T block_max(T v, T* smem)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = block_tid();
+    const int lane = tid & 31, warp = tid >> 5;
     v = warp_max(v);
     if(lane == 0) smem[warp] = v;
     __syncthreads();
-    const int nw = blockDim.x >> 5;
-    T r = (threadIdx.x < nw) ? smem[threadIdx.x] : T(0);
+    const int nw = block_threads() >> 5;
+    T r = (tid < nw) ? smem[tid] : T(0);
     if(warp == 0) r = warp_max(r);
     __syncthreads();
     return r;

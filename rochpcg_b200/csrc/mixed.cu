@@ -1,6 +1,8 @@
-// FP32 implicit-stencil V-cycle kernels (see mixed.cuh).  Per row they read
-// the float residual, the float diagonal reciprocal and the 26 gathered
-// neighbours, i.e. ~12 B of streamed data instead of 27 x 12 B of ELL.
+// Implicit-stencil kernels (see mixed.cuh).  Per row the FP32 sweeps stream
+// the float residual and diagonal reciprocal (8 B) and write x (4 B); the 26
+// neighbours are gathered with all loads issued before the ordered adds (an
+// absent neighbour contributes -0.0f, which leaves any sum unchanged, so the
+// rounding sequence is exactly the ELL sweep's).
 #include <algorithm>
 #include <array>
 
@@ -18,6 +20,7 @@ bool make_stencil_level(int nx, int ny, int nz, const int* offsets, const int co
     L.nz = nz;
     L.m = nx * ny * nz;
     L.ncolors = 8;
+    L.even = (nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0) ? 1 : 0;
     bool seen[8] = {};
     for(int p = 0; p < 8; ++p)
     {
@@ -37,43 +40,40 @@ bool make_stencil_level(int nx, int ny, int nz, const int* offsets, const int co
         if(L.offsets[v + 1] - L.offsets[v] != bx * by * bz) return false;
         L.bx[v] = bx;
         L.by[v] = by;
+    }
+    for(int v = 0; v < 8; ++v)
+    {
+        const int p = L.par[v];
+        const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
         // ELL slot order of colour v: neighbour colour, then (dz,dy,dx)
-        std::array<std::array<int, 5>, 27> e{};
+        std::array<std::array<int, 4>, 27> e{};
         int k = 0;
         for(int dz = -1; dz <= 1; ++dz)
             for(int dy = -1; dy <= 1; ++dy)
                 for(int dx = -1; dx <= 1; ++dx)
                 {
                     const int p2 = p ^ (((dx & 1) << 2) | ((dy & 1) << 1) | (dz & 1));
-                    e[k++] = {L.color_of_par[p2], dz, dy, dx, 0};
+                    e[k++] = {L.color_of_par[p2], dz, dy, dx};
                 }
         std::sort(e.begin(), e.end());
+        StencilTab& T = L.tab[v];
         for(int j = 0; j < 27; ++j)
         {
             const int v2 = e[j][0], dz = e[j][1], dy = e[j][2], dx = e[j][3];
-            L.nb[v][j] = (unsigned short)((dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4) | (v2 << 8));
-            if(dx == 0 && dy == 0 && dz == 0) L.diag_pos[v] = (unsigned char)j;
+            T.nb[j] = (unsigned short)((dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4) | (v2 << 8));
+            if(dx == 0 && dy == 0 && dz == 0) T.dp = j;
+            // brick-coordinate steps: floor((parity + d) / 2)
+            const int dkx = (px + dx + 2) / 2 - 1, dky = (py + dy + 2) / 2 - 1, dkz = (pz + dz + 2) / 2 - 1;
+            T.delta[j] = (L.offsets[v2] - L.offsets[v]) + (dkz * L.by[v2] + dky) * L.bx[v2] + dkx;
+            T.bmask[j] = (unsigned char)((dx < 0 ? 1 : 0) | (dx > 0 ? 2 : 0) | (dy < 0 ? 4 : 0) | (dy > 0 ? 8 : 0) |
+                                         (dz < 0 ? 16 : 0) | (dz > 0 ? 32 : 0));
         }
     }
     *out = L;
     return true;
 }
 
-__device__ __forceinline__ void row_coords(const StencilLevel& L, int v, int row, int& ix, int& iy, int& iz)
-{
-    const int q = row - L.offsets[v];
-    const int bx = L.bx[v], by = L.by[v];
-    const int kx = q % bx;
-    const int t = q / bx;
-    const int ky = t % by;
-    const int kz = t / by;
-    const int p = L.par[v];
-    ix = 2 * kx + ((p >> 2) & 1);
-    iy = 2 * ky + ((p >> 1) & 1);
-    iz = 2 * kz + (p & 1);
-}
-
-// Column of neighbour entry e of a row at (ix,iy,iz); false outside the grid.
+// Column of neighbour entry e of a row at (ix,iy,iz) for any grid; false outside it.
 __device__ __forceinline__ bool nb_col(const StencilLevel& L, unsigned e, int ix, int iy, int iz, int& col)
 {
     const int x = ix + (int)(e & 3) - 1;
@@ -85,16 +85,146 @@ __device__ __forceinline__ bool nb_col(const StencilLevel& L, unsigned e, int ix
     return true;
 }
 
-// Forward zero-guess sweep of colour v: only neighbours of earlier colours,
-// which are exactly the slots before the diagonal.
-template <bool kFromDouble>
-__global__ void __launch_bounds__(kBS32) k32_fwd0(const StencilLevel L, int v, const float* __restrict__ inv_diag32,
-                                                  const double* __restrict__ r64, float* __restrict__ r32, float* x)
+// Everything a launch over the rows of ONE colour needs, passed as its own
+// kernel parameter: the unrolled slot loop then reads the table from the
+// constant bank at static offsets (a table indexed by a runtime colour would
+// cost a constant-cache load per slot and per thread).
+struct ColorLaunch
 {
-    const int size = L.offsets[v + 1] - L.offsets[v];
-    const int gid = blockIdx.x * kBS32 + threadIdx.x;
-    if(gid >= size) return;
-    const int row = L.offsets[v] + gid;
+    StencilTab tb;
+    int v, off, bx, by, bz, par;
+    int nx, ny, nz, even;
+};
+
+static ColorLaunch color_launch(const StencilLevel& L, int v)
+{
+    ColorLaunch c{};
+    c.tb = L.tab[v];
+    c.v = v;
+    c.off = L.offsets[v];
+    c.bx = L.bx[v];
+    c.by = L.by[v];
+    c.par = L.par[v];
+    c.bz = (L.nz - (c.par & 1) + 1) / 2;
+    c.nx = L.nx;
+    c.ny = L.ny;
+    c.nz = L.nz;
+    c.even = L.even;
+    return c;
+}
+
+// Faces of the grid a point lies on (bit order as StencilTab::bmask).
+__device__ __forceinline__ unsigned face_mask(const ColorLaunch& c, int ix, int iy, int iz)
+{
+    return (ix == 0 ? 1u : 0u) | (ix == c.nx - 1 ? 2u : 0u) | (iy == 0 ? 4u : 0u) | (iy == c.ny - 1 ? 8u : 0u) |
+           (iz == 0 ? 16u : 0u) | (iz == c.nz - 1 ? 32u : 0u);
+}
+
+struct BrickRow
+{
+    int row, ix, iy, iz;
+    unsigned mask;
+    bool in, fast;
+};
+
+// Thread (kx, ky) of a 32 x 8 block, brick plane kz: position of the row
+// without divisions.  `fast`: even grid and no lane of the warp on a face.
+__device__ __forceinline__ BrickRow brick_row(const ColorLaunch& c, int kz)
+{
+    BrickRow b;
+    const int kx = blockIdx.x * 32 + threadIdx.x;
+    const int ky = blockIdx.y * 8 + threadIdx.y;
+    b.in = kx < c.bx && ky < c.by && kz < c.bz;
+    b.ix = 2 * kx + ((c.par >> 2) & 1);
+    b.iy = 2 * ky + ((c.par >> 1) & 1);
+    b.iz = 2 * kz + (c.par & 1);
+    b.mask = b.in ? face_mask(c, b.ix, b.iy, b.iz) : 0x3fu;
+    b.fast = c.even && __all_sync(0xffffffffu, b.mask == 0u);
+    b.row = c.off + (kz * c.by + ky) * c.bx + kx;
+    return b;
+}
+
+// Position of a given row of the colour (1-D launches: restriction).
+__device__ __forceinline__ BrickRow row_of(const ColorLaunch& c, int row, bool in)
+{
+    BrickRow b;
+    const int q = in ? row - c.off : 0;
+    const int t = q / c.bx;
+    const int kx = q - t * c.bx;
+    const int kz = t / c.by;
+    const int ky = t - kz * c.by;
+    b.in = in;
+    b.row = row;
+    b.ix = 2 * kx + ((c.par >> 2) & 1);
+    b.iy = 2 * ky + ((c.par >> 1) & 1);
+    b.iz = 2 * kz + (c.par & 1);
+    b.mask = in ? face_mask(c, b.ix, b.iy, b.iz) : 0x3fu;
+    b.fast = c.even && __all_sync(0xffffffffu, b.mask == 0u);
+    return b;
+}
+
+// Slot selection of the sweeps.
+enum Sel
+{
+    kBefore = 0,  // slots before the diagonal (earlier colours)
+    kAfter = 1,   // slots after the diagonal (later colours)
+    kOff = 2      // every off-diagonal slot
+};
+
+template <int kSel>
+__device__ __forceinline__ bool selected(int j, int dp)
+{
+    return kSel == kBefore ? j < dp : (kSel == kAfter ? j > dp : j != dp);
+}
+
+// Neighbour values of slots 0..26 in ELL order; `fill` where the slot is not
+// selected or the neighbour does not exist.  Fast path: constant deltas, no
+// masks.  Even grids: deltas + per-lane face masks.  Odd grids: per-slot
+// brick coordinates.
+template <int kSel, bool kEven, typename T>
+__device__ __forceinline__ void gather(const StencilLevel& L, const ColorLaunch& c, const BrickRow& b, const T* x,
+                                       T fill, T (&val)[27])
+{
+    if(kEven && b.fast)
+    {
+#pragma unroll
+        for(int j = 0; j < 27; ++j) val[j] = selected<kSel>(j, c.tb.dp) ? x[b.row + c.tb.delta[j]] : fill;
+        return;
+    }
+#pragma unroll
+    for(int j = 0; j < 27; ++j)
+    {
+        int col = b.row;
+        bool ok;
+        if(kEven)
+        {
+            col = b.row + c.tb.delta[j];
+            ok = selected<kSel>(j, c.tb.dp) && !(b.mask & c.tb.bmask[j]);
+        }
+        else
+        {
+            ok = selected<kSel>(j, c.tb.dp) && nb_col(L, c.tb.nb[j], b.ix, b.iy, b.iz, col);
+        }
+        val[j] = ok ? x[col] : fill;
+    }
+}
+
+constexpr unsigned kBrickThreads = 256;
+
+inline dim3 brick_grid(const ColorLaunch& c)
+{
+    return dim3((unsigned)((c.bx + 31) / 32), (unsigned)((c.by + 7) / 8), (unsigned)c.bz);
+}
+
+template <bool kEven, bool kFromDouble>
+__global__ void __launch_bounds__(kBrickThreads) k32_fwd0(const ColorLaunch c, const StencilLevel L,
+                                                          const float* __restrict__ inv_diag32,
+                                                          const double* __restrict__ r64, float* __restrict__ r32,
+                                                          float* x)
+{
+    const BrickRow b = brick_row(c, blockIdx.z);
+    if(!b.in) return;
+    const int row = b.row;
     float sum;
     if(kFromDouble)
     {
@@ -105,92 +235,74 @@ __global__ void __launch_bounds__(kBS32) k32_fwd0(const StencilLevel L, int v, c
     {
         sum = r32[row];
     }
-    if(v > 0)
+    if(c.tb.dp > 0)
     {
-        int ix, iy, iz;
-        row_coords(L, v, row, ix, iy, iz);
-        const int dp = L.diag_pos[v];
+        float val[27];
+        gather<kBefore, kEven>(L, c, b, x, -0.0f, val);
 #pragma unroll
-        for(int j = 0; j < 27; ++j)
-        {
-            if(j >= dp) break;
-            int col;
-            if(nb_col(L, L.nb[v][j], ix, iy, iz, col)) sum = sum + x[col];
-        }
+        for(int j = 0; j < 27; ++j) sum = sum + val[j];
     }
     x[row] = sum * inv_diag32[row];
 }
 
-// Backward zero-guess sweep of colour v: x = (d x - sum of later-colour
-// neighbours * (-1)) / d.
-__global__ void __launch_bounds__(kBS32) k32_bwd0(const StencilLevel L, int v, const float* __restrict__ diag32,
-                                                  const float* __restrict__ inv_diag32, float* x)
+template <bool kEven>
+__global__ void __launch_bounds__(kBrickThreads) k32_bwd0(const ColorLaunch c, const StencilLevel L,
+                                                          const float* __restrict__ diag32,
+                                                          const float* __restrict__ inv_diag32, float* x)
 {
-    const int size = L.offsets[v + 1] - L.offsets[v];
-    const int gid = blockIdx.x * kBS32 + threadIdx.x;
-    if(gid >= size) return;
-    const int row = L.offsets[v] + gid;
-    int ix, iy, iz;
-    row_coords(L, v, row, ix, iy, iz);
+    const BrickRow b = brick_row(c, blockIdx.z);
+    if(!b.in) return;
+    const int row = b.row;
+    float val[27];
+    gather<kAfter, kEven>(L, c, b, x, -0.0f, val);
     float sum = __fmul_rn(x[row], diag32[row]);
-    const int dp = L.diag_pos[v];
 #pragma unroll
-    for(int j = 0; j < 27; ++j)
-    {
-        if(j <= dp) continue;
-        int col;
-        if(nb_col(L, L.nb[v][j], ix, iy, iz, col)) sum = sum + x[col];
-    }
+    for(int j = 0; j < 27; ++j) sum = sum + val[j];
     x[row] = sum * inv_diag32[row];
 }
 
-// Full sweep of colour v; optionally stores the final value as double.
-__global__ void __launch_bounds__(kBS32) k32_sweep(const StencilLevel L, int v, const float* __restrict__ inv_diag32,
-                                                   const float* __restrict__ r, float* x, double* __restrict__ z64)
+template <bool kEven>
+__global__ void __launch_bounds__(kBrickThreads) k32_sweep(const ColorLaunch c, const StencilLevel L,
+                                                           const float* __restrict__ inv_diag32,
+                                                           const float* __restrict__ r, float* x,
+                                                           double* __restrict__ z64)
 {
-    const int size = L.offsets[v + 1] - L.offsets[v];
-    const int gid = blockIdx.x * kBS32 + threadIdx.x;
-    if(gid >= size) return;
-    const int row = L.offsets[v] + gid;
-    int ix, iy, iz;
-    row_coords(L, v, row, ix, iy, iz);
+    const BrickRow b = brick_row(c, blockIdx.z);
+    if(!b.in) return;
+    const int row = b.row;
+    float val[27];
+    gather<kOff, kEven>(L, c, b, x, -0.0f, val);
     float sum = r[row];
-    const int dp = L.diag_pos[v];
 #pragma unroll
-    for(int j = 0; j < 27; ++j)
-    {
-        if(j == dp) continue;
-        int col;
-        if(nb_col(L, L.nb[v][j], ix, iy, iz, col)) sum = sum + x[col];
-    }
+    for(int j = 0; j < 27; ++j) sum = sum + val[j];
     const float xn = sum * inv_diag32[row];
     x[row] = xn;
     if(z64) z64[row] = (double)xn;
 }
 
-// Residual at the injected rows (all of parity class 0, colour v0).
-__global__ void __launch_bounds__(kBS32) k32_restrict(const StencilLevel L, int v0, int nc, const int* __restrict__ inj_f,
-                                                      const int* __restrict__ inj_c, const float* __restrict__ diag32,
-                                                      const float* __restrict__ rf, const float* __restrict__ xf,
-                                                      float* __restrict__ rc)
+// Residual at the injected rows (all of parity class 0: launch c is that colour).
+template <bool kEven>
+__global__ void __launch_bounds__(kBS32) k32_restrict(const ColorLaunch c, const StencilLevel L, int nc,
+                                                      const int* __restrict__ inj_f, const int* __restrict__ inj_c,
+                                                      const float* __restrict__ diag32, const float* __restrict__ rf,
+                                                      const float* __restrict__ xf, float* __restrict__ rc)
 {
     const int ic = blockIdx.x * kBS32 + threadIdx.x;
-    if(ic >= nc) return;
-    const int row = inj_f[ic];
-    int ix, iy, iz;
-    row_coords(L, v0, row, ix, iy, iz);
+    const bool in = ic < nc;
+    const BrickRow b = row_of(c, in ? inj_f[ic] : 0, in);
+    if(!in) return;
+    const int row = b.row;
+    float val[27];
+    gather<kOff, kEven>(L, c, b, xf, -0.0f, val);
+    const float dterm = -diag32[row];
+    const float xr = xf[row];
     float sum = rf[row];
-    const int dp = L.diag_pos[v0];
+    // ELL order: the diagonal term at slot dp (val[dp] is the no-op -0.0f)
 #pragma unroll
     for(int j = 0; j < 27; ++j)
     {
-        if(j == dp)
-        {
-            sum = fmaf(-diag32[row], xf[row], sum);
-            continue;
-        }
-        int col;
-        if(nb_col(L, L.nb[v0][j], ix, iy, iz, col)) sum = sum + xf[col];
+        if(j == c.tb.dp) sum = fmaf(dterm, xr, sum);
+        sum = sum + val[j];
     }
     rc[inj_c[ic]] = sum;
 }
@@ -202,6 +314,86 @@ __global__ void __launch_bounds__(kBS32) k32_prolong(int nc, const int* __restri
     if(ic >= nc) return;
     xf[inj_f[ic]] += xc[inj_c[ic]];
 }
+
+// ----------------------------------------------------- FP64 stencil SpMV
+
+// ELL: sum = fma(a, x_col, sum) per existing slot from 0.0, a = -1 off the
+// diagonal: fma(-1, x, s) == s - x, and an absent slot is s - (+0.0) == s.
+template <bool kEven>
+__device__ __forceinline__ double spmv64_row(const ColorLaunch& c, const StencilLevel& L, const BrickRow& b,
+                                             const double* __restrict__ diag, const double* __restrict__ x)
+{
+    double val[27];
+    gather<kOff, kEven>(L, c, b, x, 0.0, val);
+    const double d = diag[b.row];
+    const double xr = x[b.row];
+    double sum = 0.0;
+#pragma unroll
+    for(int j = 0; j < 27; ++j)
+    {
+        if(j == c.tb.dp) sum = fma(d, xr, sum);
+        sum = sum - val[j];
+    }
+    return sum;
+}
+
+template <bool kEven>
+__global__ void __launch_bounds__(kBrickThreads) k64_spmv_color(const ColorLaunch c, const StencilLevel L,
+                                                                const double* __restrict__ diag,
+                                                                const double* __restrict__ x, double* __restrict__ y)
+{
+    const BrickRow b = brick_row(c, blockIdx.z);
+    if(!b.in) return;
+    y[b.row] = spmv64_row<kEven>(c, L, b, diag, x);
+}
+
+// Ap = A p on one colour and its blocks' partial sums of p.Ap into
+// partial[base + block].  The launch of the last colour (`finalize`) also
+// sums every partial of every colour launch (earlier launches are complete:
+// same stream) in index order and forms alpha = rtz / pAp.
+template <bool kEven>
+__global__ void __launch_bounds__(kBrickThreads) k64_pap_color(const ColorLaunch c, const StencilLevel L,
+                                                               const double* __restrict__ diag,
+                                                               const double* __restrict__ p, double* __restrict__ Ap,
+                                                               CGState* st, double* partial, int base, int total,
+                                                               unsigned int* ticket, int finalize)
+{
+    __shared__ double red[32];
+    __shared__ bool last;
+    const BrickRow b = brick_row(c, blockIdx.z);
+    double s = 0.0;
+    if(b.in)
+    {
+        const double sum = spmv64_row<kEven>(c, L, b, diag, p);
+        Ap[b.row] = sum;
+        s = sum * p[b.row];
+    }
+    s = block_sum(s, red);
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const int tid = block_tid();
+    if(tid == 0) partial[base + bid] = s;
+    if(!finalize) return;
+    if(tid == 0)
+    {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == nblocks - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(int i = tid; i < total; i += (int)kBrickThreads) acc += __ldcg(&partial[i]);
+    acc = block_sum(acc, red);
+    if(tid == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
+// ------------------------------------------------------------ set-up kernels
 
 __global__ void k_diag32(int m, const double* __restrict__ diag, float* __restrict__ d32, float* __restrict__ inv32)
 {
@@ -228,20 +420,31 @@ __global__ void k_stencil_check(const StencilLevel L, const int* __restrict__ pe
         const int expect = L.offsets[v] + ((iz >> 1) * L.by[v] + (iy >> 1)) * L.bx[v] + (ix >> 1);
         nbad += perm[i] != expect;
     }
-    // permuted row i -> its ELL row must be the implicit neighbour list
+    // permuted row i -> its ELL row must be the implicit neighbour list, and
+    // on even grids the constant-delta form must give the same columns
     {
         int v = 0;
         while(v + 1 < 8 && i >= L.offsets[v + 1]) ++v;
-        int ix, iy, iz;
-        row_coords(L, v, i, ix, iy, iz);
+        const int q = i - L.offsets[v];
+        const int t = q / L.bx[v];
+        const int kz = t / L.by[v];
+        const int ky = t - kz * L.by[v];
+        const int kx = q - t * L.bx[v];
+        const int p = L.par[v];
+        const int ix = 2 * kx + ((p >> 2) & 1), iy = 2 * ky + ((p >> 1) & 1), iz = 2 * kz + (p & 1);
+        const unsigned mask = (ix == 0 ? 1u : 0u) | (ix == L.nx - 1 ? 2u : 0u) | (iy == 0 ? 4u : 0u) |
+                              (iy == L.ny - 1 ? 8u : 0u) | (iz == 0 ? 16u : 0u) | (iz == L.nz - 1 ? 32u : 0u);
+        const StencilTab& tb = L.tab[v];
         int slot = 0;
         for(int j = 0; j < 27; ++j)
         {
             int col;
-            if(!nb_col(L, L.nb[v][j], ix, iy, iz, col)) continue;
+            const bool ok = nb_col(L, tb.nb[j], ix, iy, iz, col);
+            if(L.even) nbad += ok != !(mask & tb.bmask[j]) || (ok && col != i + tb.delta[j]);
+            if(!ok) continue;
             const size_t idx = (size_t)slot * L.m + i;
             nbad += ell_col[idx] != col;
-            if(j != L.diag_pos[v]) nbad += ell_val[idx] != -1.0;
+            if(j != tb.dp) nbad += ell_val[idx] != -1.0;
             ++slot;
         }
         for(; slot < 27; ++slot) nbad += ell_col[(size_t)slot * L.m + i] != -1;
@@ -270,19 +473,30 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
                         float* r32, float* x, cudaStream_t s)
 {
     const int n = L.ncolors;
+    const dim3 t(32, 8);
     for(int v = 0; v < n; ++v)
     {
-        const int size = L.offsets[v + 1] - L.offsets[v];
-        if(size <= 0) continue;
-        if(r64) k32_fwd0<true><<<nblk(size), kBS32, 0, s>>>(L, v, inv_diag32, r64, r32, x);
-        else k32_fwd0<false><<<nblk(size), kBS32, 0, s>>>(L, v, inv_diag32, nullptr, r32, x);
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
+        const ColorLaunch c = color_launch(L, v);
+        const dim3 g = brick_grid(c);
+        if(L.even)
+        {
+            if(r64) k32_fwd0<true, true><<<g, t, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else k32_fwd0<true, false><<<g, t, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+        }
+        else
+        {
+            if(r64) k32_fwd0<false, true><<<g, t, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else k32_fwd0<false, false><<<g, t, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+        }
         HB_LAUNCHED();
     }
     for(int v = n - 2; v >= 0; --v)
     {
-        const int size = L.offsets[v + 1] - L.offsets[v];
-        if(size <= 0) continue;
-        k32_bwd0<<<nblk(size), kBS32, 0, s>>>(L, v, diag32, inv_diag32, x);
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
+        const ColorLaunch c = color_launch(L, v);
+        if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
+        else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         HB_LAUNCHED();
     }
     return 0;
@@ -292,28 +506,26 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
                    cudaStream_t s)
 {
     const int n = L.ncolors;
-    for(int v = 0; v < n; ++v)
-    {
-        const int size = L.offsets[v + 1] - L.offsets[v];
-        if(size <= 0) continue;
-        // colour n-1 is final after the forward sweep (the backward sweep starts at n-2)
-        k32_sweep<<<nblk(size), kBS32, 0, s>>>(L, v, inv_diag32, r, x, v == n - 1 ? z64 : nullptr);
+    auto sweep = [&](int v, double* z) -> int {
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
+        const ColorLaunch c = color_launch(L, v);
+        if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
+        else k32_sweep<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         HB_LAUNCHED();
-    }
-    for(int v = n - 2; v >= 0; --v)
-    {
-        const int size = L.offsets[v + 1] - L.offsets[v];
-        if(size <= 0) continue;
-        k32_sweep<<<nblk(size), kBS32, 0, s>>>(L, v, inv_diag32, r, x, z64);
-        HB_LAUNCHED();
-    }
+        return 0;
+    };
+    // colour n-1 is final after the forward sweep (the backward sweep starts at n-2)
+    for(int v = 0; v < n; ++v) HB_RETURN_IF(sweep(v, v == n - 1 ? z64 : nullptr));
+    for(int v = n - 2; v >= 0; --v) HB_RETURN_IF(sweep(v, z64));
     return 0;
 }
 
 int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* diag32,
                       const float* rf, const float* xf, float* rc, cudaStream_t s)
 {
-    k32_restrict<<<nblk(nc), kBS32, 0, s>>>(Lf, Lf.color_of_par[0], nc, inj_f, inj_c, diag32, rf, xf, rc);
+    const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
+    if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
+    else k32_restrict<false><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     HB_LAUNCHED();
     return 0;
 }
@@ -322,6 +534,49 @@ int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc
 {
     k32_prolong<<<nblk(nc), kBS32, 0, s>>>(nc, inj_f, inj_c, xc, xf);
     HB_LAUNCHED();
+    return 0;
+}
+
+size_t stencil_pap_partials(const StencilLevel& L)
+{
+    size_t n = 0;
+    for(int v = 0; v < L.ncolors; ++v)
+    {
+        const dim3 g = brick_grid(color_launch(L, v));
+        n += (size_t)g.x * g.y * g.z;
+    }
+    return n;
+}
+
+int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s)
+{
+    for(int v = 0; v < L.ncolors; ++v)
+    {
+        const ColorLaunch c = color_launch(L, v);
+        if(L.even) k64_spmv_color<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, diag, x, y);
+        else k64_spmv_color<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, diag, x, y);
+        HB_LAUNCHED();
+    }
+    return 0;
+}
+
+int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
+                                 CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
+{
+    const int total = (int)stencil_pap_partials(L);
+    int base = 0;
+    for(int v = 0; v < L.ncolors; ++v)
+    {
+        const ColorLaunch c = color_launch(L, v);
+        const dim3 g = brick_grid(c);
+        const int fin = v == L.ncolors - 1;
+        if(L.even)
+            k64_pap_color<true><<<g, dim3(32, 8), 0, s>>>(c, L, diag, p, Ap, st, partial, base, total, ticket, fin);
+        else
+            k64_pap_color<false><<<g, dim3(32, 8), 0, s>>>(c, L, diag, p, Ap, st, partial, base, total, ticket, fin);
+        HB_LAUNCHED();
+        base += (int)(g.x * g.y * g.z);
+    }
     return 0;
 }
 

@@ -1,4 +1,5 @@
-// FP32 V-cycle on the implicit 27-point stencil (mixed-precision path).
+// Implicit-stencil kernels: the FP32 V-cycle of the mixed-precision path and
+// the FP64 stencil SpMV of its outer CG.
 //
 // After the reference's JPL multicoloring of the HPCG grid every colour is
 // one parity class (ix&1, iy&1, iz&1) and, because the colour sort is
@@ -6,30 +7,43 @@
 // dense brick.  A row's neighbours are therefore computable from its
 // position, and their ELL slot order (ascending permuted column) is fixed per
 // colour: by neighbour colour, then by (dz,dy,dx).  The kernels walk that
-// order, so their float sums round exactly like an ELL sweep with float
-// values -- without reading any matrix data.  Off-diagonal values are the
-// stencil's -1 (verified on the device before this path is enabled); the
-// diagonal stays an explicit array because TestCG rescales it.
+// order, so their sums round exactly like an ELL sweep -- without reading any
+// matrix data.  Off-diagonal values are the stencil's -1 (verified on the
+// device before these paths are enabled); the diagonal stays an explicit
+// array because TestCG rescales it.
+//
+// When all grid dimensions are even every brick has the same shape and the
+// column offset of slot j of a colour-v row is a constant delta[v][j]; a
+// 6-bit mask per row (which faces of the grid it touches) decides which
+// neighbours exist.  Odd dimensions fall back to computing each neighbour's
+// brick coordinates.
 #pragma once
 
+#include "cg.cuh"
 #include "common.cuh"
 
 namespace hb {
 
 constexpr int kMaxStencilColors = 8;
 
+struct StencilTab
+{
+    int delta[27];             // col - row of slot j (even grids)
+    unsigned char bmask[27];   // boundary faces that remove slot j
+    unsigned short nb[27];     // (dx+1) | (dy+1)<<2 | (dz+1)<<4 | colour<<8 (all grids)
+    int dp;                    // slot of the diagonal
+};
+
 struct StencilLevel
 {
     int nx, ny, nz, m;
     int ncolors;
+    int even;                  // all dimensions even: deltas are constant
     int offsets[kMaxStencilColors + 1];
     int bx[kMaxStencilColors], by[kMaxStencilColors];
     int par[kMaxStencilColors];           // parity bits (ix&1)<<2 | (iy&1)<<1 | (iz&1) of colour v
     int color_of_par[8];
-    // Per colour: the 27 stencil offsets in ELL slot order, packed as
-    // (dx+1) | (dy+1)<<2 | (dz+1)<<4 | (neighbour colour)<<8.
-    unsigned short nb[kMaxStencilColors][27];
-    unsigned char diag_pos[kMaxStencilColors];
+    StencilTab tab[kMaxStencilColors];
 };
 
 // Builds the level description from the grid and the colour of each parity
@@ -59,5 +73,15 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
                       const float* rf, const float* xf, float* rc, cudaStream_t s);
 // xf[inj_f[i]] += xc[inj_c[i]].
 int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf, cudaStream_t s);
+
+// FP64 y = A x on the implicit stencil (bitwise equal to the ELL SpMV: same
+// slot order, fma(-1, x, s) == s - x, fma(a_ii, x_i, s) on the diagonal).
+int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s);
+// Same fused with p.Ap and alpha = rtz / pAp (the CG step of k_cg_spmv_pap);
+// one partial sum per block in `partial` (stencil_pap_partials(L) entries),
+// `ticket` must start at zero and is left at zero.
+size_t stencil_pap_partials(const StencilLevel& L);
+int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
+                                 CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
 
 }  // namespace hb

@@ -35,21 +35,50 @@ ColorChunks make_chunks(int m, int ncolors, const int* offsets)
     return cc;
 }
 
+// ------------------------------------------------------------ row kernel core
+
+// sum <- fma(s * a_p, x[col_p], sum) over the ELL slots p of `row` in slot
+// order, for the slots with use_slot(p) and columns with use_col(col).  The
+// slots are processed 9 at a time: the column/value loads of a group are
+// issued together (predicated), then its gathers, then its fmas, so a row
+// costs 2 dependent memory round trips per group instead of 2 per slot.
+template <typename SlotPred, typename ColPred>
+__device__ __forceinline__ double ell_row_sum(int m, int row, const int* __restrict__ ell_col,
+                                              const double* __restrict__ ell_val, const double* x, double sum,
+                                              double s, SlotPred use_slot, ColPred use_col)
+{
+    constexpr int G = 9;
+#pragma unroll
+    for(int g = 0; g < kWidth; g += G)
+    {
+        int col[G];
+        double v[G], xv[G];
+#pragma unroll
+        for(int q = 0; q < G; ++q)
+        {
+            const int p = g + q;
+            const size_t idx = (size_t)p * m + row;
+            const bool u = use_slot(p);
+            col[q] = u ? ld_stream(ell_col + idx) : -1;
+            v[q] = u ? ld_stream(ell_val + idx) : 0.0;
+        }
+#pragma unroll
+        for(int q = 0; q < G; ++q) xv[q] = use_col(col[q]) ? x[col[q]] : 0.0;
+#pragma unroll
+        for(int q = 0; q < G; ++q)
+            if(use_col(col[q])) sum = fma(s * v[q], xv[q], sum);
+    }
+    return sum;
+}
+
 // ---------------------------------------------------------------- SpMV
 
 __device__ __forceinline__ double spmv_row(int m, int row, const int* __restrict__ ell_col,
                                            const double* __restrict__ ell_val, const double* __restrict__ x)
 {
-    double sum = 0.0;
-#pragma unroll
-    for(int p = 0; p < kWidth; ++p)
-    {
-        const size_t idx = (size_t)p * m + row;
-        const int col = ld_stream(ell_col + idx);
-        const double v = ld_stream(ell_val + idx);
-        if(col >= 0 && col < m) sum = fma(v, __ldg(x + col), sum);
-    }
-    return sum;
+    return ell_row_sum(
+        m, row, ell_col, ell_val, x, 0.0, 1.0, [](int) { return true; },
+        [m](int col) { return col >= 0 && col < m; });
 }
 
 // src/ComputeSPMV.cpp:130-170.  Blocks are interleaved over colours (block b
@@ -75,15 +104,9 @@ __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset
     const int gid = blockIdx.x * kBS + threadIdx.x;
     if(gid >= size) return;
     const int row = gid + offset;
-    double sum = r[row];
-#pragma unroll
-    for(int p = 0; p < kWidth; ++p)
-    {
-        const size_t idx = (size_t)p * m + row;
-        const int col = ld_stream(ell_col + idx);
-        const double v = ld_stream(ell_val + idx);
-        if(col >= 0 && col < m && col != row) sum = fma(-v, x[col], sum);
-    }
+    const double sum = ell_row_sum(
+        m, row, ell_col, ell_val, x, r[row], -1.0, [](int) { return true; },
+        [m, row](int col) { return col >= 0 && col < m && col != row; });
     x[row] = sum * inv_diag[row];
 }
 
@@ -104,13 +127,9 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
     if(offset > 0)
     {
         const int diag = diag_idx[row];
-        for(int p = 0; p < diag; ++p)
-        {
-            const size_t idx = (size_t)p * m + row;
-            const int col = ld_stream(ell_col + idx);
-            const double v = ld_stream(ell_val + idx);
-            if(col >= 0 && col < offset) sum = fma(-v, x[col], sum);
-        }
+        sum = ell_row_sum(
+            m, row, ell_col, ell_val, x, sum, -1.0, [diag](int p) { return p < diag; },
+            [offset](int col) { return col >= 0 && col < offset; });
     }
     x[row] = sum * inv_diag[row];
 }
@@ -125,14 +144,9 @@ __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset,
     if(gid >= size) return;
     const int row = gid + offset;
     const int d = diag_idx[row];
-    double sum = __dmul_rn(x[row], diag[row]);
-    for(int p = d + 1; p < kWidth; ++p)
-    {
-        const size_t idx = (size_t)p * m + row;
-        const int col = ld_stream(ell_col + idx);
-        const double v = ld_stream(ell_val + idx);
-        if(col >= offset && col < m) sum = fma(-v, x[col], sum);
-    }
+    const double sum = ell_row_sum(
+        m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, [d](int p) { return p > d; },
+        [offset, m](int col) { return col >= offset && col < m; });
     x[row] = sum * inv_diag[row];
 }
 
@@ -147,15 +161,9 @@ __global__ void __launch_bounds__(kBS) k_restrict(int nc, const int* __restrict_
     const int ic = blockIdx.x * kBS + threadIdx.x;
     if(ic >= nc) return;
     const int row = inj_f[ic];
-    double sum = rf[row];
-#pragma unroll
-    for(int p = 0; p < kWidth; ++p)
-    {
-        const size_t idx = (size_t)p * mf + row;
-        const int col = ld_stream(ell_col + idx);
-        const double v = ld_stream(ell_val + idx);
-        if(col >= 0 && col < mf) sum = fma(-v, __ldg(xf + col), sum);
-    }
+    const double sum = ell_row_sum(
+        mf, row, ell_col, ell_val, xf, rf[row], -1.0, [](int) { return true; },
+        [mf](int col) { return col >= 0 && col < mf; });
     rc[inj_c[ic]] = sum;
 }
 

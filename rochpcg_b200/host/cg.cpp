@@ -53,8 +53,19 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     }
     HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
     HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
-    HB_RETURN_IF(hb::launch_cg_spmv_pap(n, opt(A)->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, st,
-                                        rt().ws, s));
+    if(prec == MGPrecision::FP32)
+    {
+        // mixed path: the FP64 operator on the implicit stencil (bitwise equal to the ELL product)
+        const LevelOpt* o = opt(A);
+        HB_RETURN_IF(hb::launch64_cg_spmv_pap_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, st,
+                                                      o->pap_partial, o->pap_ticket, s));
+    }
+    else
+    {
+        const LevelOpt* o = opt(A);
+        HB_RETURN_IF(hb::launch_cg_spmv_pap(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, st,
+                                            o->spmv_partial, o->spmv_ticket, s));
+    }
     HB_RETURN_IF(hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
                                          data.z.d_values, st, rt().ws, cond, s));
     return 0;
@@ -150,6 +161,14 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
     return o->graphs.back().get();
 }
 
+int iteration_kernels(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, bool precond,
+                      MGPrecision prec, bool flexible)
+{
+    LevelOpt* o = opt(A);
+    ensure_state(o, 1);
+    return get_graph(A, data, b, x, precond, prec, flexible)->kernels_per_iteration;
+}
+
 // HPCGB200_GRAPH=0 runs the iteration body as direct launches with a host
 // check per iteration (for profilers that cannot look inside graphs with
 // conditional nodes); the kernels and their order are the same.
@@ -183,12 +202,25 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaEventCreate(&e1));
         HB_HOST_CUDA(cudaEventRecord(e0, s));
         HB_HOST_CUDA(cudaMemcpyAsync(st, &h, offsetof(hb::CGState, hist), cudaMemcpyHostToDevice, s));
-        // a fresh reduction ticket for every solve
+        // fresh reduction tickets for every solve
         HB_HOST_CUDA(cudaMemsetAsync(&rt().ws->ticket, 0, sizeof(unsigned int), s));
+        if(o->pap_ticket) HB_HOST_CUDA(cudaMemsetAsync(o->pap_ticket, 0, sizeof(unsigned int), s));
+        HB_HOST_CUDA(cudaMemsetAsync(o->spmv_ticket, 0, sizeof(unsigned int), s));
 
         // preamble: p = x; Ap = A p; r = b - Ap; normr = ||r||
         HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        check(hb::launch_spmv(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, s));
+        if(prec == MGPrecision::FP32)
+        {
+            for(const SparseMatrix* M = &A; M; M = M->Ac)
+                if(!opt(*M) || !opt(*M)->stencil_ok)
+                    return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
+                                            "mixed CG needs the 27-point stencil in parity colouring on every level");
+            check(hb::launch64_spmv_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, s));
+        }
+        else
+        {
+            check(hb::launch_spmv(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, s));
+        }
         check(hb::launch_cg_residual0(n, b.d_values, data.Ap.d_values, data.r.d_values, st, rt().ws, s));
         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
         HB_HOST_CUDA(cudaStreamSynchronize(s));

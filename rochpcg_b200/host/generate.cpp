@@ -159,6 +159,10 @@ static void delete_level_opt(SparseMatrix& A)
     dfree(o->inv_diag32);
     dfree(o->cg_state);
     dfree(o->r32);
+    dfree(o->pap_partial);
+    dfree(o->pap_ticket);
+    dfree(o->spmv_partial);
+    dfree(o->spmv_ticket);
     dfree(o->z32);
     dfree(o->vec_scratch);
     for(auto& g : o->graphs)

@@ -86,6 +86,10 @@ struct LevelOpt
     hb::CGState* cg_state = nullptr;
     int cg_state_iters = 0;
     std::vector<std::unique_ptr<CGGraph>> graphs;
+    double* pap_partial = nullptr;     // per-block partial sums of the stencil SpMV + p.Ap (level 0)
+    unsigned int* pap_ticket = nullptr;
+    double* spmv_partial = nullptr;    // per-block partial sums of the ELL SpMV + p.Ap (level 0)
+    unsigned int* spmv_ticket = nullptr;
     float* r32 = nullptr;              // FP32 right-hand side of the V-cycle (level 0)
     float* z32 = nullptr;              // FP32 V-cycle result (level 0)
     double* vec_scratch = nullptr;     // one FP64 vector of length m (TestCG / TestSymmetry)
@@ -105,6 +109,11 @@ inline MGOpt* mgopt(const SparseMatrix& A) { return A.mgData ? static_cast<MGOpt
 
 // Operators on raw FP32 level data (mixed V-cycle), defined in operators.cpp.
 int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s);
+
+// Kernel launches of one CG iteration (captures the iteration graph if it
+// does not exist yet; nothing is launched), defined in cg.cpp.
+int iteration_kernels(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, bool precond,
+                      MGPrecision prec, bool flexible);
 
 // Graph-cached solve, defined in cg.cpp.
 int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,

@@ -147,8 +147,14 @@ int OptimizeProblem(SparseMatrix& A, CGData& data, Vector& b, Vector& x, Vector&
         {
             o->r32 = dalloc<float>(m);
             o->z32 = dalloc<float>(m);
+            o->pap_partial = dalloc<double>(hb::stencil_pap_partials(o->st));
+            o->pap_ticket = dalloc<unsigned int>(1);
+            HB_HOST_CUDA(cudaMemsetAsync(o->pap_ticket, 0, sizeof(unsigned int), s));
         }
         o->vec_scratch = dalloc<double>(m);
+        o->spmv_partial = dalloc<double>(o->cc.nchunks());
+        o->spmv_ticket = dalloc<unsigned int>(1);
+        HB_HOST_CUDA(cudaMemsetAsync(o->spmv_ticket, 0, sizeof(unsigned int), s));
 
         if(!data.r.d_values) CudaInitializeSparseCGData(A, data);
         for(SparseMatrix* M = &A; M; M = M->Ac) free_generated(*M);

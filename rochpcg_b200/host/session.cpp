@@ -30,6 +30,8 @@ struct hpcgb200_problem
 
 namespace {
 
+MGPrecision prec_of(int mode) { return mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32 : MGPrecision::FP64; }
+
 template <typename F>
 int guarded(F&& f)
 {
@@ -303,7 +305,6 @@ extern "C" int hpcgb200_problem_get_x(hpcgb200_problem* p, double* host_x_natura
     });
 }
 
-static MGPrecision prec_of(int mode) { return mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32 : MGPrecision::FP64; }
 
 extern "C" int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, double tol, int precond, int* niters,
                                    double* normr, double* normr0, double* normr_hist, double* seconds)
@@ -365,14 +366,8 @@ extern "C" int hpcgb200_problem_kernels_per_iteration(hpcgb200_problem* p, int m
 {
     if(!p || !kernels) return hb::record_error(HPCGB200_ERR_ARG, "null argument");
     return guarded([&] {
-        const LevelOpt* o = opt(p->A);
-        for(const auto& g : o->graphs)
-        {
-            if(g->mode != (mode == HPCGB200_MODE_MIXED ? 1 : 0) || g->precond != (precond != 0)) continue;
-            *kernels = g->kernels_per_iteration;
-            return 0;
-        }
-        return hb::record_error(HPCGB200_ERR_ARG, "no solve of this mode has run yet");
+        *kernels = iteration_kernels(p->A, p->data, p->b, p->x, precond != 0, prec_of(mode), mode != HPCGB200_MODE_FP64);
+        return 0;
     });
 }
 
@@ -415,6 +410,17 @@ extern "C" int hpcgb200_problem_spmv(hpcgb200_problem* p, int level, const doubl
     if(!M || !x || !y) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     Vector xv = wrap(x, M->localNumberOfRows), yv = wrap(y, M->localNumberOfRows);
     return ComputeSPMV(*M, xv, yv);
+}
+
+extern "C" int hpcgb200_problem_spmv_stencil(hpcgb200_problem* p, int level, const double* x, double* y)
+{
+    SparseMatrix* M = level_of(p, level);
+    if(!M || !x || !y) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
+    return guarded([&] {
+        const LevelOpt* o = opt(*M);
+        if(!o->stencil_ok) return hb::record_error(HPCGB200_ERR_NOT_STENCIL, "level %d is not the verified stencil", level);
+        return hb::launch64_spmv_stencil(o->st, o->diag, x, y, rt().stream);
+    });
 }
 
 extern "C" int hpcgb200_problem_symgs(hpcgb200_problem* p, int level, const double* r, double* x)
@@ -482,6 +488,18 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
         else if(o == "symgs_zero") f = [&] { return ComputeSYMGSZeroGuess(A, r, z); };
         else if(o == "mg") f = [&] { return ComputeMG(A, r, z); };
         else if(o == "mg_mixed") f = [&] { return ComputeMG_Mixed(A, r, z); };
+        else if(o == "symgs32_sweep" || o == "spmv_stencil")
+        {
+            const LevelOpt* lo = opt(A);
+            if(!lo->stencil_ok) return hb::record_error(HPCGB200_ERR_NOT_STENCIL, "level 0 is not the verified stencil");
+            if(o == "spmv_stencil") f = [&, lo] { return hb::launch64_spmv_stencil(lo->st, lo->diag, p->data.p.d_values, p->data.Ap.d_values, s); };
+            else
+            {
+                // one FP32 SymGS step on level 0 (15 colour launches), averaged per launch
+                f = [&, lo] { return hb::launch32_symgs(lo->st, lo->inv_diag32, lo->r32, lo->z32, nullptr, s); };
+                per_call = 15;
+            }
+        }
         else return hb::record_error(HPCGB200_ERR_ARG, "unknown op '%s'", op);
         HB_RETURN_IF(f());  // warm-up
         cudaEvent_t e0, e1;

@@ -56,3 +56,21 @@ def test_mixed_test_symmetry_and_test_cg():
     assert s["depsym_mg"] / FLT_OVER_DBL <= 1.0
     t = P.test_cg(mode=R.MODE_MIXED)
     assert t["count_fail"] == 0, t
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32)])
+def test_stencil_spmv_equals_ell_spmv_bitwise(dims):
+    """The mixed path's implicit FP64 operator is the ELL operator, bit for bit."""
+    P, O = problems(*dims)
+    for l in range(4):
+        m = O.levels[l].m
+        x = np.random.default_rng(40 + l).uniform(-1, 1, m)
+        xd = to_dev(x)
+        y1 = torch.empty(m, dtype=torch.float64, device="cuda")
+        y2 = torch.empty_like(y1)
+        torch.cuda.synchronize()
+        P.spmv(l, xd.data_ptr(), y1.data_ptr())
+        P.spmv_stencil(l, xd.data_ptr(), y2.data_ptr())
+        sync(P)
+        assert torch.equal(y1, y2)
+        assert np.array_equal(host(y2), O.levels[l].spmv(x))
