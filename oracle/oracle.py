@@ -214,6 +214,14 @@ def colored_lib():
         L.oc_mg_f32.argtypes = [vp, ctypes.c_int, vp, vp]
         L.oc_cg.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                             _c_int_p, _c_dbl_p, _c_dbl_p, vp]
+        L.oc_bf16.argtypes = [ctypes.c_float]
+        L.oc_bf16.restype = ctypes.c_float
+        L.oc_conv16.argtypes = [ctypes.c_int] * 3 + [vp, vp, vp, ctypes.c_int]
+        L.oc_flip_transpose.argtypes = [vp, vp]
+        L.oc_conv16_wgrad.argtypes = [ctypes.c_int] * 3 + [vp, vp, vp, ctypes.c_int]
+        L.oc_net_forward.argtypes = [ctypes.c_int] * 3 + [vp] * 7 + [ctypes.c_int]
+        L.oc_net_loss_grad.argtypes = [ctypes.c_int] * 3 + [vp] * 8 + [ctypes.c_int]
+        L.oc_net_loss_grad.restype = ctypes.c_double
         _oc_lib = L
     return _oc_lib
 
@@ -356,3 +364,62 @@ class ColoredProblem:
         colored_lib().oc_cg(ctypes.cast(self._struct, ctypes.c_void_p), self.nlevels, _ptr(b), _ptr(x), max_iter, tol,
                             int(precond), ctypes.byref(it), ctypes.byref(nr), ctypes.byref(nr0), _ptr(hist))
         return dict(x=x, niters=it.value, normr=nr.value, normr0=nr0.value, hist=hist[: it.value + 1])
+
+
+# --------------------------------------------------------------------------
+# learned smoother (conv net) restatement
+
+
+def bf16(a: np.ndarray) -> np.ndarray:
+    """fp32 -> bf16 (round to nearest even) -> fp32, vectorised like oc_bf16."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def conv16(dims, x, w, round_=True):
+    nz, ny, nx = dims
+    x = np.ascontiguousarray(x, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.empty_like(x)
+    colored_lib().oc_conv16(nz, ny, nx, _ptr(x), _ptr(w), _ptr(out), int(round_))
+    return out
+
+
+def flip_transpose(w):
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.empty_like(w)
+    colored_lib().oc_flip_transpose(_ptr(w), _ptr(out))
+    return out
+
+
+def conv16_wgrad(dims, x, g, round_=True):
+    nz, ny, nx = dims
+    x = np.ascontiguousarray(x, np.float32)
+    g = np.ascontiguousarray(g, np.float32)
+    dw = np.empty(27 * 16 * 16, np.float32)
+    colored_lib().oc_conv16_wgrad(nz, ny, nx, _ptr(x), _ptr(g), _ptr(dw), int(round_))
+    return dw
+
+
+def net_forward(dims, w1, w2, w3, r, round_=True):
+    nz, ny, nx = dims
+    n = nz * ny * nx
+    r = np.ascontiguousarray(r, np.float32)
+    ws = [np.ascontiguousarray(w, np.float32) for w in (w1, w2, w3)]
+    y = np.empty(n, np.float32)
+    a1 = np.empty(n * 16, np.float32)
+    a2 = np.empty(n * 16, np.float32)
+    colored_lib().oc_net_forward(nz, ny, nx, *[_ptr(w) for w in ws], _ptr(r), _ptr(y), _ptr(a1), _ptr(a2), int(round_))
+    return y, a1, a2
+
+
+def net_loss_grad(dims, w1, w2, w3, r, e, round_=True):
+    nz, ny, nx = dims
+    r = np.ascontiguousarray(r, np.float32)
+    e = np.ascontiguousarray(e, np.float32)
+    ws = [np.ascontiguousarray(w, np.float32) for w in (w1, w2, w3)]
+    d = [np.empty(27 * 256, np.float32) for _ in range(3)]
+    loss = colored_lib().oc_net_loss_grad(nz, ny, nx, *[_ptr(w) for w in ws], _ptr(r), _ptr(e),
+                                          *[_ptr(x) for x in d], int(round_))
+    return loss, d
