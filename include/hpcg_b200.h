@@ -173,6 +173,34 @@ int hpcgb200_waxpby_dot(int n, double alpha, const double* x, double* y, double*
 int hpcgb200_residual_inf(int n, const double* v1, const double* v2, double* result, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------ learned smoother kernels
+ * No reference counterpart: the conv-net smoother that replaces SymGS on the
+ * coarse MG levels (a 3-layer 3x3x3 network, 1 -> 16 -> 16 -> 1 channels,
+ * ReLU, BF16 weights and activations, FP32 accumulation).  Tensors are
+ * channel-last BF16 [nb][nz][ny][nx][16] (16-byte aligned DEVICE memory);
+ * weights w[tap][ci][co] FP32 with tap = (dz+1)*9 + (dy+1)*3 + (dx+1); zero
+ * padding outside each sample's grid.  *status (device int) is set non-zero
+ * if a tensor-core wait timed out (the launch then returns early). */
+
+/* Bytes of one layer's prepared BF16 operand tiles (27 x 16 x 16 x 2). */
+size_t hpcgb200_conv_weight_tile_bytes(void);
+/* w (device, 6912 FP32) -> wB (device, tile bytes); flip != 0 prepares the
+ * transposed convolution's weights (mirrored taps, swapped channels). */
+int hpcgb200_conv_prepare_weights(const float* w, void* wB, int flip, void* stream);
+#define HPCGB200_CONV_RELU_BF16 0  /* out = bf16(relu(conv)), 16 channels */
+#define HPCGB200_CONV_MASK_BF16 1  /* out = bf16(act > 0 ? conv : 0), 16 channels */
+#define HPCGB200_CONV_F32 2        /* out = conv, FP32 16 channels */
+#define HPCGB200_CONV_F32_C0 3     /* out = channel 0 of conv, FP32 [nb][nz][ny][nx] */
+/* out = conv(in, W) on tcgen05 tensor cores; act is read by the masked mode. */
+int hpcgb200_conv16(int nb, int nz, int ny, int nx, const void* in, const void* wB, int out_mode, void* out,
+                    const void* act, int* status, void* stream);
+/* Workspace of hpcgb200_conv16_wgrad (per-CTA partial sums). */
+size_t hpcgb200_conv_wgrad_partial_bytes(int nb, int nz, int ny, int nx);
+/* dw[tap][ci][co] (device, 6912 FP32) = sum_p x[p + tap][ci] * g[p][co]
+ * (deterministic: fixed partition, fixed-order reduction). */
+int hpcgb200_conv16_wgrad(int nb, int nz, int ny, int nx, const void* x, const void* g, float* partial, float* dw,
+                          int* status, void* stream);
+
 /* ------------------------------------------------------ problem handle
  * A handle owns the device hierarchy built exactly as src/main.cpp:198-210 +
  * src/OptimizeProblem.cpp:69-160 do (GenerateProblem, SetupHalo,

@@ -41,6 +41,11 @@ SIGNATURES = {
     "hpcgb200_waxpby": (_i, [_i, _d, _vp, _d, _vp, _vp, _vp]),
     "hpcgb200_waxpby_dot": (_i, [_i, _d, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hpcgb200_residual_inf": (_i, [_i, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "hpcgb200_conv_weight_tile_bytes": (_sz, []),
+    "hpcgb200_conv_prepare_weights": (_i, [_vp, _vp, _i, _vp]),
+    "hpcgb200_conv16": (_i, [_i, _i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
+    "hpcgb200_conv_wgrad_partial_bytes": (_sz, [_i, _i, _i, _i]),
+    "hpcgb200_conv16_wgrad": (_i, [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_problem_create": (_i, [_i, _i, _i, _i, _vp]),
     "hpcgb200_problem_create_ex": (_i, [_i, _i, _i, _i, _i, _vp]),
     "hpcgb200_problem_destroy": (_i, [_vp]),

@@ -1,0 +1,718 @@
+// Learned smoother kernels on the 5th-generation tensor cores (tcgen05).  No
+// reference counterpart: the conv-net smoother is new in this library.
+//
+// Forward / input-gradient convolution (k_conv16).  Every layer runs as a
+// 16 -> 16 channel 3x3x3 convolution (layer 1 has one real input channel and
+// layer 3 one real output channel, the other weights are zero), so one kernel
+// serves the forward pass and the input gradient (the transposed convolution
+// is a convolution with mirrored taps and swapped channels).  A CTA owns a
+// brick of 16 x 8 x 2 points = two 128-row M tiles (one per z plane) and
+// stages the brick's halo once, as three copies shifted by dx = -1, 0, +1.
+// Each copy keeps one 16-byte row (8 BF16 channels) per point, the two
+// channel halves in separate regions, so in the no-swizzle K-major operand
+// layout every 8-row core matrix is contiguous and consecutive rows are 16
+// bytes apart.  A tap (dz, dy, dx) is then only a start-address offset into
+// copy dx: 27 taps x 2 tiles = 54 tcgen05.mma (M=128, N=16, K=16) accumulate
+// the brick's outputs in 32 TMEM columns, read back with tcgen05.ld.
+//
+// Weight gradient (k_conv16_wgrad).  dW[tap][ci][co] = sum_p x[p+tap][ci] *
+// g[p][co] is a GEMM over points: M = (8 taps x 16 input channels), N = 16
+// output channels, K = points.  Both operands are MN-major (8 channels = one
+// 16-byte core-matrix row), staged per block of 64 points; four M tiles (taps
+// 0-7, 8-15, 16-23, 24-26 + padding) accumulate in 64 TMEM columns.  Per-CTA
+// partial sums are reduced in a fixed order, so the gradient is deterministic.
+//
+// Operand layouts are the canonical no-swizzle ("interleaved") forms, in
+// 16-byte units: K-major ((8,m),2):((1,SBO),LBO); MN-major
+// ((1,m),(8,k)):((.,SBO),(1,LBO)).
+//
+// Waits.  The only waits are on an mbarrier completed by tcgen05.commit; each
+// is bounded.  On timeout the CTA records an error in *status, waits once more
+// (bounded) for its MMAs, leaves its loop as a whole block and still frees its
+// TMEM, so the context stays usable.
+#include <cuda_bf16.h>
+
+#include <cmath>
+
+#include "learned.cuh"
+
+namespace hb {
+
+namespace tc {
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, no swizzle (layout type 0), sm_100 version.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: BF16 x BF16 -> FP32, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N, bool a_mn_major, bool b_mn_major)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Bounded wait for the completion of phase `parity`; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(mbar);
+    for(uint32_t i = 0; i < kSpinLimit; ++i)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if(done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* holder, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(holder)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (32x32b shape: warp
+// w of a warpgroup reads lanes 32(w%4) .. 32(w%4)+31).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for(int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace tc
+
+using namespace tc;
+
+PermMap make_perm_map(const StencilLevel& L)
+{
+    PermMap pm{};
+    for(int v = 0; v <= 8; ++v) pm.offsets[v] = L.offsets[v];
+    for(int v = 0; v < 8; ++v)
+    {
+        pm.bx[v] = L.bx[v];
+        pm.by[v] = L.by[v];
+        pm.color_of_par[v] = L.color_of_par[v];
+    }
+    return pm;
+}
+
+__device__ __forceinline__ int perm_row(const PermMap& pm, int z, int y, int x)
+{
+    const int v = pm.color_of_par[((x & 1) << 2) | ((y & 1) << 1) | (z & 1)];
+    return pm.offsets[v] + ((z >> 1) * pm.by[v] + (y >> 1)) * pm.bx[v] + (x >> 1);
+}
+
+__device__ __forceinline__ uint4 pack_bf16x8(const float* v)
+{
+    __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+    for(int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    return *reinterpret_cast<uint4*>(h);
+}
+
+// K-major no-swizzle offset (bytes) of row r, 8-element K chunk c, for
+// 16-column (K = 16) operands with SBO = 256 B, LBO = 128 B.
+__host__ __device__ constexpr uint32_t kmajor_off(int r, int c) { return (uint32_t)((r >> 3) * 256 + c * 128 + (r & 7) * 16); }
+
+// ------------------------------------------------------------ forward conv
+
+constexpr int kTX = 16, kTY = 8, kTZ = 2;
+constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2;
+constexpr int kCopyRows = kTX * kHY * kHZ;            // 640 rows per shifted copy
+constexpr int kRegion = kCopyRows * 16;               // one 8-channel half: 10240 B (the K-major LBO)
+constexpr int kCopyBytes = 2 * kRegion;
+constexpr int kStageBytes = 3 * kCopyBytes;           // 61440 B
+constexpr int kHaloItems = 2 * kHX * kHY * kHZ;       // 16-byte loads per brick: 1440
+constexpr int kConvThreads = 256;
+constexpr int kConvSmem = kStageBytes + kNetWeightTileBytes + 64 + 128;
+
+static_assert((kRegion >> 4) < (1 << 14), "LBO field");
+static_assert(kTX * kTY == 128, "one z plane of the brick is one 128-row M tile");
+
+template <int kOut>
+__global__ void __launch_bounds__(kConvThreads, 2)
+    k_conv16(ConvGrid g, const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wB, void* out,
+             const __nv_bfloat16* __restrict__ act, PermMap pm, int* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    unsigned char* sA = smem;
+    unsigned char* sW = smem + kStageBytes;
+    uint64_t* mbar = (uint64_t*)(sW + kNetWeightTileBytes);
+    uint32_t* tholder = (uint32_t*)(mbar + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY, tz = (g.nz + kTZ - 1) / kTZ;
+    const long per_sample = (long)tx * ty * tz;
+    const long ntiles = per_sample * g.nb;
+
+    for(int i = tid; i < kNetWeightTileBytes / 16; i += kConvThreads)
+        reinterpret_cast<uint4*>(sW)[i] = reinterpret_cast<const uint4*>(wB)[i];
+    if(tid == 0) mbar_init(mbar, 1);
+    if(warp == 0) tmem_alloc(tholder, 32);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tholder;
+    constexpr uint32_t idesc = umma_idesc_bf16(128, 16, false, false);
+    uint32_t phase = 0;
+
+    for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    {
+        const int b = (int)(tile / per_sample);
+        long t2 = tile - (long)b * per_sample;
+        const int bz = (int)(t2 / ((long)tx * ty));
+        t2 -= (long)bz * tx * ty;
+        const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
+        const int x0 = bx * kTX, y0 = by * kTY, z0 = bz * kTZ;
+        const __nv_bfloat16* inb = in + (long)b * g.nz * g.ny * g.nx * kNetCh;
+
+        // halo brick -> three dx-shifted copies (half-channel regions)
+        for(int it = tid; it < kHaloItems; it += kConvThreads)
+        {
+            const int c8 = it / (kHX * kHY * kHZ);
+            const int q = it - c8 * (kHX * kHY * kHZ);
+            const int jx = q % kHX, rest = q / kHX;
+            const int ly = rest % kHY, lz = rest / kHY;
+            const int x = x0 + jx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)
+                v = __ldg(reinterpret_cast<const uint4*>(inb + (((long)z * g.ny + y) * g.nx + x) * kNetCh) + c8);
+            const int rowbase = (lz * kHY + ly) * kTX;
+#pragma unroll
+            for(int dxi = 0; dxi < 3; ++dxi)
+            {
+                const int lx = jx - dxi;  // copy dx = dxi-1 holds point x0 + lx + dx at lx
+                if(lx >= 0 && lx < kTX)
+                    *reinterpret_cast<uint4*>(sA + dxi * kCopyBytes + c8 * kRegion + (rowbase + lx) * 16) = v;
+            }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if(tid == 0)
+        {
+            const uint32_t a0 = smem_u32(sA), w0 = smem_u32(sW);
+#pragma unroll 1
+            for(int t = 0; t < 27; ++t)
+            {
+                const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                const uint64_t bd = umma_desc(w0 + t * 512, 128, 256);
+#pragma unroll
+                for(int mt = 0; mt < kTZ; ++mt)
+                {
+                    const int row0 = ((mt + dz + 1) * kHY + (dy + 1)) * kTX;
+                    const uint64_t ad = umma_desc(a0 + (dx + 1) * kCopyBytes + row0 * 16, kRegion, 128);
+                    mma_bf16(tmem + mt * 16, ad, bd, idesc, t > 0 ? 1u : 0u);
+                }
+            }
+            mma_commit(mbar);
+        }
+        __syncwarp();
+        const bool done = mbar_wait(mbar, phase);
+        const bool ok = __syncthreads_and(done) != 0;
+        if(!ok)
+        {
+            if(tid == 0) atomicExch(status, 1);
+            if(!done) mbar_wait(mbar, phase);  // one more bounded chance for the MMAs in flight
+            break;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+
+        const int qd = warp & 3, mt = warp >> 2;
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(mt * 16), v);
+        const int m = qd * 32 + lane;
+        const int x = x0 + (m & 15), y = y0 + (m >> 4), z = z0 + mt;
+        if(x < g.nx && y < g.ny && z < g.nz)
+        {
+            const long p = (((long)b * g.nz + z) * g.ny + y) * g.nx + x;
+            if constexpr(kOut == kOutReluBf16 || kOut == kOutMaskBf16)
+            {
+                if constexpr(kOut == kOutReluBf16)
+                {
+#pragma unroll
+                    for(int c = 0; c < 16; ++c) v[c] = v[c] > 0.f ? v[c] : 0.f;
+                }
+                else
+                {
+                    const uint4* ap = reinterpret_cast<const uint4*>(act + p * kNetCh);
+                    __align__(16) __nv_bfloat16 h[16];
+                    *reinterpret_cast<uint4*>(h) = ap[0];
+                    *reinterpret_cast<uint4*>(h + 8) = ap[1];
+#pragma unroll
+                    for(int c = 0; c < 16; ++c) v[c] = __bfloat162float(h[c]) > 0.f ? v[c] : 0.f;
+                }
+                uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(out) + p * kNetCh);
+                dst[0] = pack_bf16x8(v);
+                dst[1] = pack_bf16x8(v + 8);
+            }
+            else if constexpr(kOut == kOutF32)
+            {
+                float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + p * kNetCh);
+#pragma unroll
+                for(int c = 0; c < 4; ++c) dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+            }
+            else if constexpr(kOut == kOutF32C0)
+            {
+                reinterpret_cast<float*>(out)[p] = v[0];
+            }
+            else
+            {
+                float* xo = reinterpret_cast<float*>(out) + perm_row(pm, z, y, x);
+                if constexpr(kOut == kOutPermSet) *xo = v[0];
+                else *xo += v[0];
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM read and staging consumed before the next brick
+        tc_fence_after();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if(warp == 0) tmem_free(tmem, 32);
+}
+
+// ------------------------------------------------------------ weight gradient
+
+constexpr int kWgK = 64;                  // points per K block
+constexpr int kWgATile = 128 * kWgK * 2;  // 16 KB per M tile (8 taps x 16 channels)
+constexpr int kWgB = 16 * kWgK * 2;       // 2 KB
+constexpr int kWgThreads = 128;
+constexpr int kWgSmem = 4 * kWgATile + kWgB + 64 + 128;
+
+// MN-major no-swizzle offsets (bytes) of 8-element M chunk j, K index k.
+//   A: SBO (chunk stride) 128 B, LBO (8-k group stride) 16 chunks x 128 B = 2048 B
+//   B: SBO 128 B, LBO 2 chunks x 128 B = 256 B
+__device__ __forceinline__ uint32_t mn_off_a(int j, int k) { return (uint32_t)(j * 128 + (k & 7) * 16 + (k >> 3) * 2048); }
+__device__ __forceinline__ uint32_t mn_off_b(int j, int k) { return (uint32_t)(j * 128 + (k & 7) * 16 + (k >> 3) * 256); }
+
+__global__ void __launch_bounds__(kWgThreads) k_conv16_wgrad(ConvGrid g, const __nv_bfloat16* __restrict__ x,
+                                                             const __nv_bfloat16* __restrict__ gr,
+                                                             float* __restrict__ partial, int* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + 4 * kWgATile;
+    uint64_t* mbar = (uint64_t*)(sB + kWgB);
+    uint32_t* tholder = (uint32_t*)(mbar + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long n = per * g.nb;
+    const long nblk = (n + kWgK - 1) / kWgK;
+
+    if(tid == 0) mbar_init(mbar, 1);
+    if(warp == 0) tmem_alloc(tholder, 64);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tholder;
+    constexpr uint32_t idesc = umma_idesc_bf16(128, 16, true, true);
+    uint32_t phase = 0;
+    bool first = true, ok = true;
+
+    for(long blk = blockIdx.x; blk < nblk; blk += gridDim.x)
+    {
+        for(int i = tid; i < kWgK * 2; i += kWgThreads)
+        {
+            const int k = i >> 1, c8 = i & 1;
+            const long p = blk * kWgK + k;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if(p < n) v = __ldg(reinterpret_cast<const uint4*>(gr + p * kNetCh) + c8);
+            *reinterpret_cast<uint4*>(sB + mn_off_b(c8, k)) = v;
+        }
+        for(int i = tid; i < kWgK * 32 * 2; i += kWgThreads)
+        {
+            // i -> (k, tap slot 0..31, c8); tap slots >= 27 are zero padding
+            const int c8 = i & 1;
+            const int ts = (i >> 1) & 31;
+            const int k = i >> 6;
+            const long p = blk * kWgK + k;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if(ts < 27 && p < n)
+            {
+                const long b = p / per;
+                const long rem = p - b * per;
+                const int z = (int)(rem / ((long)g.ny * g.nx));
+                const long r2 = rem - (long)z * g.ny * g.nx;
+                const int y = (int)(r2 / g.nx);
+                const int xx = (int)(r2 - (long)y * g.nx);
+                const int zz = z + ts / 9 - 1, yy = y + (ts / 3) % 3 - 1, x2 = xx + ts % 3 - 1;
+                if(zz >= 0 && zz < g.nz && yy >= 0 && yy < g.ny && x2 >= 0 && x2 < g.nx)
+                    v = __ldg(reinterpret_cast<const uint4*>(
+                                  x + (((b * g.nz + zz) * g.ny + yy) * g.nx + x2) * kNetCh) +
+                              c8);
+            }
+            const int mt = ts >> 3;
+            const int j = (ts & 7) * 2 + c8;
+            *reinterpret_cast<uint4*>(sA + mt * kWgATile + mn_off_a(j, k)) = v;
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if(tid == 0)
+        {
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+            for(int s = 0; s < kWgK / 16; ++s)
+            {
+                const uint64_t bd = umma_desc(b0 + s * 2 * 256, 256, 128);
+#pragma unroll
+                for(int mt = 0; mt < 4; ++mt)
+                {
+                    const uint64_t ad = umma_desc(a0 + mt * kWgATile + s * 2 * 2048, 2048, 128);
+                    mma_bf16(tmem + (uint32_t)(mt * 16), ad, bd, idesc, (first && s == 0) ? 0u : 1u);
+                }
+            }
+            mma_commit(mbar);
+        }
+        first = false;
+        __syncwarp();
+        const bool done = mbar_wait(mbar, phase);
+        ok = __syncthreads_and(done) != 0;
+        if(!ok)
+        {
+            if(tid == 0) atomicExch(status, 2);
+            if(!done) mbar_wait(mbar, phase);
+            break;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();  // staging consumed before it is rewritten
+    }
+    tc_fence_after();
+    // row m of M tile mt = TMEM lane m: tap mt*8 + m/16, input channel m%16
+    for(int mt = 0; mt < 4; ++mt)
+    {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * 16), v);
+        const int tap = mt * 8 + (tid >> 4), ci = tid & 15;
+        if(tap < 27)
+        {
+            float4* dst = reinterpret_cast<float4*>(partial + (((size_t)blockIdx.x * 27 + tap) * 16 + ci) * 16);
+            const bool zero = first || !ok;
+#pragma unroll
+            for(int c = 0; c < 4; ++c)
+                dst[c] = zero ? make_float4(0.f, 0.f, 0.f, 0.f)
+                              : make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if(warp == 0) tmem_free(tmem, 64);
+}
+
+__global__ void k_wgrad_reduce(int nparts, const float* __restrict__ partial, float* __restrict__ dw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= kNetLayerWeights) return;
+    float s = 0.f;
+    for(int c = 0; c < nparts; ++c) s += partial[(size_t)c * kNetLayerWeights + i];
+    dw[i] = s;
+}
+
+// ------------------------------------------------------------ small kernels
+
+// w[tap][ci][co] (FP32) -> per-tap K-major B operand (N = co rows, K = ci).
+// flip != 0: W'[t][ci'][co'] = W[26-t][co'][ci'] (transposed convolution).
+__global__ void k_prepare_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wB, int flip)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= kNetLayerWeights) return;
+    const int t = i / 256, nn = (i / 16) % 16, kk = i % 16;
+    const float v = flip ? w[((26 - t) * 16 + nn) * 16 + kk] : w[(t * 16 + kk) * 16 + nn];
+    unsigned char* base = reinterpret_cast<unsigned char*>(wB) + t * 512;
+    *reinterpret_cast<__nv_bfloat16*>(base + kmajor_off(nn, kk >> 3) + (kk & 7) * 2) = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ void store_embed(__nv_bfloat16* a, long p, float r0)
+{
+    const float v[8] = {r0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    uint4* dst = reinterpret_cast<uint4*>(a + p * kNetCh);
+    dst[0] = pack_bf16x8(v);
+    dst[1] = make_uint4(0, 0, 0, 0);
+}
+
+__global__ void k_embed_perm(PermMap pm, int nz, int ny, int nx, const float* __restrict__ r,
+                             __nv_bfloat16* __restrict__ a)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= (long)nz * ny * nx) return;
+    const int z = (int)(p / ((long)ny * nx));
+    const long rem = p - (long)z * ny * nx;
+    const int y = (int)(rem / nx), x = (int)(rem - (long)y * nx);
+    store_embed(a, p, r[perm_row(pm, z, y, x)]);
+}
+
+__global__ void k_embed_f32(long n, const float* __restrict__ r, __nv_bfloat16* __restrict__ a)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p < n) store_embed(a, p, r[p]);
+}
+
+constexpr int kLossBlocks = 1184;
+
+__global__ void __launch_bounds__(256) k_loss_grad(ConvGrid g, const float* __restrict__ y, const float* __restrict__ e,
+                                                   const float* __restrict__ inv_ee, float scale,
+                                                   __nv_bfloat16* __restrict__ G, float* __restrict__ loss_partial)
+{
+    __shared__ float red[32];
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long n = per * g.nb;
+    float acc = 0.f;
+    for(long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
+    {
+        const float w = inv_ee[p / per] * scale;
+        const float d = y[p] - e[p];
+        acc += d * d * w;
+        store_embed(G, p, 2.f * d * w);
+    }
+    acc = block_sum(acc, red);
+    if(threadIdx.x == 0) loss_partial[blockIdx.x] = acc;
+}
+
+__global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ dw, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float beta1, float beta2, float eps, float c1, float c2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const float gi = dw[i];
+    const float mi = beta1 * m[i] + (1.f - beta1) * gi;
+    const float vi = beta2 * v[i] + (1.f - beta2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+// ------------------------------------------------------------ launchers
+
+static int sm_count()
+{
+    static int sms = 0;
+    if(sms == 0)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if(sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+template <int kOut>
+static int conv_launch(const ConvGrid& g, const void* in, const void* wB, void* out, const void* act, const PermMap& pm,
+                       int* status, cudaStream_t s)
+{
+    static bool attr = false;
+    if(!attr)
+    {
+        HB_CUDA(cudaFuncSetAttribute(k_conv16<kOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+        attr = true;
+    }
+    const long tiles = (long)g.nb * ((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ);
+    const long cap = 2L * sm_count();
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    k_conv16<kOut><<<grid, kConvThreads, kConvSmem, s>>>(g, (const __nv_bfloat16*)in, (const __nv_bfloat16*)wB, out,
+                                                         (const __nv_bfloat16*)act, pm, status);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mode, void* out, const void* act,
+                  const PermMap* pm, int* status, cudaStream_t s)
+{
+    const PermMap none{};
+    const PermMap& m = pm ? *pm : none;
+    switch(out_mode)
+    {
+        case kOutReluBf16: return conv_launch<kOutReluBf16>(g, in, wB, out, act, m, status, s);
+        case kOutMaskBf16: return conv_launch<kOutMaskBf16>(g, in, wB, out, act, m, status, s);
+        case kOutF32: return conv_launch<kOutF32>(g, in, wB, out, act, m, status, s);
+        case kOutF32C0: return conv_launch<kOutF32C0>(g, in, wB, out, act, m, status, s);
+        case kOutPermSet: return conv_launch<kOutPermSet>(g, in, wB, out, act, m, status, s);
+        case kOutPermAdd: return conv_launch<kOutPermAdd>(g, in, wB, out, act, m, status, s);
+        default: return record_error(HPCGB200_ERR_ARG, "conv16: unknown output mode %d", out_mode);
+    }
+}
+
+int conv16_wgrad_parts(long points)
+{
+    const long nblk = (points + kWgK - 1) / kWgK;
+    const long cap = 3L * sm_count();
+    return (int)(nblk < cap ? nblk : cap);
+}
+
+int launch_conv16_wgrad(const ConvGrid& g, const void* x, const void* gr, float* partial, float* dw, int* status,
+                        cudaStream_t s)
+{
+    static bool attr = false;
+    if(!attr)
+    {
+        HB_CUDA(cudaFuncSetAttribute(k_conv16_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
+        attr = true;
+    }
+    const int parts = conv16_wgrad_parts(g.points());
+    k_conv16_wgrad<<<parts, kWgThreads, kWgSmem, s>>>(g, (const __nv_bfloat16*)x, (const __nv_bfloat16*)gr, partial,
+                                                      status);
+    HB_LAUNCHED();
+    k_wgrad_reduce<<<(kNetLayerWeights + 255) / 256, 256, 0, s>>>(parts, partial, dw);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s)
+{
+    k_prepare_weights<<<(kNetLayerWeights + 255) / 256, 256, 0, s>>>(w, (__nv_bfloat16*)wB, flip);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_embed_perm(const PermMap& pm, int nz, int ny, int nx, const float* r, void* a, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    k_embed_perm<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, (__nv_bfloat16*)a);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_embed_f32(long n, const float* r, void* a, cudaStream_t s)
+{
+    k_embed_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, r, (__nv_bfloat16*)a);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int loss_parts(long points)
+{
+    (void)points;
+    return kLossBlocks;
+}
+
+int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, const float* inv_ee, float scale, void* G,
+                     float* loss_partial, cudaStream_t s)
+{
+    k_loss_grad<<<kLossBlocks, 256, 0, s>>>(g, y, e, inv_ee, scale, (__nv_bfloat16*)G, loss_partial);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_adam(int n, float* w, const float* dw, float* m, float* v, float lr, float beta1, float beta2, float eps,
+                int t, cudaStream_t s)
+{
+    const float c1 = 1.f / (1.f - std::pow(beta1, (float)t));
+    const float c2 = 1.f / (1.f - std::pow(beta2, (float)t));
+    k_adam<<<(n + 255) / 256, 256, 0, s>>>(n, w, dw, m, v, lr, beta1, beta2, eps, c1, c2);
+    HB_LAUNCHED();
+    return 0;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" size_t hpcgb200_conv_weight_tile_bytes(void) { return kNetWeightTileBytes; }
+
+extern "C" int hpcgb200_conv_prepare_weights(const float* w, void* wB, int flip, void* stream)
+{
+    HB_CHECK_ARG(w && wB, "bad arguments");
+    HB_CHECK_ARG((reinterpret_cast<uintptr_t>(wB) & 15) == 0, "wB must be 16-byte aligned");
+    return launch_prepare_weights(w, wB, flip, as_stream(stream));
+}
+
+extern "C" int hpcgb200_conv16(int nb, int nz, int ny, int nx, const void* in, const void* wB, int out_mode, void* out,
+                               const void* act, int* status, void* stream)
+{
+    HB_CHECK_ARG(nb > 0 && nz > 0 && ny > 0 && nx > 0 && in && wB && out && status, "bad arguments");
+    HB_CHECK_ARG(out_mode >= kOutReluBf16 && out_mode <= kOutF32C0, "out_mode must be 0..3");
+    HB_CHECK_ARG(out_mode != kOutMaskBf16 || act, "the masked mode needs the activation tensor");
+    HB_CHECK_ARG((reinterpret_cast<uintptr_t>(in) & 15) == 0 && (reinterpret_cast<uintptr_t>(wB) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(out) & 15) == 0 && (reinterpret_cast<uintptr_t>(act) & 15) == 0,
+                 "tensors must be 16-byte aligned");
+    const ConvGrid g{nb, nz, ny, nx};
+    return launch_conv16(g, in, wB, out_mode, out, act, nullptr, status, as_stream(stream));
+}
+
+extern "C" size_t hpcgb200_conv_wgrad_partial_bytes(int nb, int nz, int ny, int nx)
+{
+    return sizeof(float) * kNetLayerWeights * (size_t)conv16_wgrad_parts((long)nb * nz * ny * nx);
+}
+
+extern "C" int hpcgb200_conv16_wgrad(int nb, int nz, int ny, int nx, const void* x, const void* g, float* partial,
+                                     float* dw, int* status, void* stream)
+{
+    HB_CHECK_ARG(nb > 0 && nz > 0 && ny > 0 && nx > 0 && x && g && partial && dw && status, "bad arguments");
+    HB_CHECK_ARG((reinterpret_cast<uintptr_t>(x) & 15) == 0 && (reinterpret_cast<uintptr_t>(g) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(partial) & 15) == 0,
+                 "tensors must be 16-byte aligned");
+    const ConvGrid cg{nb, nz, ny, nx};
+    return launch_conv16_wgrad(cg, x, g, partial, dw, status, as_stream(stream));
+}

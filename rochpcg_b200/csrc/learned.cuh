@@ -1,0 +1,74 @@
+// Learned smoother kernels: a 3-layer 3x3x3 convolutional network (1 -> 16
+// -> 16 -> 1 channels, ReLU, no bias, BF16 weights and activations, FP32
+// accumulation) as implicit GEMMs on the tcgen05 tensor cores, with its
+// training kernels (input and weight gradients, loss, Adam).
+#pragma once
+
+#include "common.cuh"
+#include "mixed.cuh"
+
+namespace hb {
+
+constexpr int kNetCh = 16;                     // channels of every layer tensor
+constexpr int kNetLayerWeights = 27 * 16 * 16; // w[tap][ci][co], tap = (dz+1)*9 + (dy+1)*3 + (dx+1)
+constexpr int kNetWeightTileBytes = 27 * 16 * 16 * 2;  // one layer's BF16 B operands
+
+// Epilogues of the forward convolution.
+enum ConvOut : int
+{
+    kOutReluBf16 = 0,  // out = bf16(relu(v)), 16 channels (hidden layers)
+    kOutMaskBf16 = 1,  // out = bf16(act > 0 ? v : 0), 16 channels (ReLU backward)
+    kOutF32 = 2,       // out = v, FP32 16 channels
+    kOutF32C0 = 3,     // out = v[0], FP32 scalar field
+    kOutPermSet = 4,   // x[row(p)] = v[0] on a stencil level's colour-permuted vector
+    kOutPermAdd = 5,   // x[row(p)] += v[0]
+};
+
+// Natural grid point -> colour-permuted row of a parity-coloured level.
+struct PermMap
+{
+    int offsets[9];
+    int bx[8], by[8];
+    int color_of_par[8];
+};
+PermMap make_perm_map(const StencilLevel& L);
+
+// nb samples of nz x ny x nx points, channel-last, samples back to back.
+struct ConvGrid
+{
+    int nb, nz, ny, nx;
+    long points() const { return (long)nb * nz * ny * nx; }
+};
+
+// FP32 weights -> BF16 tensor-core operand tiles (flip != 0: the mirrored-tap,
+// swapped-channel weights of the transposed convolution).
+int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s);
+
+// out = conv(in, W) with the epilogue `out_mode`; `act` is the activation
+// tensor of kOutMaskBf16, `pm` the row map of the permuted modes (nb == 1).
+int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mode, void* out, const void* act,
+                  const PermMap* pm, int* status, cudaStream_t s);
+
+// dw[tap][ci][co] = sum_p x[p + tap][ci] * gr[p][co] (partial: one block of
+// conv16_wgrad_parts(points) x 27*256 floats).
+int conv16_wgrad_parts(long points);
+int launch_conv16_wgrad(const ConvGrid& g, const void* x, const void* gr, float* partial, float* dw, int* status,
+                        cudaStream_t s);
+
+// BF16 16-channel tensor whose channel 0 is a scalar field (others zero):
+// from a colour-permuted FP32 level vector, or from an FP32 natural field.
+int launch_embed_perm(const PermMap& pm, int nz, int ny, int nx, const float* r, void* a, cudaStream_t s);
+int launch_embed_f32(long n, const float* r, void* a, cudaStream_t s);
+
+// Loss of a batch: sum_b ||y_b - e_b||^2 * inv_ee[b] * scale (per-block
+// partial sums, `loss_partial` of loss_parts(points) floats) and its
+// gradient 2 (y - e) inv_ee[b] scale as BF16 channel 0 of G.
+int loss_parts(long points);
+int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, const float* inv_ee, float scale, void* G,
+                     float* loss_partial, cudaStream_t s);
+
+// One Adam step on n parameters (bias-corrected, step t >= 1).
+int launch_adam(int n, float* w, const float* dw, float* m, float* v, float lr, float beta1, float beta2, float eps,
+                int t, cudaStream_t s);
+
+}  // namespace hb
