@@ -209,6 +209,9 @@ typedef struct hpcgb200_problem hpcgb200_problem;
 
 #define HPCGB200_MODE_FP64 0    /* plain FP64 drop-in (the reference's optimized path) */
 #define HPCGB200_MODE_MIXED 1   /* FP64 outer CG, FP32 V-cycle on the implicit stencil */
+#define HPCGB200_MODE_LEARNED 2 /* as MIXED, with the attached learned smoother on the coarse levels
+                                   (flexible CG; falls back to MIXED once an iteration does not
+                                   reduce the FP64 residual) */
 
 int hpcgb200_problem_create(int nx, int ny, int nz, int nlevels, hpcgb200_problem** out);
 /* flags: HPCGB200_FLAG_KEEP_GENERATED keeps the row-major generated arrays
@@ -284,6 +287,70 @@ int hpcgb200_problem_symgs_zero(hpcgb200_problem* p, int level, const double* r,
 int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* r, double* x);
 int hpcgb200_problem_restrict(hpcgb200_problem* p, int level, const double* rf, const double* xf, double* rc);
 int hpcgb200_problem_prolong(hpcgb200_problem* p, int level, const double* xc, double* xf);
+
+/* ------------------------------------------------------ learned smoother
+ * No reference counterpart.  A smoother handle owns the conv net's FP32
+ * master weights (HPCGB200_SMOOTHER_WEIGHTS floats: layers 1..3 back to back,
+ * each w[tap][ci][co]), its BF16 operand tiles, activation buffers and Adam
+ * state, all in device memory.  Fields r, e, y are FP32 DEVICE arrays in
+ * natural grid order, samples back to back. */
+typedef struct hpcgb200_smoother hpcgb200_smoother;
+#define HPCGB200_SMOOTHER_WEIGHTS (3 * 27 * 16 * 16)
+
+int hpcgb200_smoother_create(hpcgb200_smoother** out);
+/* Detach it from every problem (hpcgb200_problem_set_smoother(p, NULL, 0))
+ * before destroying it. */
+int hpcgb200_smoother_destroy(hpcgb200_smoother* s);
+int hpcgb200_smoother_set_weights(hpcgb200_smoother* s, const float* host_w);
+int hpcgb200_smoother_get_weights(hpcgb200_smoother* s, float* host_w);
+/* Host-side initial weights: the network computes omega * r / 26 (a damped
+ * Jacobi step: channel 0 = relu(r), channel 1 = relu(-r)) plus uniform noise
+ * in [-noise, noise] on every other used weight, from a SplitMix64 stream. */
+int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsigned long long seed);
+/* y = N(r) for nb samples of nz x ny x nx points. */
+int hpcgb200_smoother_forward(hpcgb200_smoother* s, int nb, int nz, int ny, int nx, const float* r, float* y,
+                              void* stream);
+/* loss = scale * sum_b ||N(r_b) - e_b||^2 * inv_ee[b] (inv_ee: device, nb
+ * floats) and its gradient with respect to the weights, copied to dw (device,
+ * HPCGB200_SMOOTHER_WEIGHTS floats) when not NULL; the handle keeps it for
+ * hpcgb200_smoother_adam_step.  *loss (host) may be NULL. */
+int hpcgb200_smoother_loss_grad(hpcgb200_smoother* s, int nb, int nz, int ny, int nx, const float* r, const float* e,
+                                const float* inv_ee, float scale, float* dw, double* loss, void* stream);
+/* One bias-corrected Adam step with the last gradient. */
+int hpcgb200_smoother_adam_step(hpcgb200_smoother* s, float lr, float beta1, float beta2, float eps, void* stream);
+
+/* A set of `count` training pairs of one grid size, trained `batch` samples
+ * per step (r, e: count * nz*ny*nx floats; inv_ee: count floats, 1/||e||^2). */
+typedef struct
+{
+    const float* r;
+    const float* e;
+    const float* inv_ee;
+    int count, nz, ny, nx, batch;
+} hpcgb200_pair_set;
+/* Adam training over the sets for `epochs` passes (batches of all sets in a
+ * seeded shuffled order; learning rate geometric from lr0 to lr1; loss per
+ * sample relative to ||e||^2).  epoch_loss (host, may be NULL): mean loss of
+ * each epoch. */
+int hpcgb200_smoother_train(hpcgb200_smoother* s, const hpcgb200_pair_set* sets, int nsets, int epochs, float lr0,
+                            float lr1, unsigned long long seed, double* epoch_loss, void* stream);
+/* Training pairs from the plain FP32 V-cycle: for seeds first_seed ..
+ * first_seed+count-1, b ~ N(0,1) (hpcgb200_normal_rhs) on a fine_n^3 grid;
+ * r = the residual the V-cycle hands to MG level `level`, e = A_level^-1 r
+ * (FP64 MG-PCG to relative residual tol); both in natural order of the
+ * (fine_n >> level)^3 level grid, FP32 device arrays of count * points;
+ * inv_ee (device, count floats) = 1 / ||e||^2. */
+int hpcgb200_make_training_pairs(int fine_n, int level, unsigned long long first_seed, int count, float* r,
+                                 float* e, float* inv_ee, double tol);
+/* N(0,1) values by natural index (SplitMix64 + Box-Muller, the generator of
+ * rochpcg_b200/rhs.py) into out (device, m doubles). */
+int hpcgb200_normal_rhs(long long m, unsigned long long seed, double* out, void* stream);
+
+/* Attach a smoother (NULL detaches) to the problem's levels >= first_level
+ * for HPCGB200_MODE_LEARNED; the handle must outlive the attachment. */
+int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* s, int first_level);
+/* Iteration at which the last learned solve fell back to SymGS (0: never). */
+int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter);
 
 /* Time n back-to-back launches of one level-0 operator with CUDA events on
  * the problem's stream; *ms_per_launch = average.  op: "spmv","symgs_sweep"

@@ -22,6 +22,7 @@ from ._lib import LIB_PATH, load, HpcgError, check  # noqa: F401
 
 MODE_FP64 = 0
 MODE_MIXED = 1
+MODE_LEARNED = 2
 FLAG_KEEP_GENERATED = 1
 
 _FIELD_DTYPES = {
@@ -90,6 +91,7 @@ class Problem:
         if getattr(self, "h", None):
             self.L.hpcgb200_problem_destroy(self.h)
             self.h = None
+            self._smoother = None
 
     def __del__(self):
         try:
@@ -207,6 +209,23 @@ class Problem:
 
     def prolong(self, level: int, xc_ptr: int, xf_ptr: int):
         check(self.L, self.L.hpcgb200_problem_prolong(self.h, level, ctypes.c_void_p(xc_ptr), ctypes.c_void_p(xf_ptr)))
+
+    # -- learned smoother --------------------------------------------------
+    def set_smoother(self, smoother, first_level: int = 2):
+        """Attach a ``rochpcg_b200.learned.Smoother`` to levels >= first_level
+        for MODE_LEARNED (None detaches)."""
+        if smoother is None:
+            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, None, 0))
+            self._smoother = None
+        else:
+            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, smoother.h, first_level))
+            self._smoother = smoother  # kept alive while attached
+
+    def last_fallback(self) -> int:
+        """Iteration at which the last MODE_LEARNED solve fell back to SymGS (0: never)."""
+        it = ctypes.c_int()
+        check(self.L, self.L.hpcgb200_problem_last_fallback(self.h, ctypes.byref(it)))
+        return it.value
 
     def time_op(self, op: str, n: int) -> float:
         ms = ctypes.c_double()

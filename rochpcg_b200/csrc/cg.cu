@@ -167,12 +167,19 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const do
 // the WHILE node ends after at most max_iter iterations whatever the
 // reductions produced.  src/CG.cpp:148: continue while k <= max_iter &&
 // normr/normr0 > tol (a NaN residual compares false and ends the loop).
-__global__ void k_cg_loop_control(CGState* st, unsigned long long cond)
+__global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watch_net)
 {
     const int k = st->k;
     st->niters = k;
     st->k = k + 1;
-    const unsigned go = (k + 1 <= st->max_iter) && (st->normr / st->normr0 > st->tol);
+    // learned smoother: fall back for good once an iteration fails to reduce normr
+    if(st->net == 1 && !(st->normr < st->hist[k - 1]))
+    {
+        st->net = 2;
+        st->fallback_iter = k;
+    }
+    unsigned go = (k + 1 <= st->max_iter) && (st->normr / st->normr0 > st->tol);
+    if(watch_net && st->net == 2) go = 0;
     if(cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, go);
 }
 
@@ -219,11 +226,11 @@ int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const d
 }
 
 int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, cudaStream_t s)
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
 {
     k_cg_update_xr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
     HB_LAUNCHED();
-    k_cg_loop_control<<<1, 1, 0, s>>>(st, cond);
+    k_cg_loop_control<<<1, 1, 0, s>>>(st, cond, watch_net);
     HB_LAUNCHED();
     return 0;
 }

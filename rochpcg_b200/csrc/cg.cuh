@@ -19,7 +19,9 @@ struct CGState
     int niters;
     int flexible;         // 1: Polak-Ribiere beta (flexible CG); 0: Fletcher-Reeves as the reference
     int status;           // nonzero: a device-side check failed
-    int pad[3];
+    int net;              // learned smoother: 0 not used, 1 active, 2 failed to reduce normr (fell back)
+    int fallback_iter;    // iteration at which it failed (0: never)
+    int pad;
     double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
 };
 
@@ -39,9 +41,11 @@ int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const d
                        double* Ap, CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
 // r -= alpha Ap, normr = ||r||, x += alpha p, history; then (own 1-thread
 // kernel) k++ and the loop condition (k <= max_iter && normr/normr0 > tol)
-// written to `cond` (a graph conditional handle; 0 = none).
+// written to `cond` (a graph conditional handle; 0 = none).  While the
+// learned smoother is active (net == 1) an iteration that does not reduce
+// normr marks it failed (net = 2); with watch_net the loop then also ends.
 int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, cudaStream_t s);
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
 
 // Mixed precision glue: r32 = (float) r and z = (double) z32.
 int launch_cast_d2f(int n, const double* in, float* out, cudaStream_t s);

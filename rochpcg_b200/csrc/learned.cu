@@ -500,15 +500,94 @@ __device__ __forceinline__ void store_embed(__nv_bfloat16* a, long p, float r0)
     dst[1] = make_uint4(0, 0, 0, 0);
 }
 
-__global__ void k_embed_perm(PermMap pm, int nz, int ny, int nx, const float* __restrict__ r,
-                             __nv_bfloat16* __restrict__ a)
+// Channel 0 = r (x == nullptr) or the residual r - A x of the 27-point
+// stencil (diagonal diag32, off-diagonals -1), read from colour-permuted
+// level vectors at natural point p.
+__global__ void k_embed_level(PermMap pm, int nz, int ny, int nx, const float* __restrict__ r,
+                              const float* __restrict__ x, const float* __restrict__ diag32,
+                              __nv_bfloat16* __restrict__ a)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= (long)nz * ny * nx) return;
+    const int z = (int)(p / ((long)ny * nx));
+    const long rem = p - (long)z * ny * nx;
+    const int y = (int)(rem / nx), xx = (int)(rem - (long)y * nx);
+    const int row = perm_row(pm, z, y, xx);
+    float v = r[row];
+    if(x)
+    {
+        float off = 0.f;
+#pragma unroll
+        for(int t = 0; t < 27; ++t)
+        {
+            const int z2 = z + t / 9 - 1, y2 = y + (t / 3) % 3 - 1, x2 = xx + t % 3 - 1;
+            if(t != 13 && z2 >= 0 && z2 < nz && y2 >= 0 && y2 < ny && x2 >= 0 && x2 < nx)
+                off += x[perm_row(pm, z2, y2, x2)];
+        }
+        v = v - (diag32[row] * x[row] - off);
+    }
+    store_embed(a, p, v);
+}
+
+// Natural <-> colour-permuted copies of a level vector (training-pair set-up).
+template <typename Tin, typename Tout, bool kToNatural>
+__global__ void k_perm_copy(PermMap pm, int nz, int ny, int nx, const Tin* __restrict__ in, Tout* __restrict__ out)
 {
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= (long)nz * ny * nx) return;
     const int z = (int)(p / ((long)ny * nx));
     const long rem = p - (long)z * ny * nx;
     const int y = (int)(rem / nx), x = (int)(rem - (long)y * nx);
-    store_embed(a, p, r[perm_row(pm, z, y, x)]);
+    const int row = perm_row(pm, z, y, x);
+    if(kToNatural) out[p] = (Tout)in[row];
+    else out[row] = (Tout)in[p];
+}
+
+// 1 / sum e^2 (one block, FP64 accumulation).
+__global__ void k_inv_sumsq(long n, const float* __restrict__ e, float* __restrict__ out)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for(long i = threadIdx.x; i < n; i += blockDim.x) s += (double)e[i] * e[i];
+    s = block_sum(s, red);
+    if(threadIdx.x == 0) *out = (float)(1.0 / s);
+}
+
+// Sum of a step's loss partials into acc (one block, fixed order).
+__global__ void k_loss_accumulate(int parts, const float* __restrict__ partial, double* __restrict__ acc)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for(int i = threadIdx.x; i < parts; i += blockDim.x) s += partial[i];
+    s = block_sum(s, red);
+    if(threadIdx.x == 0) *acc += s;
+}
+
+// b ~ N(0,1) by natural row id: SplitMix64 finalizer over (key + 2i, key + 2i + 1)
+// with key = mix(seed), 53-bit uniforms u1 in (0,1], u2 in [0,1), Box-Muller
+// sqrt(-2 ln u1) cos(2 pi u2).  Stored at out[perm[i]] (perm may be null).
+__device__ __forceinline__ unsigned long long splitmix(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_normal_rhs(long long m, unsigned long long seed, const int* __restrict__ perm, double* out64,
+                             float* out32)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m) return;
+    const unsigned long long key = splitmix(seed);
+    const unsigned long long a = splitmix(key + 2ULL * (unsigned long long)i);
+    const unsigned long long b = splitmix(key + 2ULL * (unsigned long long)i + 1ULL);
+    const double u1 = ((double)(a >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    const double u2 = (double)(b >> 11) * (1.0 / 9007199254740992.0);
+    const double v = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    const long long o = perm ? perm[i] : i;
+    if(out64) out64[o] = v;
+    if(out32) out32[o] = (float)v;
 }
 
 __global__ void k_embed_f32(long n, const float* __restrict__ r, __nv_bfloat16* __restrict__ a)
@@ -634,10 +713,57 @@ int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s)
     return 0;
 }
 
-int launch_embed_perm(const PermMap& pm, int nz, int ny, int nx, const float* r, void* a, cudaStream_t s)
+int launch_embed_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
+                       const float* diag32, void* a, cudaStream_t s)
 {
     const long n = (long)nz * ny * nx;
-    k_embed_perm<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, (__nv_bfloat16*)a);
+    k_embed_level<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, x, diag32, (__nv_bfloat16*)a);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_natural_from_perm(const PermMap& pm, int nz, int ny, int nx, const float* in, float* out, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    k_perm_copy<float, float, true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, in, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_natural_from_perm(const PermMap& pm, int nz, int ny, int nx, const double* in, float* out, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    k_perm_copy<double, float, true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, in, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_perm_from_natural(const PermMap& pm, int nz, int ny, int nx, const float* in, double* out, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    k_perm_copy<float, double, false><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, in, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_inv_sumsq(long n, const float* e, float* out, cudaStream_t s)
+{
+    k_inv_sumsq<<<1, 1024, 0, s>>>(n, e, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_loss_accumulate(const float* partial, double* acc, cudaStream_t s)
+{
+    k_loss_accumulate<<<1, 1024, 0, s>>>(kLossBlocks, partial, acc);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_normal_rhs(long long m, unsigned long long seed, const int* perm, double* out64, float* out32,
+                      cudaStream_t s)
+{
+    k_normal_rhs<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(m, seed, perm, out64, out32);
     HB_LAUNCHED();
     return 0;
 }
@@ -715,4 +841,11 @@ extern "C" int hpcgb200_conv16_wgrad(int nb, int nz, int ny, int nx, const void*
                  "tensors must be 16-byte aligned");
     const ConvGrid cg{nb, nz, ny, nx};
     return launch_conv16_wgrad(cg, x, g, partial, dw, status, as_stream(stream));
+}
+
+extern "C" int hpcgb200_normal_rhs(long long m, unsigned long long seed, double* out, void* stream)
+{
+    HB_CHECK_ARG(m >= 0 && (m == 0 || out), "bad arguments");
+    if(m == 0) return 0;
+    return launch_normal_rhs(m, seed, nullptr, out, nullptr, as_stream(stream));
 }

@@ -56,9 +56,24 @@ int launch_conv16_wgrad(const ConvGrid& g, const void* x, const void* gr, float*
                         cudaStream_t s);
 
 // BF16 16-channel tensor whose channel 0 is a scalar field (others zero):
-// from a colour-permuted FP32 level vector, or from an FP32 natural field.
-int launch_embed_perm(const PermMap& pm, int nz, int ny, int nx, const float* r, void* a, cudaStream_t s);
+// from colour-permuted FP32 level vectors (r, or the residual r - A x when x
+// is not null), or from an FP32 natural field.
+int launch_embed_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
+                       const float* diag32, void* a, cudaStream_t s);
 int launch_embed_f32(long n, const float* r, void* a, cudaStream_t s);
+
+// Natural <-> colour-permuted copies of level vectors.
+int launch_natural_from_perm(const PermMap& pm, int nz, int ny, int nx, const float* in, float* out, cudaStream_t s);
+int launch_natural_from_perm(const PermMap& pm, int nz, int ny, int nx, const double* in, float* out, cudaStream_t s);
+int launch_perm_from_natural(const PermMap& pm, int nz, int ny, int nx, const float* in, double* out, cudaStream_t s);
+// *out = 1 / sum e^2.
+int launch_inv_sumsq(long n, const float* e, float* out, cudaStream_t s);
+// *acc += sum of the loss partials of launch_loss_grad.
+int launch_loss_accumulate(const float* partial, double* acc, cudaStream_t s);
+// N(0,1) right-hand side by natural row id (the generator of rochpcg_b200/rhs.py),
+// stored at out[perm[i]] (perm may be null) as double and/or float.
+int launch_normal_rhs(long long m, unsigned long long seed, const int* perm, double* out64, float* out32,
+                      cudaStream_t s);
 
 // Loss of a batch: sum_b ||y_b - e_b||^2 * inv_ee[b] * scale (per-block
 // partial sums, `loss_partial` of loss_parts(points) floats) and its

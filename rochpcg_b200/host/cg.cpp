@@ -16,6 +16,7 @@
 
 #include "hpcg_b200.h"
 #include "internal.hpp"
+#include "learned.hpp"
 
 using namespace hpcg_b200;
 
@@ -43,7 +44,9 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     const int n = A.localNumberOfRows;
     if(precond)
     {
-        HB_RETURN_IF(prec == MGPrecision::FP64 ? ComputeMG(A, data.r, data.z) : ComputeMG_Mixed(A, data.r, data.z));
+        if(prec == MGPrecision::FP64) HB_RETURN_IF(ComputeMG(A, data.r, data.z));
+        else if(prec == MGPrecision::FP32) HB_RETURN_IF(ComputeMG_Mixed(A, data.r, data.z));
+        else HB_RETURN_IF(ComputeMG_Learned(A, data.r, data.z));
     }
     else
     {
@@ -53,7 +56,7 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     }
     HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
     HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
-    if(prec == MGPrecision::FP32)
+    if(prec != MGPrecision::FP64)
     {
         // mixed path: the FP64 operator on the implicit stencil (bitwise equal to the ELL product)
         const LevelOpt* o = opt(A);
@@ -67,7 +70,8 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
                                             o->spmv_partial, o->spmv_ticket, s));
     }
     HB_RETURN_IF(hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
-                                         data.z.d_values, st, rt().ws, cond, s));
+                                         data.z.d_values, st, rt().ws, cond, prec == MGPrecision::LEARNED ? 1 : 0,
+                                         s));
     return 0;
 }
 
@@ -92,16 +96,28 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
     LevelOpt* o = opt(A);
     const double* key[6] = {data.r.d_values, data.z.d_values, data.p.d_values, data.Ap.d_values, b.d_values,
                             x.d_values};
-    for(auto& g : o->graphs)
-        if(!std::memcmp(g->key, key, sizeof(key)) && g->mode == (int)prec && g->precond == precond &&
-           g->flexible == flexible)
-            return g.get();
+    const void* sm = prec == MGPrecision::LEARNED ? o->smoother : nullptr;
+    const long long sm_epoch = sm ? o->smoother->epoch : -1;
+    for(auto it = o->graphs.begin(); it != o->graphs.end(); ++it)
+    {
+        CGGraph* g = it->get();
+        if(std::memcmp(g->key, key, sizeof(key)) || g->mode != (int)prec || g->precond != precond ||
+           g->flexible != flexible)
+            continue;
+        if(g->smoother == sm && g->smoother_epoch == sm_epoch) return g;
+        if(g->exec) cudaGraphExecDestroy(g->exec);  // captured other smoother buffers
+        if(g->graph) cudaGraphDestroy(g->graph);
+        o->graphs.erase(it);
+        break;
+    }
 
     auto G = std::make_unique<CGGraph>();
     std::memcpy(G->key, key, sizeof(key));
     G->mode = (int)prec;
     G->precond = precond;
     G->flexible = flexible;
+    G->smoother = sm;
+    G->smoother_epoch = sm_epoch;
     cudaStream_t s = rt().stream;
 
     // Preferred: WHILE conditional node around the iteration body.
@@ -166,6 +182,11 @@ int iteration_kernels(const SparseMatrix& A, CGData& data, const Vector& b, Vect
 {
     LevelOpt* o = opt(A);
     ensure_state(o, 1);
+    if(prec == MGPrecision::LEARNED)
+    {
+        if(!o->smoother) throw Error(HPCGB200_ERR_ARG, "learned CG: no smoother attached to the problem");
+        check(smoother_prepare(*o->smoother, rt().stream));
+    }
     return get_graph(A, data, b, x, precond, prec, flexible)->kernels_per_iteration;
 }
 
@@ -197,6 +218,10 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         h.tol = tol;
         h.max_iter = max_iter;
         h.flexible = flexible ? 1 : 0;
+        h.net = prec == MGPrecision::LEARNED ? 1 : 0;
+        if(prec == MGPrecision::LEARNED && !o->smoother)
+            return hb::record_error(HPCGB200_ERR_ARG, "learned CG: no smoother attached to the problem");
+        if(prec == MGPrecision::LEARNED) check(smoother_prepare(*o->smoother, s));
         cudaEvent_t e0, e1;
         HB_HOST_CUDA(cudaEventCreate(&e0));
         HB_HOST_CUDA(cudaEventCreate(&e1));
@@ -209,7 +234,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
 
         // preamble: p = x; Ap = A p; r = b - Ap; normr = ||r||
         HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        if(prec == MGPrecision::FP32)
+        if(prec != MGPrecision::FP64)
         {
             for(const SparseMatrix* M = &A; M; M = M->Ac)
                 if(!opt(*M) || !opt(*M)->stencil_ok)
@@ -225,34 +250,46 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
         HB_HOST_CUDA(cudaStreamSynchronize(s));
 
-        const bool iterate = max_iter >= 1 && (h.normr / h.normr0 > tol);
-        if(iterate && !graphs_enabled())
+        // Iterations: the learned mode runs until converged or until its
+        // smoother fails to reduce normr; the plain FP32 V-cycle then takes
+        // over from the same state (flexible CG tolerates the switch).
+        MGPrecision cur = prec;
+        for(int phase = 0; phase < 2; ++phase)
         {
-            for(int k = 1; k <= max_iter; ++k)
+            const bool iterate = h.k <= max_iter && max_iter >= 1 && (h.normr / h.normr0 > tol);
+            if(!iterate) break;
+            if(!graphs_enabled())
             {
-                check(capture_body(A, data, x, precond, prec, st, 0ULL, s));
-                HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
-                HB_HOST_CUDA(cudaStreamSynchronize(s));
-                if(!(h.normr / h.normr0 > tol)) break;
-            }
-        }
-        else if(iterate)
-        {
-            CGGraph* G = get_graph(A, data, b, x, precond, prec, flexible);
-            if(G->conditional)
-            {
-                HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
+                for(int k = h.k; k <= max_iter; ++k)
+                {
+                    check(capture_body(A, data, x, precond, cur, st, 0ULL, s));
+                    HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+                    HB_HOST_CUDA(cudaStreamSynchronize(s));
+                    if(!(h.normr / h.normr0 > tol) || (cur == MGPrecision::LEARNED && h.net == 2)) break;
+                }
             }
             else
             {
-                for(int k = 1; k <= max_iter; ++k)
+                CGGraph* G = get_graph(A, data, b, x, precond, cur, flexible);
+                if(G->conditional)
                 {
                     HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
-                    HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
-                    HB_HOST_CUDA(cudaStreamSynchronize(s));
-                    if(!(h.normr / h.normr0 > tol)) break;
+                }
+                else
+                {
+                    for(int k = h.k; k <= max_iter; ++k)
+                    {
+                        HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
+                        HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+                        HB_HOST_CUDA(cudaStreamSynchronize(s));
+                        if(!(h.normr / h.normr0 > tol) || (cur == MGPrecision::LEARNED && h.net == 2)) break;
+                    }
                 }
             }
+            HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+            HB_HOST_CUDA(cudaStreamSynchronize(s));
+            if(cur != MGPrecision::LEARNED || h.net != 2) break;
+            cur = MGPrecision::FP32;
         }
         HB_HOST_CUDA(cudaEventRecord(e1, s));
         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
@@ -266,6 +303,8 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             HB_HOST_CUDA(cudaMemcpy(hist, st->hist, sizeof(double) * (h.niters + 1), cudaMemcpyDeviceToHost));
             for(int k = h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
         }
+        o->last_fallback_iter = h.fallback_iter;
+        if(prec == MGPrecision::LEARNED) check(smoother_status(*o->smoother, s));
         niters = h.niters;
         normr = h.normr;
         normr0 = h.normr0;

@@ -147,8 +147,9 @@ typedef struct TestNormsData_STRUCT TestNormsData;
 // Preconditioner precision of a solve (the FP64 outer recurrence is the same).
 enum class MGPrecision
 {
-    FP64 = 0,   // the reference's optimized path, FP64 ELL
-    FP32 = 1    // FP32 vectors + FP32 accumulation, implicit stencil values
+    FP64 = 0,    // the reference's optimized path, FP64 ELL
+    FP32 = 1,    // FP32 vectors + FP32 accumulation, implicit stencil values
+    LEARNED = 2  // FP32 V-cycle whose coarse levels use the learned conv-net smoother
 };
 
 // ---------------------------------------------------------------- runtime
@@ -200,6 +201,11 @@ int ComputeResidual(local_int_t n, const Vector& v1, const Vector& v2, double& r
 
 // FP32 V-cycle on FP64 vectors (no reference counterpart): z = M32^{-1} r.
 int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x);
+// FP32 V-cycle with the learned smoother attached to A (no reference
+// counterpart): on levels >= its first level the conv net replaces the pre-
+// and post-smoothing SymGS (x = N(r); ...; x += N(r - A x)) and the coarsest
+// solve.  Nonlinear and non-symmetric: use it inside flexible CG.
+int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x);
 
 // --------------------------------------------------------------- solver
 int CG(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const int max_iter, const double tolerance,

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../csrc/cg.cuh"
+#include "../csrc/learned.cuh"
 #include "../csrc/mixed.cuh"
 #include "../csrc/ops64.cuh"
 #include "hpcg.hpp"
@@ -65,6 +66,8 @@ struct CGGraph
     bool precond = true;
     bool flexible = false;
     int kernels_per_iteration = 0;     // kernel nodes of one iteration body
+    const void* smoother = nullptr;    // learned mode: smoother and buffer epoch the body captured
+    long long smoother_epoch = -1;
 };
 
 // Per-level implementation data (SparseMatrix::optimizationData).
@@ -93,6 +96,12 @@ struct LevelOpt
     float* r32 = nullptr;              // FP32 right-hand side of the V-cycle (level 0)
     float* z32 = nullptr;              // FP32 V-cycle result (level 0)
     double* vec_scratch = nullptr;     // one FP64 vector of length m (TestCG / TestSymmetry)
+
+    // learned smoother (level 0 holds it for the hierarchy)
+    struct Smoother* smoother = nullptr;
+    int smoother_first_level = 2;
+    int last_fallback_iter = 0;        // learned CG: iteration at which the last solve fell back (0: none)
+    hb::PermMap pm{};                  // natural point -> permuted row (stencil levels)
 };
 
 // Per-level transfer data (MGData::optimizationData).

@@ -90,6 +90,7 @@ static void optimize_level(SparseMatrix& A)
     }
     if(o->stencil_ok)
     {
+        o->pm = hb::make_perm_map(o->st);
         o->diag32 = dalloc<float>(m);
         o->inv_diag32 = dalloc<float>(m);
         check(hb::launch_diag32(m, o->diag, o->diag32, o->inv_diag32, s));

@@ -9,6 +9,7 @@
 
 #include "hpcg_b200.h"
 #include "internal.hpp"
+#include "problem.hpp"
 
 using namespace hpcg_b200;
 
@@ -16,21 +17,19 @@ namespace hpcg_b200 {
 extern bool g_keep_generated;
 }
 
-struct hpcgb200_problem
-{
-    Geometry* geom = nullptr;
-    SparseMatrix A{};
-    Vector b, x, xexact;
-    CGData data{};
-    int nlevels = 0;
-    double setup_s = 0.0, optimize_s = 0.0;
-    double* b_generated = nullptr;  // permuted generated b (restored by set_rhs(NULL))
-    std::vector<SparseMatrix*> levels;
-};
 
 namespace {
 
-MGPrecision prec_of(int mode) { return mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32 : MGPrecision::FP64; }
+MGPrecision prec_of(int mode)
+{
+    return mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32
+                                       : (mode == HPCGB200_MODE_LEARNED ? MGPrecision::LEARNED : MGPrecision::FP64);
+}
+
+bool mode_ok(int mode)
+{
+    return mode == HPCGB200_MODE_FP64 || mode == HPCGB200_MODE_MIXED || mode == HPCGB200_MODE_LEARNED;
+}
 
 template <typename F>
 int guarded(F&& f)
@@ -310,7 +309,7 @@ extern "C" int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, 
                                    double* normr, double* normr0, double* normr_hist, double* seconds)
 {
     if(!p || !niters || !normr || !normr0) return hb::record_error(HPCGB200_ERR_ARG, "null argument");
-    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
+    if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     return guarded([&] {
         CudaZeroVector(p->x);
         return run_cg(p->A, p->data, p->b, p->x, max_iter, tol, *niters, *normr, *normr0, precond != 0, prec_of(mode),
@@ -324,7 +323,7 @@ extern "C" int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const 
 {
     if(!p || !b_natural || !x_natural || !niters || !normr || !normr0)
         return hb::record_error(HPCGB200_ERR_ARG, "null argument");
-    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
+    if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     return guarded([&] {
         const auto t0 = std::chrono::steady_clock::now();
         const int m = p->A.localNumberOfRows;
@@ -365,6 +364,7 @@ extern "C" int hpcgb200_problem_true_residual(hpcgb200_problem* p, double* rel)
 extern "C" int hpcgb200_problem_kernels_per_iteration(hpcgb200_problem* p, int mode, int precond, int* kernels)
 {
     if(!p || !kernels) return hb::record_error(HPCGB200_ERR_ARG, "null argument");
+    if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     return guarded([&] {
         *kernels = iteration_kernels(p->A, p->data, p->b, p->x, precond != 0, prec_of(mode), mode != HPCGB200_MODE_FP64);
         return 0;
@@ -375,6 +375,8 @@ extern "C" int hpcgb200_problem_test_cg(hpcgb200_problem* p, int mode, int* out_
                                         int* count_fail)
 {
     if(!p) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
+    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED)
+        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED");
     TestCGData d{};
     const int rc = TestCG_B200(p->A, p->data, p->b, p->x, d, prec_of(mode));
     if(out_niters)
@@ -388,6 +390,8 @@ extern "C" int hpcgb200_problem_test_symmetry(hpcgb200_problem* p, int mode, dou
                                               double* residual_inf)
 {
     if(!p) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
+    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED)
+        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED");
     TestSymmetryData d{};
     const int rc = TestSymmetry_B200(p->A, p->b, p->xexact, d, prec_of(mode));
     if(depsym_spmv) *depsym_spmv = d.depsym_spmv;
@@ -443,6 +447,7 @@ extern "C" int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* 
 {
     if(!p || !r || !x) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     Vector rv = wrap(r, p->A.localNumberOfRows), xv = wrap(x, p->A.localNumberOfRows);
+    if(mode == HPCGB200_MODE_LEARNED) return ComputeMG_Learned(p->A, rv, xv);
     return mode == HPCGB200_MODE_MIXED ? ComputeMG_Mixed(p->A, rv, xv) : ComputeMG(p->A, rv, xv);
 }
 

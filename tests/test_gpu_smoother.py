@@ -1,0 +1,152 @@
+"""The learned smoother end to end on the GPU: forward and gradients of the
+whole network against the conv-net oracle, training pairs against the
+coloured-path oracle, training on the device, and the learned V-cycle inside
+flexible CG with its fallback to SymGS.
+
+Gradient tolerance: both sides use the same BF16 rounding points and FP32
+accumulation; they differ by summation order, which can move a value across a
+BF16 rounding boundary or flip a ReLU mask at a near-zero pre-activation, so
+each layer's gradient must agree to 2 % in relative L2 norm (cosine > 0.999).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import rochpcg_b200 as R
+from rochpcg_b200 import learned as LS
+from rochpcg_b200.rhs import normal_rhs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def layers(w):
+    n = 27 * 256
+    return w[:n], w[n:2 * n], w[2 * n:]
+
+
+def test_normal_rhs_device_matches_python():
+    L = R.load()
+    m = 100_003
+    out = torch.empty(m, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.hpcgb200_normal_rhs(m, 9999, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)) == 0
+    torch.cuda.synchronize()
+    ref = normal_rhs(m, 9999)
+    got = out.cpu().numpy()
+    # same integer stream; log/cos may round differently by an ulp or two
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("dims,nb", [((6, 9, 20), 2), ((16, 16, 16), 1), ((8, 8, 8), 4)])
+def test_forward_matches_oracle(dims, nb):
+    rng = np.random.default_rng(1)
+    per = int(np.prod(dims))
+    w = LS.jacobi_weights(0.8, 0.1, 3)
+    S = LS.Smoother(w)
+    r = rng.standard_normal(nb * per).astype(np.float32)
+    y = S.forward(dev(r), dims, nb)
+    torch.cuda.synchronize()
+    got = y.cpu().numpy()
+    w1, w2, w3 = layers(w)
+    ref = np.concatenate([O.net_forward(dims, w1, w2, w3, r[b * per:(b + 1) * per])[0] for b in range(nb)])
+    assert np.linalg.norm(got - ref) <= 1e-2 * np.linalg.norm(ref)
+    assert np.max(np.abs(got - ref)) <= 5e-2 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("dims,nb", [((6, 9, 20), 2), ((12, 12, 12), 3)])
+def test_gradients_match_oracle(dims, nb):
+    rng = np.random.default_rng(2)
+    per = int(np.prod(dims))
+    w = LS.jacobi_weights(0.8, 0.15, 5)
+    S = LS.Smoother(w)
+    r = rng.standard_normal(nb * per).astype(np.float32)
+    e = (rng.standard_normal(nb * per) * 0.05).astype(np.float32)
+    inv = np.array([1.0 / np.sum(e[b * per:(b + 1) * per].astype(np.float64) ** 2) for b in range(nb)], np.float32)
+    scale = 1.0 / nb
+    loss, dw = S.loss_grad(dev(r), dev(e), dev(inv), dims, nb, scale)
+    torch.cuda.synchronize()
+    got = dw.cpu().numpy()
+    w1, w2, w3 = layers(w)
+    ref_loss = 0.0
+    ref = np.zeros(3 * 27 * 256)
+    for b in range(nb):
+        sl = slice(b * per, (b + 1) * per)
+        lb, gb = O.net_loss_grad(dims, w1, w2, w3, r[sl], e[sl])
+        ref_loss += scale * lb
+        ref += scale * np.concatenate(gb)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss
+    for a, b in zip(layers(got), layers(ref)):
+        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b)
+        assert np.dot(a, b) >= 0.999 * np.linalg.norm(a) * np.linalg.norm(b)
+    # structural zeros stay zero: layer 1 has one input channel, layer 3 one output channel
+    g1 = layers(got)[0].reshape(27, 16, 16)
+    g3 = layers(got)[2].reshape(27, 16, 16)
+    assert np.all(g1[:, 1:, :] == 0) and np.all(g3[:, :, 1:] == 0)
+
+
+def test_training_pairs_match_oracle_vcycle():
+    P = LS.make_pairs(32, 2, 41, 3, tol=1e-10)
+    torch.cuda.synchronize()
+    n = 8
+    per = n ** 3
+    C = O.ColoredProblem(32, 32, 32)
+    L0, L1, L2 = C.levels[0], C.levels[1], C.levels[2]
+    rs, es = P.r.cpu().numpy(), P.e.cpu().numpy()
+    inv = P.inv_ee.cpu().numpy()
+    for i in range(3):
+        b = L0.permute(normal_rhs(L0.m, 41 + i))
+        x0 = L0.symgs_zero(b)
+        r1 = C.restrict_fused(0, b, x0)
+        x1 = L1.symgs_zero(r1)
+        r2 = L2.unpermute(C.restrict_fused(1, r1, x1))
+        r = rs[i * per:(i + 1) * per].astype(np.float64)
+        assert np.linalg.norm(r - r2) <= 1e-5 * np.linalg.norm(r2)  # FP32 device leg vs FP64 oracle leg
+        e = es[i * per:(i + 1) * per].astype(np.float64)
+        Ae = L2.unpermute(L2.spmv(L2.permute(e)))
+        assert np.linalg.norm(Ae - r) <= 1e-5 * np.linalg.norm(r)  # e is the level's exact correction
+        assert abs(inv[i] * np.sum(e * e) - 1.0) < 1e-5
+
+
+def test_training_reduces_loss_and_is_deterministic():
+    P = LS.make_pairs(32, 2, 1, 32, batch=8)
+    w0 = LS.jacobi_weights(1.0, 0.02, 7)
+    S = LS.Smoother(w0)
+    hist = S.train([P], epochs=25, lr0=3e-3, lr1=5e-4, seed=1)
+    assert hist[-1] < 0.8 * hist[0], hist
+    w1 = S.get_weights()
+    S2 = LS.Smoother(w0)
+    S2.train([P], epochs=25, lr0=3e-3, lr1=5e-4, seed=1)
+    assert np.array_equal(w1, S2.get_weights())
+
+
+def test_learned_cg_converges_and_falls_back():
+    Pr = R.Problem(64, 64, 64)
+    Pr.set_rhs(normal_rhs(Pr.rows[0], 9999))
+    S = LS.Smoother(LS.jacobi_weights(1.0, 0.0, 0))
+    Pr.set_smoother(S, 2)
+    r = Pr.cg(500, 1e-9, mode=R.MODE_LEARNED)
+    assert r["normr"] / r["normr0"] <= 1e-9
+    assert Pr.true_residual() <= 2e-9
+    # a smoother that amplifies the residual (planted on the host): the solve
+    # falls back to SymGS at the first iteration that fails and still converges
+    bad = LS.Smoother(LS.jacobi_weights(-40.0, 0.0, 0))
+    Pr.set_smoother(bad, 2)
+    r2 = Pr.cg(500, 1e-9, mode=R.MODE_LEARNED)
+    fb = Pr.last_fallback()
+    assert fb >= 1
+    assert r2["normr"] / r2["normr0"] <= 1e-9
+    assert Pr.true_residual() <= 2e-9
+    h = r2["hist"]
+    assert all(h[k] < h[k - 1] for k in range(1, fb))
+    assert h[fb] >= h[fb - 1]
+    mixed = Pr.cg(500, 1e-9, mode=R.MODE_MIXED)
+    assert Pr.last_fallback() == 0
+    assert r2["niters"] <= 2 * mixed["niters"]
+    Pr.set_smoother(None)
