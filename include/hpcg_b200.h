@@ -310,12 +310,19 @@ int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsig
 /* y = N(r) for nb samples of nz x ny x nx points. */
 int hpcgb200_smoother_forward(hpcgb200_smoother* s, int nb, int nz, int ny, int nx, const float* r, float* y,
                               void* stream);
-/* loss = scale * sum_b ||N(r_b) - e_b||^2 * inv_ee[b] (inv_ee: device, nb
- * floats) and its gradient with respect to the weights, copied to dw (device,
+/* odd != 0: the network is evaluated as (N(r) - N(-r)) / 2, an odd function
+ * of r (both branches run as one batch of two); the default is N(r). */
+int hpcgb200_smoother_configure(hpcgb200_smoother* s, int odd);
+/* loss = scale * sum_b d_b.M d_b * inv_norm[b], d = y - e with y the network
+ * output; kind 0: M = I, kind 1: M = the 27-point stencil A (energy norm).
+ * inv_norm (device, nb floats) = 1/(e.e) or 1/(e.Ae): hpcgb200_sample_norms.
+ * The gradient with respect to the weights is copied to dw (device,
  * HPCGB200_SMOOTHER_WEIGHTS floats) when not NULL; the handle keeps it for
  * hpcgb200_smoother_adam_step.  *loss (host) may be NULL. */
 int hpcgb200_smoother_loss_grad(hpcgb200_smoother* s, int nb, int nz, int ny, int nx, const float* r, const float* e,
-                                const float* inv_ee, float scale, float* dw, double* loss, void* stream);
+                                const float* inv_norm, float scale, int kind, float* dw, double* loss, void* stream);
+/* out[b] = 1/(e_b.e_b) (kind 0) or 1/(e_b.A e_b) (kind 1) for nb samples. */
+int hpcgb200_sample_norms(int nb, int nz, int ny, int nx, const float* e, int kind, float* out, void* stream);
 /* One bias-corrected Adam step with the last gradient. */
 int hpcgb200_smoother_adam_step(hpcgb200_smoother* s, float lr, float beta1, float beta2, float eps, void* stream);
 
@@ -329,11 +336,12 @@ typedef struct
     int count, nz, ny, nx, batch;
 } hpcgb200_pair_set;
 /* Adam training over the sets for `epochs` passes (batches of all sets in a
- * seeded shuffled order; learning rate geometric from lr0 to lr1; loss per
- * sample relative to ||e||^2).  epoch_loss (host, may be NULL): mean loss of
- * each epoch. */
+ * seeded shuffled order; learning rate geometric from lr0 to lr1; per-sample
+ * loss of hpcgb200_smoother_loss_grad with the given kind, relative to the
+ * sample's e.e or e.Ae).  epoch_loss (host, may be NULL): mean loss of each
+ * epoch. */
 int hpcgb200_smoother_train(hpcgb200_smoother* s, const hpcgb200_pair_set* sets, int nsets, int epochs, float lr0,
-                            float lr1, unsigned long long seed, double* epoch_loss, void* stream);
+                            float lr1, int kind, unsigned long long seed, double* epoch_loss, void* stream);
 /* Training pairs from the plain FP32 V-cycle: for seeds first_seed ..
  * first_seed+count-1, b ~ N(0,1) (hpcgb200_normal_rhs) on a fine_n^3 grid;
  * r = the residual the V-cycle hands to MG level `level`, e = A_level^-1 r

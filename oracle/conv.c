@@ -120,47 +120,128 @@ void oc_net_forward(int nz, int ny, int nx, const float* w1, const float* w2, co
     free(p);
 }
 
-double oc_net_loss_grad(int nz, int ny, int nx, const float* w1, const float* w2, const float* w3, const float* r,
-                        const float* e, float* dw1, float* dw2, float* dw3, int round)
+/* Backward of one network evaluation (input r, stored activations a1, a2)
+ * for the output gradient g (scalar field): adds the weight gradients. */
+static void branch_backward(int nz, int ny, int nx, const float* w2, const float* w3, const float* r,
+                            const float* a1, const float* a2, const float* gs, float* dw1, float* dw2, float* dw3,
+                            int round)
 {
     const long n = (long)nz * ny * nx;
-    float* y = (float*)malloc(sizeof(float) * (size_t)n);
-    float* a1 = (float*)malloc(sizeof(float) * (size_t)n * CH);
-    float* a2 = (float*)malloc(sizeof(float) * (size_t)n * CH);
-    oc_net_forward(nz, ny, nx, w1, w2, w3, r, y, a1, a2, round);
-    double ee = 0.0, rr = 0.0;
-    for(long i = 0; i < n; ++i)
-    {
-        ee += (double)e[i] * e[i];
-        rr += ((double)y[i] - e[i]) * ((double)y[i] - e[i]);
-    }
-    const double loss = rr / ee;
-    /* dL/dy = 2 (y - e) / sum e^2 */
     float* g = (float*)calloc((size_t)n * CH, sizeof(float));
-    for(long i = 0; i < n; ++i) g[i * CH] = (float)(2.0 * ((double)y[i] - e[i]) / ee);
     float* wt = (float*)malloc(sizeof(float) * 27 * CH * CH);
     float* d = (float*)malloc(sizeof(float) * (size_t)n * CH);
-    float* a0 = (float*)calloc((size_t)n * CH, sizeof(float));
-    for(long i = 0; i < n; ++i) a0[i * CH] = r[i];
-
-    oc_conv16_wgrad(nz, ny, nx, a2, g, dw3, round);
-    oc_flip_transpose(w3, wt);
-    oc_conv16(nz, ny, nx, g, wt, d, round); /* d = dL/da2 */
-    for(long i = 0; i < n * CH; ++i) d[i] = a2[i] > 0.f ? d[i] : 0.f;
-    oc_conv16_wgrad(nz, ny, nx, a1, d, dw2, round);
-    oc_flip_transpose(w2, wt);
     float* d1 = (float*)malloc(sizeof(float) * (size_t)n * CH);
+    float* a0 = (float*)calloc((size_t)n * CH, sizeof(float));
+    float* dw = (float*)malloc(sizeof(float) * 27 * CH * CH);
+    for(long i = 0; i < n; ++i)
+    {
+        g[i * CH] = gs[i];
+        a0[i * CH] = r[i];
+    }
+    oc_conv16_wgrad(nz, ny, nx, a2, g, dw, round);
+    for(int i = 0; i < 27 * CH * CH; ++i) dw3[i] += dw[i];
+    oc_flip_transpose(w3, wt);
+    oc_conv16(nz, ny, nx, g, wt, d, round); /* dL/da2 */
+    for(long i = 0; i < n * CH; ++i) d[i] = a2[i] > 0.f ? d[i] : 0.f;
+    oc_conv16_wgrad(nz, ny, nx, a1, d, dw, round);
+    for(int i = 0; i < 27 * CH * CH; ++i) dw2[i] += dw[i];
+    oc_flip_transpose(w2, wt);
     oc_conv16(nz, ny, nx, d, wt, d1, round); /* dL/da1 */
     for(long i = 0; i < n * CH; ++i) d1[i] = a1[i] > 0.f ? d1[i] : 0.f;
-    oc_conv16_wgrad(nz, ny, nx, a0, d1, dw1, round);
-
-    free(y);
-    free(a1);
-    free(a2);
+    oc_conv16_wgrad(nz, ny, nx, a0, d1, dw, round);
+    for(int i = 0; i < 27 * CH * CH; ++i) dw1[i] += dw[i];
     free(g);
     free(wt);
     free(d);
     free(d1);
     free(a0);
-    return loss;
+    free(dw);
+}
+
+/* 27-point stencil A (diagonal 26, off-diagonals -1, zero outside the grid). */
+void oc_stencil_apply(int nz, int ny, int nx, const float* v, float* out)
+{
+    for(int z = 0; z < nz; ++z)
+        for(int y = 0; y < ny; ++y)
+            for(int x = 0; x < nx; ++x)
+            {
+                const long p = ((long)z * ny + y) * nx + x;
+                float off = 0.f;
+                for(int t = 0; t < 27; ++t)
+                {
+                    const int z2 = z + t / 9 - 1, y2 = y + (t / 3) % 3 - 1, x2 = x + t % 3 - 1;
+                    if(t != 13 && z2 >= 0 && z2 < nz && y2 >= 0 && y2 < ny && x2 >= 0 && x2 < nx)
+                        off += v[((long)z2 * ny + y2) * nx + x2];
+                }
+                out[p] = 26.f * v[p] - off;
+            }
+}
+
+double oc_net_loss_grad2(int nz, int ny, int nx, const float* w1, const float* w2, const float* w3, const float* r,
+                         const float* e, float* dw1, float* dw2, float* dw3, int round, int odd, int kind)
+{
+    const long n = (long)nz * ny * nx;
+    float* yp = (float*)malloc(sizeof(float) * (size_t)n);
+    float* ym = (float*)malloc(sizeof(float) * (size_t)n);
+    float* rm = (float*)malloc(sizeof(float) * (size_t)n);
+    float* a1p = (float*)malloc(sizeof(float) * (size_t)n * CH);
+    float* a2p = (float*)malloc(sizeof(float) * (size_t)n * CH);
+    float* a1m = (float*)malloc(sizeof(float) * (size_t)n * CH);
+    float* a2m = (float*)malloc(sizeof(float) * (size_t)n * CH);
+    float* d = (float*)malloc(sizeof(float) * (size_t)n);
+    float* md = (float*)malloc(sizeof(float) * (size_t)n);
+    float* me = (float*)malloc(sizeof(float) * (size_t)n);
+    float* gs = (float*)malloc(sizeof(float) * (size_t)n);
+    oc_net_forward(nz, ny, nx, w1, w2, w3, r, yp, a1p, a2p, round);
+    if(odd)
+    {
+        for(long i = 0; i < n; ++i) rm[i] = -r[i];
+        oc_net_forward(nz, ny, nx, w1, w2, w3, rm, ym, a1m, a2m, round);
+    }
+    for(long i = 0; i < n; ++i) d[i] = (odd ? 0.5f * (yp[i] - ym[i]) : yp[i]) - e[i];
+    if(kind)
+    {
+        oc_stencil_apply(nz, ny, nx, d, md);
+        oc_stencil_apply(nz, ny, nx, e, me);
+    }
+    else
+    {
+        memcpy(md, d, sizeof(float) * (size_t)n);
+        memcpy(me, e, sizeof(float) * (size_t)n);
+    }
+    double num = 0.0, den = 0.0;
+    for(long i = 0; i < n; ++i)
+    {
+        num += (double)d[i] * md[i];
+        den += (double)e[i] * me[i];
+    }
+    memset(dw1, 0, sizeof(float) * 27 * CH * CH);
+    memset(dw2, 0, sizeof(float) * 27 * CH * CH);
+    memset(dw3, 0, sizeof(float) * 27 * CH * CH);
+    /* dL/dy = 2 M d / den, split +/- half over the two branches when odd */
+    for(long i = 0; i < n; ++i) gs[i] = (float)((odd ? 1.0 : 2.0) * md[i] / den);
+    branch_backward(nz, ny, nx, w2, w3, r, a1p, a2p, gs, dw1, dw2, dw3, round);
+    if(odd)
+    {
+        for(long i = 0; i < n; ++i) gs[i] = -gs[i];
+        branch_backward(nz, ny, nx, w2, w3, rm, a1m, a2m, gs, dw1, dw2, dw3, round);
+    }
+    free(yp);
+    free(ym);
+    free(rm);
+    free(a1p);
+    free(a2p);
+    free(a1m);
+    free(a2m);
+    free(d);
+    free(md);
+    free(me);
+    free(gs);
+    return num / den;
+}
+
+double oc_net_loss_grad(int nz, int ny, int nx, const float* w1, const float* w2, const float* w3, const float* r,
+                        const float* e, float* dw1, float* dw2, float* dw3, int round)
+{
+    return oc_net_loss_grad2(nz, ny, nx, w1, w2, w3, r, e, dw1, dw2, dw3, round, 0, 0);
 }

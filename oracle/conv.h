@@ -26,6 +26,12 @@ void oc_net_forward(int nz, int ny, int nx, const float* w1, const float* w2, co
 /* loss = ||y - e||^2 / ||e||^2 and its weight gradients */
 double oc_net_loss_grad(int nz, int ny, int nx, const float* w1, const float* w2, const float* w3, const float* r,
                         const float* e, float* dw1, float* dw2, float* dw3, int round);
+/* Same with options: odd != 0 evaluates y = (N(r) - N(-r)) / 2; kind 1 uses
+ * the energy norm of the 27-point stencil A: loss = (y-e).A(y-e) / e.Ae. */
+double oc_net_loss_grad2(int nz, int ny, int nx, const float* w1, const float* w2, const float* w3, const float* r,
+                         const float* e, float* dw1, float* dw2, float* dw3, int round, int odd, int kind);
+/* out = A v for the 27-point stencil (diagonal 26, off-diagonals -1). */
+void oc_stencil_apply(int nz, int ny, int nx, const float* v, float* out);
 
 #ifdef __cplusplus
 }

@@ -222,6 +222,9 @@ def colored_lib():
         L.oc_net_forward.argtypes = [ctypes.c_int] * 3 + [vp] * 7 + [ctypes.c_int]
         L.oc_net_loss_grad.argtypes = [ctypes.c_int] * 3 + [vp] * 8 + [ctypes.c_int]
         L.oc_net_loss_grad.restype = ctypes.c_double
+        L.oc_net_loss_grad2.argtypes = [ctypes.c_int] * 3 + [vp] * 8 + [ctypes.c_int] * 3
+        L.oc_net_loss_grad2.restype = ctypes.c_double
+        L.oc_stencil_apply.argtypes = [ctypes.c_int] * 3 + [vp, vp]
         _oc_lib = L
     return _oc_lib
 
@@ -414,12 +417,21 @@ def net_forward(dims, w1, w2, w3, r, round_=True):
     return y, a1, a2
 
 
-def net_loss_grad(dims, w1, w2, w3, r, e, round_=True):
+def net_loss_grad(dims, w1, w2, w3, r, e, round_=True, odd=False, kind=0):
+    """Loss and weight gradients; odd: y = (N(r) - N(-r)) / 2; kind 1: energy norm of the stencil."""
     nz, ny, nx = dims
     r = np.ascontiguousarray(r, np.float32)
     e = np.ascontiguousarray(e, np.float32)
     ws = [np.ascontiguousarray(w, np.float32) for w in (w1, w2, w3)]
     d = [np.empty(27 * 256, np.float32) for _ in range(3)]
-    loss = colored_lib().oc_net_loss_grad(nz, ny, nx, *[_ptr(w) for w in ws], _ptr(r), _ptr(e),
-                                          *[_ptr(x) for x in d], int(round_))
+    loss = colored_lib().oc_net_loss_grad2(nz, ny, nx, *[_ptr(w) for w in ws], _ptr(r), _ptr(e),
+                                           *[_ptr(x) for x in d], int(round_), int(odd), int(kind))
     return loss, d
+
+
+def stencil_apply(dims, v):
+    nz, ny, nx = dims
+    v = np.ascontiguousarray(v, np.float32)
+    out = np.empty_like(v)
+    colored_lib().oc_stencil_apply(nz, ny, nx, _ptr(v), _ptr(out))
+    return out

@@ -505,7 +505,7 @@ __device__ __forceinline__ void store_embed(__nv_bfloat16* a, long p, float r0)
 // level vectors at natural point p.
 __global__ void k_embed_level(PermMap pm, int nz, int ny, int nx, const float* __restrict__ r,
                               const float* __restrict__ x, const float* __restrict__ diag32,
-                              __nv_bfloat16* __restrict__ a)
+                              __nv_bfloat16* __restrict__ a, int pair)
 {
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= (long)nz * ny * nx) return;
@@ -527,6 +527,23 @@ __global__ void k_embed_level(PermMap pm, int nz, int ny, int nx, const float* _
         v = v - (diag32[row] * x[row] - off);
     }
     store_embed(a, p, v);
+    if(pair) store_embed(a, p + (long)nz * ny * nx, -v);  // second sample: -v (odd evaluation)
+}
+
+// x[row(p)] = (or +=) (y[p] - y[p + n]) / 2: the odd part of the network.
+template <bool kAdd>
+__global__ void k_odd_combine(PermMap pm, int nz, int ny, int nx, const float* __restrict__ y, float* __restrict__ x)
+{
+    const long n = (long)nz * ny * nx;
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const int z = (int)(p / ((long)ny * nx));
+    const long rem = p - (long)z * ny * nx;
+    const int yy = (int)(rem / nx), xx = (int)(rem - (long)yy * nx);
+    const float v = 0.5f * (y[p] - y[p + n]);
+    float* o = x + perm_row(pm, z, yy, xx);
+    if(kAdd) *o += v;
+    else *o = v;
 }
 
 // Natural <-> colour-permuted copies of a level vector (training-pair set-up).
@@ -590,16 +607,75 @@ __global__ void k_normal_rhs(long long m, unsigned long long seed, const int* __
     if(out32) out32[o] = (float)v;
 }
 
-__global__ void k_embed_f32(long n, const float* __restrict__ r, __nv_bfloat16* __restrict__ a)
+__global__ void k_embed_f32(long n, const float* __restrict__ r, __nv_bfloat16* __restrict__ a, int pair)
 {
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if(p < n) store_embed(a, p, r[p]);
+    if(p >= n) return;
+    store_embed(a, p, r[p]);
+    if(pair) store_embed(a, p + n, -r[p]);
+}
+
+// 27-point stencil (diagonal 26, off-diagonals -1, zero outside the sample's grid).
+__device__ __forceinline__ float stencil_at(const ConvGrid& g, const float* __restrict__ v, long p)
+{
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long b = p / per;
+    const long q = p - b * per;
+    const int z = (int)(q / ((long)g.ny * g.nx));
+    const long rem = q - (long)z * g.ny * g.nx;
+    const int y = (int)(rem / g.nx), x = (int)(rem - (long)y * g.nx);
+    const float* vb = v + b * per;
+    float off = 0.f;
+#pragma unroll
+    for(int t = 0; t < 27; ++t)
+    {
+        const int z2 = z + t / 9 - 1, y2 = y + (t / 3) % 3 - 1, x2 = x + t % 3 - 1;
+        if(t != 13 && z2 >= 0 && z2 < g.nz && y2 >= 0 && y2 < g.ny && x2 >= 0 && x2 < g.nx)
+            off += vb[((long)z2 * g.ny + y2) * g.nx + x2];
+    }
+    return 26.f * v[p] - off;
+}
+
+// out[p] = (y[p] - y[p + n]) / 2 (natural order).
+__global__ void k_odd_natural(long n, const float* __restrict__ y, float* __restrict__ out)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p < n) out[p] = 0.5f * (y[p] - y[p + n]);
+}
+
+// 1 / (e.e) (kind 0) or 1 / (e.Ae) (kind 1) per sample: one block per sample.
+__global__ void k_sample_norm(ConvGrid g, const float* __restrict__ e, int kind, float* __restrict__ out)
+{
+    __shared__ double red[32];
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long base = (long)blockIdx.x * per;
+    double s = 0.0;
+    for(long i = threadIdx.x; i < per; i += blockDim.x)
+    {
+        const float ev = e[base + i];
+        s += (double)ev * (kind ? stencil_at(g, e, base + i) : ev);
+    }
+    s = block_sum(s, red);
+    if(threadIdx.x == 0) out[blockIdx.x] = (float)(1.0 / s);
+}
+
+// d = y - e, y the network output (odd: (y[p] - y[p + n]) / 2).
+__global__ void k_loss_diff(long n, const float* __restrict__ y, const float* __restrict__ e, int odd,
+                            float* __restrict__ d)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const float yv = odd ? 0.5f * (y[p] - y[p + n]) : y[p];
+    d[p] = yv - e[p];
 }
 
 constexpr int kLossBlocks = 1184;
 
-__global__ void __launch_bounds__(256) k_loss_grad(ConvGrid g, const float* __restrict__ y, const float* __restrict__ e,
-                                                   const float* __restrict__ inv_ee, float scale,
+// Loss terms d.Md * w (M = I for kind 0, the stencil A for kind 1, i.e. the
+// error's energy norm) and the output gradient 2 M d w as BF16 channel 0 of
+// G (odd: +/- half of it for the two branches).
+__global__ void __launch_bounds__(256) k_loss_grad(ConvGrid g, const float* __restrict__ d,
+                                                   const float* __restrict__ wnorm, float scale, int kind, int odd,
                                                    __nv_bfloat16* __restrict__ G, float* __restrict__ loss_partial)
 {
     __shared__ float red[32];
@@ -608,10 +684,19 @@ __global__ void __launch_bounds__(256) k_loss_grad(ConvGrid g, const float* __re
     float acc = 0.f;
     for(long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
     {
-        const float w = inv_ee[p / per] * scale;
-        const float d = y[p] - e[p];
-        acc += d * d * w;
-        store_embed(G, p, 2.f * d * w);
+        const float w = wnorm[p / per] * scale;
+        const float md = kind ? stencil_at(g, d, p) : d[p];
+        acc += d[p] * md * w;
+        const float gv = 2.f * md * w;
+        if(odd)
+        {
+            store_embed(G, p, 0.5f * gv);
+            store_embed(G, p + n, -0.5f * gv);
+        }
+        else
+        {
+            store_embed(G, p, gv);
+        }
     }
     acc = block_sum(acc, red);
     if(threadIdx.x == 0) loss_partial[blockIdx.x] = acc;
@@ -714,10 +799,34 @@ int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s)
 }
 
 int launch_embed_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
-                       const float* diag32, void* a, cudaStream_t s)
+                       const float* diag32, void* a, int pair, cudaStream_t s)
 {
     const long n = (long)nz * ny * nx;
-    k_embed_level<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, x, diag32, (__nv_bfloat16*)a);
+    k_embed_level<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, x, diag32, (__nv_bfloat16*)a,
+                                                              pair);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_odd_combine(const PermMap& pm, int nz, int ny, int nx, const float* y, float* x, bool add, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    if(add) k_odd_combine<true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, y, x);
+    else k_odd_combine<false><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, y, x);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_odd_natural(long n, const float* y, float* out, cudaStream_t s)
+{
+    k_odd_natural<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, y, out);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_sample_norm(const ConvGrid& g, const float* e, int kind, float* out, cudaStream_t s)
+{
+    k_sample_norm<<<g.nb, 512, 0, s>>>(g, e, kind, out);
     HB_LAUNCHED();
     return 0;
 }
@@ -768,9 +877,9 @@ int launch_normal_rhs(long long m, unsigned long long seed, const int* perm, dou
     return 0;
 }
 
-int launch_embed_f32(long n, const float* r, void* a, cudaStream_t s)
+int launch_embed_f32(long n, const float* r, void* a, int pair, cudaStream_t s)
 {
-    k_embed_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, r, (__nv_bfloat16*)a);
+    k_embed_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, r, (__nv_bfloat16*)a, pair);
     HB_LAUNCHED();
     return 0;
 }
@@ -781,10 +890,13 @@ int loss_parts(long points)
     return kLossBlocks;
 }
 
-int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, const float* inv_ee, float scale, void* G,
-                     float* loss_partial, cudaStream_t s)
+int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, float* d, const float* wnorm, float scale,
+                     int kind, int odd, void* G, float* loss_partial, cudaStream_t s)
 {
-    k_loss_grad<<<kLossBlocks, 256, 0, s>>>(g, y, e, inv_ee, scale, (__nv_bfloat16*)G, loss_partial);
+    const long n = g.points();
+    k_loss_diff<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, y, e, odd, d);
+    HB_LAUNCHED();
+    k_loss_grad<<<kLossBlocks, 256, 0, s>>>(g, d, wnorm, scale, kind, odd, (__nv_bfloat16*)G, loss_partial);
     HB_LAUNCHED();
     return 0;
 }
@@ -848,4 +960,10 @@ extern "C" int hpcgb200_normal_rhs(long long m, unsigned long long seed, double*
     HB_CHECK_ARG(m >= 0 && (m == 0 || out), "bad arguments");
     if(m == 0) return 0;
     return launch_normal_rhs(m, seed, nullptr, out, nullptr, as_stream(stream));
+}
+
+extern "C" int hpcgb200_sample_norms(int nb, int nz, int ny, int nx, const float* e, int kind, float* out, void* stream)
+{
+    HB_CHECK_ARG(nb > 0 && nz > 0 && ny > 0 && nx > 0 && e && out && (kind == 0 || kind == 1), "bad arguments");
+    return launch_sample_norm(ConvGrid{nb, nz, ny, nx}, e, kind, out, as_stream(stream));
 }

@@ -58,9 +58,17 @@ int launch_conv16_wgrad(const ConvGrid& g, const void* x, const void* gr, float*
 // BF16 16-channel tensor whose channel 0 is a scalar field (others zero):
 // from colour-permuted FP32 level vectors (r, or the residual r - A x when x
 // is not null), or from an FP32 natural field.
+// pair != 0 also writes the negated field as a second sample right after the
+// first (the odd evaluation N(v) - N(-v) as one batch of two).
 int launch_embed_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
-                       const float* diag32, void* a, cudaStream_t s);
-int launch_embed_f32(long n, const float* r, void* a, cudaStream_t s);
+                       const float* diag32, void* a, int pair, cudaStream_t s);
+int launch_embed_f32(long n, const float* r, void* a, int pair, cudaStream_t s);
+// x[row(p)] = (or +=) (y[p] - y[p + n]) / 2.
+int launch_odd_combine(const PermMap& pm, int nz, int ny, int nx, const float* y, float* x, bool add, cudaStream_t s);
+// out[p] = (y[p] - y[p + n]) / 2.
+int launch_odd_natural(long n, const float* y, float* out, cudaStream_t s);
+// out[b] = 1 / (e_b . e_b) (kind 0) or 1 / (e_b . A e_b) (kind 1, 27-point stencil).
+int launch_sample_norm(const ConvGrid& g, const float* e, int kind, float* out, cudaStream_t s);
 
 // Natural <-> colour-permuted copies of level vectors.
 int launch_natural_from_perm(const PermMap& pm, int nz, int ny, int nx, const float* in, float* out, cudaStream_t s);
@@ -75,12 +83,14 @@ int launch_loss_accumulate(const float* partial, double* acc, cudaStream_t s);
 int launch_normal_rhs(long long m, unsigned long long seed, const int* perm, double* out64, float* out32,
                       cudaStream_t s);
 
-// Loss of a batch: sum_b ||y_b - e_b||^2 * inv_ee[b] * scale (per-block
-// partial sums, `loss_partial` of loss_parts(points) floats) and its
-// gradient 2 (y - e) inv_ee[b] scale as BF16 channel 0 of G.
+// Loss of a batch: sum_b d_b.M d_b * wnorm[b] * scale with d = y - e (y the
+// odd part (y[p] - y[p+n])/2 when odd), M = I (kind 0) or the stencil A
+// (kind 1), as per-block partial sums (`loss_partial`, loss_parts(points)
+// floats), and its gradient 2 M d wnorm scale as BF16 channel 0 of G (odd:
+// +/- half for the two branches).  d: scratch of g.points() floats.
 int loss_parts(long points);
-int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, const float* inv_ee, float scale, void* G,
-                     float* loss_partial, cudaStream_t s);
+int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, float* d, const float* wnorm, float scale,
+                     int kind, int odd, void* G, float* loss_partial, cudaStream_t s);
 
 // One Adam step on n parameters (bias-corrected, step t >= 1).
 int launch_adam(int n, float* w, const float* dw, float* m, float* v, float lr, float beta1, float beta2, float eps,

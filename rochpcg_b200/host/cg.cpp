@@ -185,7 +185,7 @@ int iteration_kernels(const SparseMatrix& A, CGData& data, const Vector& b, Vect
     if(prec == MGPrecision::LEARNED)
     {
         if(!o->smoother) throw Error(HPCGB200_ERR_ARG, "learned CG: no smoother attached to the problem");
-        check(smoother_prepare(*o->smoother, rt().stream));
+        check(smoother_ready(A, rt().stream));
     }
     return get_graph(A, data, b, x, precond, prec, flexible)->kernels_per_iteration;
 }
@@ -221,7 +221,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         h.net = prec == MGPrecision::LEARNED ? 1 : 0;
         if(prec == MGPrecision::LEARNED && !o->smoother)
             return hb::record_error(HPCGB200_ERR_ARG, "learned CG: no smoother attached to the problem");
-        if(prec == MGPrecision::LEARNED) check(smoother_prepare(*o->smoother, s));
+        if(prec == MGPrecision::LEARNED) check(smoother_ready(A, s));
         cudaEvent_t e0, e1;
         HB_HOST_CUDA(cudaEventCreate(&e0));
         HB_HOST_CUDA(cudaEventCreate(&e1));

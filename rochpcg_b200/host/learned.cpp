@@ -36,13 +36,21 @@ Smoother::Smoother()
 
 Smoother::~Smoother()
 {
-    for(void* p : {(void*)w, (void*)wB, (void*)wT, a0, a1, a2, g, d, (void*)y, (void*)dw, (void*)adam_m,
-                   (void*)adam_v, (void*)partial, (void*)loss_partial, (void*)loss_acc, (void*)status})
+    for(void* p : {(void*)w, (void*)wB, (void*)wT, a0, a1, a2, g, d, (void*)y, (void*)dbuf, (void*)dw,
+                   (void*)adam_m, (void*)adam_v, (void*)partial, (void*)loss_partial, (void*)loss_acc, (void*)status})
         dfree(p);
+}
+
+void smoother_configure(Smoother& S, bool odd)
+{
+    if(S.odd == odd) return;
+    S.odd = odd;
+    S.cap = 0;  // branch count changed: reallocate on next use
 }
 
 void smoother_reserve(Smoother& S, long points, bool training)
 {
+    const long br = S.odd ? 2 : 1;  // network evaluations per grid point
     const bool grow = points > S.cap;
     if(grow)
     {
@@ -52,21 +60,24 @@ void smoother_reserve(Smoother& S, long points, bool training)
             *p = nullptr;
         }
         dfree(S.y);
+        dfree(S.dbuf);
         S.y = nullptr;
-        S.a0 = dalloc<uint4>((size_t)points * 2);
-        S.a1 = dalloc<uint4>((size_t)points * 2);
-        S.a2 = dalloc<uint4>((size_t)points * 2);
+        S.dbuf = nullptr;
+        S.a0 = dalloc<uint4>((size_t)points * br * 2);
+        S.a1 = dalloc<uint4>((size_t)points * br * 2);
+        S.a2 = dalloc<uint4>((size_t)points * br * 2);
+        S.y = dalloc<float>((size_t)points * br);
         S.cap = points;
         S.epoch += 1;  // solve graphs that captured the old buffers are stale
     }
     if(!training) return;
     if(!S.g)
     {
-        S.g = dalloc<uint4>((size_t)S.cap * 2);
-        S.d = dalloc<uint4>((size_t)S.cap * 2);
-        S.y = dalloc<float>((size_t)S.cap);
+        S.g = dalloc<uint4>((size_t)S.cap * br * 2);
+        S.d = dalloc<uint4>((size_t)S.cap * br * 2);
+        S.dbuf = dalloc<float>((size_t)S.cap);
     }
-    const size_t pf = hb::kNetLayerWeights * (size_t)hb::conv16_wgrad_parts(S.cap);
+    const size_t pf = hb::kNetLayerWeights * (size_t)hb::conv16_wgrad_parts(S.cap * br);
     if(pf > S.partial_floats)
     {
         dfree(S.partial);
@@ -120,38 +131,48 @@ static const void* tiles_t(const Smoother& S, int layer) { return S.wT + layer *
 int smoother_level_apply(Smoother& S, const LevelOpt& o, const float* r, float* x, bool residual, cudaStream_t s)
 {
     const hb::StencilLevel& L = o.st;
-    const hb::ConvGrid g{1, L.nz, L.ny, L.nx};
-    if(g.points() > S.cap) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: buffers not reserved");
+    const hb::ConvGrid g{S.odd ? 2 : 1, L.nz, L.ny, L.nx};
+    if((long)L.nz * L.ny * L.nx > S.cap)
+        return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: buffers not reserved");
     if(S.tiles_stale) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: weights not prepared");
-    HB_RETURN_IF(hb::launch_embed_level(o.pm, L.nz, L.ny, L.nx, r, residual ? x : nullptr, o.diag32, S.a0, s));
+    HB_RETURN_IF(hb::launch_embed_level(o.pm, L.nz, L.ny, L.nx, r, residual ? x : nullptr, o.diag32, S.a0,
+                                        S.odd ? 1 : 0, s));
     HB_RETURN_IF(hb::launch_conv16(g, S.a0, tiles(S, 0), hb::kOutReluBf16, S.a1, nullptr, nullptr, S.status, s));
     HB_RETURN_IF(hb::launch_conv16(g, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
-    return hb::launch_conv16(g, S.a2, tiles(S, 2), residual ? hb::kOutPermAdd : hb::kOutPermSet, x, nullptr, &o.pm,
-                             S.status, s);
+    if(!S.odd)
+        return hb::launch_conv16(g, S.a2, tiles(S, 2), residual ? hb::kOutPermAdd : hb::kOutPermSet, x, nullptr,
+                                 &o.pm, S.status, s);
+    HB_RETURN_IF(hb::launch_conv16(g, S.a2, tiles(S, 2), hb::kOutF32C0, S.y, nullptr, nullptr, S.status, s));
+    return hb::launch_odd_combine(o.pm, L.nz, L.ny, L.nx, S.y, x, residual, s);
 }
 
+// Raw network output of a batch into y (both branches, 2 g.nb samples, when odd).
 static int forward_batch(Smoother& S, const hb::ConvGrid& g, const float* r, float* y, cudaStream_t s)
 {
+    const hb::ConvGrid gg{S.odd ? 2 * g.nb : g.nb, g.nz, g.ny, g.nx};
     HB_RETURN_IF(smoother_prepare(S, s));
-    HB_RETURN_IF(hb::launch_embed_f32(g.points(), r, S.a0, s));
-    HB_RETURN_IF(hb::launch_conv16(g, S.a0, tiles(S, 0), hb::kOutReluBf16, S.a1, nullptr, nullptr, S.status, s));
-    HB_RETURN_IF(hb::launch_conv16(g, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
-    return hb::launch_conv16(g, S.a2, tiles(S, 2), hb::kOutF32C0, y, nullptr, nullptr, S.status, s);
+    HB_RETURN_IF(hb::launch_embed_f32(g.points(), r, S.a0, S.odd ? 1 : 0, s));
+    HB_RETURN_IF(hb::launch_conv16(gg, S.a0, tiles(S, 0), hb::kOutReluBf16, S.a1, nullptr, nullptr, S.status, s));
+    HB_RETURN_IF(hb::launch_conv16(gg, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
+    return hb::launch_conv16(gg, S.a2, tiles(S, 2), hb::kOutF32C0, y, nullptr, nullptr, S.status, s);
 }
 
 int smoother_forward(Smoother& S, const hb::ConvGrid& g, const float* r, float* y, cudaStream_t s)
 {
     smoother_reserve(S, g.points(), false);
-    return forward_batch(S, g, r, y, s);
+    if(!S.odd) return forward_batch(S, g, r, y, s);
+    HB_RETURN_IF(forward_batch(S, g, r, S.y, s));
+    return hb::launch_odd_natural(g.points(), S.y, y, s);
 }
 
-int smoother_loss_grad(Smoother& S, const hb::ConvGrid& g, const float* r, const float* e, const float* inv_ee,
-                       float scale, cudaStream_t s)
+int smoother_loss_grad(Smoother& S, const hb::ConvGrid& g0, const float* r, const float* e, const float* wnorm,
+                       float scale, int kind, cudaStream_t s)
 {
-    smoother_reserve(S, g.points(), true);
-    HB_RETURN_IF(forward_batch(S, g, r, S.y, s));
-    HB_RETURN_IF(hb::launch_loss_grad(g, S.y, e, inv_ee, scale, S.g, S.loss_partial, s));
+    smoother_reserve(S, g0.points(), true);
+    HB_RETURN_IF(forward_batch(S, g0, r, S.y, s));
+    HB_RETURN_IF(hb::launch_loss_grad(g0, S.y, e, S.dbuf, wnorm, scale, kind, S.odd ? 1 : 0, S.g, S.loss_partial, s));
     HB_RETURN_IF(hb::launch_loss_accumulate(S.loss_partial, S.loss_acc, s));
+    const hb::ConvGrid g{S.odd ? 2 * g0.nb : g0.nb, g0.nz, g0.ny, g0.nx};
     float* dw1 = S.dw;
     float* dw2 = S.dw + hb::kNetLayerWeights;
     float* dw3 = S.dw + 2 * hb::kNetLayerWeights;
@@ -185,6 +206,16 @@ int smoother_status(Smoother& S, cudaStream_t s)
         return hb::record_error(HPCGB200_ERR_DEVICE_STATUS, "learned smoother: tensor-core wait timed out (%d)", h);
     }
     return 0;
+}
+
+int smoother_ready(const SparseMatrix& A, cudaStream_t s)
+{
+    LevelOpt* o = opt(A);
+    const SparseMatrix* M = &A;
+    for(int l = 0; l < o->smoother_first_level && M; ++l) M = M->Ac;
+    if(!M) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: first level beyond the hierarchy");
+    smoother_reserve(*o->smoother, M->localNumberOfRows, false);
+    return smoother_prepare(*o->smoother, s);
 }
 
 // FP32 V-cycle below level 0 with the learned levels (same recursion as mg_fp32).
@@ -228,7 +259,7 @@ int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
         // reads the tile buffers, which later refreshes update in place)
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         HB_HOST_CUDA(cudaStreamIsCapturing(s, &cs));
-        if(cs == cudaStreamCaptureStatusNone) HB_RETURN_IF(smoother_prepare(S, s));
+        if(cs == cudaStreamCaptureStatusNone) HB_RETURN_IF(smoother_ready(A, s));
         HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r.d_values, o->r32, o->z32, s));
         if(!A.mgData) return hb::launch_cast_f2d(m, o->z32, x.d_values, s);
         const MGOpt* mo = mgopt(A);
@@ -366,18 +397,28 @@ extern "C" int hpcgb200_smoother_forward(hpcgb200_smoother* h, int nb, int nz, i
     });
 }
 
-extern "C" int hpcgb200_smoother_loss_grad(hpcgb200_smoother* h, int nb, int nz, int ny, int nx, const float* r,
-                                           const float* e, const float* inv_ee, float scale, float* dw, double* loss,
-                                           void* stream)
+extern "C" int hpcgb200_smoother_configure(hpcgb200_smoother* h, int odd)
 {
-    if(!h || nb <= 0 || nz <= 0 || ny <= 0 || nx <= 0 || !r || !e || !inv_ee)
+    if(!h) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
+    return guarded([&] {
+        HB_HOST_CUDA(cudaStreamSynchronize(h->stream));
+        smoother_configure(h->S, odd != 0);
+        return 0;
+    });
+}
+
+extern "C" int hpcgb200_smoother_loss_grad(hpcgb200_smoother* h, int nb, int nz, int ny, int nx, const float* r,
+                                           const float* e, const float* inv_norm, float scale, int kind, float* dw,
+                                           double* loss, void* stream)
+{
+    if(!h || nb <= 0 || nz <= 0 || ny <= 0 || nx <= 0 || !r || !e || !inv_norm || (kind != 0 && kind != 1))
         return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     return guarded([&] {
         cudaStream_t s = stream_of(stream);
         Smoother& S = h->S;
         smoother_reserve(S, (long)nb * nz * ny * nx, true);
         HB_HOST_CUDA(cudaMemsetAsync(S.loss_acc, 0, sizeof(double), s));
-        HB_RETURN_IF(smoother_loss_grad(S, hb::ConvGrid{nb, nz, ny, nx}, r, e, inv_ee, scale, s));
+        HB_RETURN_IF(smoother_loss_grad(S, hb::ConvGrid{nb, nz, ny, nx}, r, e, inv_norm, scale, kind, s));
         if(dw)
             HB_HOST_CUDA(cudaMemcpyAsync(dw, S.dw, sizeof(float) * kNetWeights, cudaMemcpyDeviceToDevice, s));
         double l = 0.0;
@@ -396,9 +437,10 @@ extern "C" int hpcgb200_smoother_adam_step(hpcgb200_smoother* h, float lr, float
 }
 
 extern "C" int hpcgb200_smoother_train(hpcgb200_smoother* h, const hpcgb200_pair_set* sets, int nsets, int epochs,
-                                       float lr0, float lr1, unsigned long long seed, double* epoch_loss, void* stream)
+                                       float lr0, float lr1, int kind, unsigned long long seed, double* epoch_loss,
+                                       void* stream)
 {
-    if(!h || !sets || nsets <= 0 || epochs <= 0 || !(lr0 > 0.f) || !(lr1 > 0.f))
+    if(!h || !sets || nsets <= 0 || epochs <= 0 || !(lr0 > 0.f) || !(lr1 > 0.f) || (kind != 0 && kind != 1))
         return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     for(int i = 0; i < nsets; ++i)
         if(!sets[i].r || !sets[i].e || !sets[i].inv_ee || sets[i].count <= 0 || sets[i].batch <= 0 ||
@@ -417,6 +459,22 @@ extern "C" int hpcgb200_smoother_train(hpcgb200_smoother* h, const hpcgb200_pair
         }
         const int nsteps = (int)steps.size();
         smoother_reserve(S, maxpts, true);
+        // per-sample loss normalisation 1/(e.e) or 1/(e.Ae)
+        std::vector<float*> norms(nsets, nullptr);
+        struct Free
+        {
+            std::vector<float*>& v;
+            ~Free()
+            {
+                for(float* p : v) dfree(p);
+            }
+        } free_norms{norms};
+        for(int i = 0; i < nsets; ++i)
+        {
+            norms[i] = dalloc<float>(sets[i].count);
+            check(hb::launch_sample_norm(hb::ConvGrid{sets[i].count, sets[i].nz, sets[i].ny, sets[i].nx}, sets[i].e,
+                                         kind, norms[i], s));
+        }
         Rng rng{seed};
         for(int ep = 0; ep < epochs; ++ep)
         {
@@ -431,8 +489,8 @@ extern "C" int hpcgb200_smoother_train(hpcgb200_smoother* h, const hpcgb200_pair
                 const long per = (long)P.nz * P.ny * P.nx;
                 const long off = (long)st.second * P.batch;
                 const hb::ConvGrid g{P.batch, P.nz, P.ny, P.nx};
-                HB_RETURN_IF(smoother_loss_grad(S, g, P.r + off * per, P.e + off * per, P.inv_ee + off,
-                                                1.f / (float)P.batch, s));
+                HB_RETURN_IF(smoother_loss_grad(S, g, P.r + off * per, P.e + off * per, norms[st.first] + off,
+                                                1.f / (float)P.batch, kind, s));
                 HB_RETURN_IF(smoother_adam(S, lr, 0.9f, 0.999f, 1e-8f, s));
             }
             double l = 0.0;

@@ -82,14 +82,21 @@ def make_pairs(fine_n: int, level: int, first_seed: int, count: int, tol: float 
 class Smoother:
     """Device state of the conv-net smoother (weights, tiles, activations, Adam)."""
 
-    def __init__(self, weights: np.ndarray | None = None):
+    def __init__(self, weights: np.ndarray | None = None, odd: bool = False):
         self.L = load()
         h = ctypes.c_void_p()
         check(self.L, self.L.hpcgb200_smoother_create(ctypes.byref(h)))
         self.h = h
         self.meta: dict = {}
+        self.odd = False
+        self.configure(odd)
         if weights is not None:
             self.set_weights(weights)
+
+    def configure(self, odd: bool):
+        """odd: evaluate (N(r) - N(-r)) / 2, an odd function of the residual."""
+        check(self.L, self.L.hpcgb200_smoother_configure(self.h, int(odd)))
+        self.odd = bool(odd)
 
     def close(self):
         if getattr(self, "h", None):
@@ -119,19 +126,19 @@ class Smoother:
         check(self.L, self.L.hpcgb200_smoother_forward(self.h, nb, nz, ny, nx, _vp(r), _vp(y), _stream()))
         return y
 
-    def loss_grad(self, r, e, inv_ee, dims, nb: int = 1, scale: float = 1.0):
+    def loss_grad(self, r, e, inv_norm, dims, nb: int = 1, scale: float = 1.0, kind: int = 0):
         torch = _torch()
         nz, ny, nx = dims
         dw = torch.empty(WEIGHTS, dtype=torch.float32, device="cuda")
         loss = ctypes.c_double()
-        check(self.L, self.L.hpcgb200_smoother_loss_grad(self.h, nb, nz, ny, nx, _vp(r), _vp(e), _vp(inv_ee), scale,
-                                                         _vp(dw), ctypes.byref(loss), _stream()))
+        check(self.L, self.L.hpcgb200_smoother_loss_grad(self.h, nb, nz, ny, nx, _vp(r), _vp(e), _vp(inv_norm),
+                                                         scale, kind, _vp(dw), ctypes.byref(loss), _stream()))
         return loss.value, dw
 
     def adam_step(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8):
         check(self.L, self.L.hpcgb200_smoother_adam_step(self.h, lr, beta1, beta2, eps, _stream()))
 
-    def train(self, sets: list, epochs: int, lr0: float = 2e-3, lr1: float = 2e-4, seed: int = 0):
+    def train(self, sets: list, epochs: int, lr0: float = 2e-3, lr1: float = 2e-4, seed: int = 0, kind: int = 0):
         """Adam over the pair sets on the device; returns the mean loss of each epoch."""
         torch = _torch()
         cs = (_CPairSet * len(sets))()
@@ -140,21 +147,21 @@ class Smoother:
             cs[i] = _CPairSet(s.r.data_ptr(), s.e.data_ptr(), s.inv_ee.data_ptr(), s.count, nz, ny, nx, s.batch)
         hist = np.zeros(epochs)
         torch.cuda.synchronize()
-        check(self.L, self.L.hpcgb200_smoother_train(self.h, cs, len(sets), epochs, lr0, lr1, seed,
+        check(self.L, self.L.hpcgb200_smoother_train(self.h, cs, len(sets), epochs, lr0, lr1, kind, seed,
                                                      hist.ctypes.data_as(ctypes.c_void_p), None))
         return hist
 
     # -- weight files -------------------------------------------------------
     def save(self, path: str, **meta):
         w = self.get_weights()
-        meta = dict(meta, sha256=hashlib.sha256(w.tobytes()).hexdigest())
+        meta = dict(meta, odd=self.odd, sha256=hashlib.sha256(w.tobytes()).hexdigest())
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, w=w, meta=np.array(json.dumps(meta)))
 
     @classmethod
     def load(cls, path: str = DEFAULT_WEIGHTS) -> "Smoother":
         w, meta = read_weights(path)
-        s = cls(w)
+        s = cls(w, odd=bool(meta.get("odd", False)))
         s.meta = meta
         return s
 
@@ -167,3 +174,13 @@ def read_weights(path: str = DEFAULT_WEIGHTS):
     if w.size != WEIGHTS or hashlib.sha256(w.tobytes()).hexdigest() != meta.get("sha256"):
         raise ValueError(f"{path}: not a smoother weight file (size or checksum mismatch)")
     return w, meta
+
+
+def sample_norms(e, dims, nb: int, kind: int = 0):
+    """1/(e.e) (kind 0) or 1/(e.Ae) (kind 1) per sample, on the device."""
+    torch = _torch()
+    L = load()
+    nz, ny, nx = dims
+    out = torch.empty(nb, dtype=torch.float32, device="cuda")
+    check(L, L.hpcgb200_sample_norms(nb, nz, ny, nx, _vp(e), kind, _vp(out), _stream()))
+    return out

@@ -44,33 +44,46 @@ def test_normal_rhs_device_matches_python():
     assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("dims,nb", [((6, 9, 20), 2), ((16, 16, 16), 1), ((8, 8, 8), 4)])
-def test_forward_matches_oracle(dims, nb):
+@pytest.mark.parametrize("dims,nb,odd", [((6, 9, 20), 2, False), ((16, 16, 16), 1, False), ((8, 8, 8), 4, False),
+                                         ((6, 9, 20), 2, True), ((16, 16, 16), 1, True)])
+def test_forward_matches_oracle(dims, nb, odd):
     rng = np.random.default_rng(1)
     per = int(np.prod(dims))
     w = LS.jacobi_weights(0.8, 0.1, 3)
-    S = LS.Smoother(w)
+    S = LS.Smoother(w, odd=odd)
     r = rng.standard_normal(nb * per).astype(np.float32)
     y = S.forward(dev(r), dims, nb)
     torch.cuda.synchronize()
     got = y.cpu().numpy()
     w1, w2, w3 = layers(w)
-    ref = np.concatenate([O.net_forward(dims, w1, w2, w3, r[b * per:(b + 1) * per])[0] for b in range(nb)])
+
+    def net(v):
+        yp = O.net_forward(dims, w1, w2, w3, v)[0]
+        return 0.5 * (yp - O.net_forward(dims, w1, w2, w3, -v)[0]) if odd else yp
+
+    ref = np.concatenate([net(r[b * per:(b + 1) * per]) for b in range(nb)])
     assert np.linalg.norm(got - ref) <= 1e-2 * np.linalg.norm(ref)
     assert np.max(np.abs(got - ref)) <= 5e-2 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("dims,nb", [((6, 9, 20), 2), ((12, 12, 12), 3)])
-def test_gradients_match_oracle(dims, nb):
+@pytest.mark.parametrize("dims,nb,odd,kind", [((6, 9, 20), 2, False, 0), ((12, 12, 12), 3, False, 0),
+                                              ((6, 9, 20), 2, True, 0), ((6, 9, 20), 2, False, 1),
+                                              ((12, 12, 12), 2, True, 1)])
+def test_gradients_match_oracle(dims, nb, odd, kind):
     rng = np.random.default_rng(2)
     per = int(np.prod(dims))
     w = LS.jacobi_weights(0.8, 0.15, 5)
-    S = LS.Smoother(w)
+    S = LS.Smoother(w, odd=odd)
     r = rng.standard_normal(nb * per).astype(np.float32)
     e = (rng.standard_normal(nb * per) * 0.05).astype(np.float32)
-    inv = np.array([1.0 / np.sum(e[b * per:(b + 1) * per].astype(np.float64) ** 2) for b in range(nb)], np.float32)
+    inv = LS.sample_norms(dev(e), dims, nb, kind)
+    want_inv = [1.0 / np.dot(e[b * per:(b + 1) * per].astype(np.float64),
+                             (O.stencil_apply(dims, e[b * per:(b + 1) * per]) if kind else e[b * per:(b + 1) * per]))
+                for b in range(nb)]
+    torch.cuda.synchronize()
+    assert np.allclose(inv.cpu().numpy(), want_inv, rtol=1e-5)
     scale = 1.0 / nb
-    loss, dw = S.loss_grad(dev(r), dev(e), dev(inv), dims, nb, scale)
+    loss, dw = S.loss_grad(dev(r), dev(e), inv, dims, nb, scale, kind)
     torch.cuda.synchronize()
     got = dw.cpu().numpy()
     w1, w2, w3 = layers(w)
@@ -78,7 +91,7 @@ def test_gradients_match_oracle(dims, nb):
     ref = np.zeros(3 * 27 * 256)
     for b in range(nb):
         sl = slice(b * per, (b + 1) * per)
-        lb, gb = O.net_loss_grad(dims, w1, w2, w3, r[sl], e[sl])
+        lb, gb = O.net_loss_grad(dims, w1, w2, w3, r[sl], e[sl], odd=odd, kind=kind)
         ref_loss += scale * lb
         ref += scale * np.concatenate(gb)
     assert abs(loss - ref_loss) <= 1e-3 * ref_loss

@@ -68,7 +68,8 @@ def test_wgrad_is_bilinear_derivative():
     assert abs(f - np.dot(dw.astype(np.float64), w)) <= 1e-4 * (abs(f) + 1.0)
 
 
-def test_net_gradient_finite_differences():
+@pytest.mark.parametrize("odd,kind", [(False, 0), (True, 0), (False, 1), (True, 1)])
+def test_net_gradient_finite_differences(odd, kind):
     dims = (5, 4, 6)
     n = 120
     rng = np.random.default_rng(5)
@@ -77,7 +78,7 @@ def test_net_gradient_finite_differences():
     w3 = _rand_weights(rng, co_used=1, scale=0.15)
     r = rng.standard_normal(n).astype(np.float32)
     e = rng.standard_normal(n).astype(np.float32)
-    loss, grads = O.net_loss_grad(dims, w1, w2, w3, r, e, round_=False)
+    loss, grads = O.net_loss_grad(dims, w1, w2, w3, r, e, round_=False, odd=odd, kind=kind)
     ws = [w1, w2, w3]
     used = [np.nonzero(w1)[0], np.nonzero(w2)[0], np.nonzero(w3)[0]]
     h = 3e-3
@@ -88,8 +89,8 @@ def test_net_gradient_finite_differences():
             wm = [w.copy() for w in ws]
             wp[layer][idx] += h
             wm[layer][idx] -= h
-            lp, _ = O.net_loss_grad(dims, *wp, r, e, round_=False)
-            lm, _ = O.net_loss_grad(dims, *wm, r, e, round_=False)
+            lp, _ = O.net_loss_grad(dims, *wp, r, e, round_=False, odd=odd, kind=kind)
+            lm, _ = O.net_loss_grad(dims, *wm, r, e, round_=False, odd=odd, kind=kind)
             fd = (lp - lm) / (2 * h)
             rel.append(abs(fd - float(grads[layer][idx])) / max(abs(fd), 1e-3))
     # the net is piecewise linear: a step that crosses a ReLU kink spoils a
@@ -113,3 +114,25 @@ def test_net_bf16_close_to_fp32():
     y16, a1, _ = O.net_forward(dims, w1, w2, w3, r, round_=True)
     assert np.array_equal(a1, O.bf16(a1))  # hidden activations are stored as bf16
     assert np.linalg.norm(y16 - y32) <= 2e-2 * np.linalg.norm(y32)
+
+
+def test_odd_network_is_odd_and_energy_loss_matches_definition():
+    dims = (4, 5, 6)
+    n = 120
+    rng = np.random.default_rng(8)
+    w1 = _rand_weights(rng, ci_used=1, scale=0.5)
+    w2 = _rand_weights(rng, scale=0.15)
+    w3 = _rand_weights(rng, co_used=1, scale=0.15)
+    r = rng.standard_normal(n).astype(np.float32)
+    e = rng.standard_normal(n).astype(np.float32)
+    yp = O.net_forward(dims, w1, w2, w3, r, round_=False)[0]
+    ym = O.net_forward(dims, w1, w2, w3, -r, round_=False)[0]
+    y = 0.5 * (yp - ym)
+    d = (y - e).astype(np.float32)
+    want = np.dot(d.astype(np.float64), O.stencil_apply(dims, d)) / np.dot(e.astype(np.float64),
+                                                                           O.stencil_apply(dims, e))
+    loss, _ = O.net_loss_grad(dims, w1, w2, w3, r, e, round_=False, odd=True, kind=1)
+    assert abs(loss - want) <= 1e-5 * want
+    # the stencil is the HPCG matrix: symmetric, diagonal 26
+    v = rng.standard_normal(n).astype(np.float32)
+    assert abs(np.dot(O.stencil_apply(dims, v), e) - np.dot(v, O.stencil_apply(dims, e))) < 1e-3
