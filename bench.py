@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
+    ap.add_argument("--learned-nx", type=int, default=256)
+    ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
 
 
@@ -343,6 +345,11 @@ def run_ours(args):
     if not args.no_mixed:
         mixed = mixed_comparison(args, R, barrier)
 
+    # ---- learned coarse-level smoother vs SymGS at 256^3, b ~ N(0,1) seed 9999
+    learned = None
+    if not args.no_learned:
+        learned = learned_comparison(args, R, barrier)
+
     # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -371,6 +378,7 @@ def run_ours(args):
             "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m,
                     "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err},
             "roofline": roofline, "kernels": extra_kernels, "cpu_baseline": cpu, "mixed": mixed,
+            "learned": learned,
             "gpu_launches": launches, "clocks": clocks,
         }
         print(json.dumps(line))
@@ -419,6 +427,103 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
     res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
     Q.close()
     return res
+
+
+def conv_kernel_timing(nb, n, reps=50):
+    """Layer-2 convolution (16 -> 16 channels, tcgen05) on nb samples of n^3
+    points, timed with CUDA events on torch's stream."""
+    import ctypes
+
+    import torch
+
+    L = R_load()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    g = torch.Generator(device="cuda").manual_seed(1)
+    w = torch.randn(27 * 256, device="cuda", generator=g) * 0.1
+    wB = torch.empty(L.hpcgb200_conv_weight_tile_bytes(), dtype=torch.uint8, device="cuda")
+    L.hpcgb200_conv_prepare_weights(vp(w), vp(wB), 0, st)
+    pts = nb * n ** 3
+    x = (torch.randn(pts * 16, device="cuda", generator=g)).to(torch.bfloat16)
+    out = torch.empty_like(x)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(3):
+        L.hpcgb200_conv16(nb, n, n, n, vp(x), vp(wB), 0, vp(out), None, vp(status), st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        L.hpcgb200_conv16(nb, n, n, n, vp(x), vp(wB), 0, vp(out), None, vp(status), st)
+    e1.record()
+    torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / reps
+    flops = pts * 27 * 16 * 16 * 2
+    return {"points": pts, "us_per_launch": us, "tflops": flops / us * 1e-6, "status": int(status.item())}
+
+
+def R_load():
+    import rochpcg_b200 as R
+
+    return R.load()
+
+
+def learned_comparison(args, R, barrier, steps=2):
+    """levels 2-3 SymGS replaced by the trained conv net (committed
+    weights), flexible CG with fallback, vs the plain FP32 V-cycle and FP64, on
+    an n^3 system with b ~ N(0,1) (seed 9999), all to args.tol."""
+    from rochpcg_b200 import learned as LS
+    from rochpcg_b200.rhs import normal_rhs
+
+    n = args.learned_nx
+    Q = R.Problem(n)
+    Q.set_rhs(normal_rhs(Q.rows[0], 9999))
+    f, _ = Q.model()
+    S = LS.Smoother.load()
+    res = {}
+    for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED), ("learned", R.MODE_LEARNED)):
+        if mode == R.MODE_LEARNED:
+            Q.set_smoother(S, 2)
+        Q.cg(args.max_iter, args.tol, mode=mode)  # warm-up
+        barrier()
+        ts = []
+        for _ in range(steps):
+            r = Q.cg(args.max_iter, args.tol, mode=mode)
+            ts.append(r["seconds"])
+        res[name] = {"time_to_1e-9_s": min(ts), "iterations": r["niters"],
+                     "rel_residual_fp64_true": Q.true_residual(),
+                     "gflops_hpcg_model": f * r["niters"] / min(ts) / 1e9,
+                     "kernels_per_iteration": Q.kernels_per_iteration(mode)}
+        if mode == R.MODE_LEARNED:
+            res[name]["fallback_iteration"] = Q.last_fallback()
+            res[name]["vcycle_ms"] = Q.time_op("mg_learned", 10)
+        elif mode == R.MODE_MIXED:
+            res[name]["vcycle_ms"] = Q.time_op("mg_mixed", 10)
+    res["speedup_learned_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
+    res["speedup_learned_vs_mixed"] = res["mixed"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
+    Q.set_smoother(None)
+    Q.close()
+    meta = S.meta
+    conv = conv_kernel_timing(2, n >> 2)  # level 2, both branches of the odd evaluation
+    peak = measured_bf16_peak()
+    res["conv_kernel"] = dict(conv, kernel="k_conv16 (layer 2, 16->16, tcgen05 M128 N16 K16, TMA-pipelined)",
+                              bound="tensor", peak_tflops=peak, frac=conv["tflops"] / peak if peak else None)
+    res["weights"] = {"file": "rochpcg_b200/weights/smoother_l23.npz", "sha256": meta.get("sha256"),
+                      "symmetry": meta.get("symmetry"), "heldout": meta.get("heldout"),
+                      "training": {k: meta.get("training", {}).get(k) for k in ("epochs", "loss", "lr0", "lr1")}}
+    res["grid"] = [n, n, n]
+    res["rhs"] = "N(0,1) i.i.d., seed 9999"
+    return res
+
+
+def measured_bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        for k in ("bf16_tflops", "bf16_dense_tflops"):
+            if k in d:
+                return float(d[k])
+    except Exception:
+        pass
+    return 1590.0
 
 
 def run_mixed_only(args, R, barrier):

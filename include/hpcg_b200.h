@@ -298,21 +298,28 @@ typedef struct hpcgb200_smoother hpcgb200_smoother;
 #define HPCGB200_SMOOTHER_WEIGHTS (3 * 27 * 16 * 16)
 
 int hpcgb200_smoother_create(hpcgb200_smoother** out);
-/* Detach it from every problem (hpcgb200_problem_set_smoother(p, NULL, 0))
+/* Detach it from every problem (hpcgb200_problem_set_smoother(p, NULL, 0, 0))
  * before destroying it. */
 int hpcgb200_smoother_destroy(hpcgb200_smoother* s);
 int hpcgb200_smoother_set_weights(hpcgb200_smoother* s, const float* host_w);
 int hpcgb200_smoother_get_weights(hpcgb200_smoother* s, float* host_w);
 /* Host-side initial weights: the network computes omega * r / 26 (a damped
- * Jacobi step: channel 0 = relu(r), channel 1 = relu(-r)) plus uniform noise
- * in [-noise, noise] on every other used weight, from a SplitMix64 stream. */
-int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsigned long long seed);
+ * Jacobi step: channel 0 = relu(r), channel `twin` (1..15; 8 for the tied
+ * form) = relu(-r)) plus uniform noise in [-noise, noise] on every other used
+ * weight, from a SplitMix64 stream. */
+int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsigned long long seed, int twin);
 /* y = N(r) for nb samples of nz x ny x nx points. */
 int hpcgb200_smoother_forward(hpcgb200_smoother* s, int nb, int nz, int ny, int nx, const float* r, float* y,
                               void* stream);
-/* odd != 0: the network is evaluated as (N(r) - N(-r)) / 2, an odd function
- * of r (both branches run as one batch of two); the default is N(r). */
-int hpcgb200_smoother_configure(hpcgb200_smoother* s, int odd);
+/* Symmetry of the network in r.  0 (default): plain N(r).  1: evaluated as
+ * (N(r) - N(-r)) / 2, an odd function (both branches run as one batch of
+ * two).  2: tied weights -- hidden channel k+8 is the negated twin of channel
+ * k in every layer, enforced on every weight update -- so one evaluation of N
+ * is already odd. */
+#define HPCGB200_SMOOTHER_PLAIN 0
+#define HPCGB200_SMOOTHER_ODD 1
+#define HPCGB200_SMOOTHER_TIED 2
+int hpcgb200_smoother_configure(hpcgb200_smoother* s, int symmetry);
 /* loss = scale * sum_b d_b.M d_b * inv_norm[b], d = y - e with y the network
  * output; kind 0: M = I, kind 1: M = the 27-point stencil A (energy norm).
  * inv_norm (device, nb floats) = 1/(e.e) or 1/(e.Ae): hpcgb200_sample_norms.
@@ -355,8 +362,11 @@ int hpcgb200_make_training_pairs(int fine_n, int level, unsigned long long first
 int hpcgb200_normal_rhs(long long m, unsigned long long seed, double* out, void* stream);
 
 /* Attach a smoother (NULL detaches) to the problem's levels >= first_level
- * for HPCGB200_MODE_LEARNED; the handle must outlive the attachment. */
-int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* s, int first_level);
+ * for HPCGB200_MODE_LEARNED; the handle must outlive the attachment.  On
+ * those levels the V-cycle's pre- and post-smoothing SymGS become x = N(r)
+ * and x += N(r - A x); the coarsest level's single SymGS becomes x = N(r)
+ * followed by coarse_steps - 1 steps x += N(r - A x) (1..64). */
+int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* s, int first_level, int coarse_steps);
 /* Iteration at which the last learned solve fell back to SymGS (0: never). */
 int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter);
 
@@ -364,7 +374,8 @@ int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter
  * the problem's stream; *ms_per_launch = average.  op: "spmv","symgs_sweep"
  * (one full-row color sweep, averaged over the 15 of a SymGS step),
  * "symgs","symgs_zero","mg","mg_mixed", "symgs32_sweep" (one FP32 implicit
- * colour sweep, averaged over a SymGS step), "spmv_stencil". */
+ * colour sweep, averaged over a SymGS step), "spmv_stencil", "mg_learned"
+ * (the V-cycle with the attached learned smoother). */
 int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
 
 #ifdef __cplusplus

@@ -211,14 +211,15 @@ class Problem:
         check(self.L, self.L.hpcgb200_problem_prolong(self.h, level, ctypes.c_void_p(xc_ptr), ctypes.c_void_p(xf_ptr)))
 
     # -- learned smoother --------------------------------------------------
-    def set_smoother(self, smoother, first_level: int = 2):
+    def set_smoother(self, smoother, first_level: int = 2, coarse_steps: int = 1):
         """Attach a ``rochpcg_b200.learned.Smoother`` to levels >= first_level
-        for MODE_LEARNED (None detaches)."""
+        for MODE_LEARNED (None detaches); coarse_steps learned Richardson steps
+        replace the coarsest level's SymGS."""
         if smoother is None:
-            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, None, 0))
+            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, None, 0, 0))
             self._smoother = None
         else:
-            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, smoother.h, first_level))
+            check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, smoother.h, first_level, coarse_steps))
             self._smoother = smoother  # kept alive while attached
 
     def last_fallback(self) -> int:

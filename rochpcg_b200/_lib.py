@@ -50,7 +50,7 @@ SIGNATURES = {
     "hpcgb200_smoother_destroy": (_i, [_vp]),
     "hpcgb200_smoother_set_weights": (_i, [_vp, _vp]),
     "hpcgb200_smoother_get_weights": (_i, [_vp, _vp]),
-    "hpcgb200_smoother_init_jacobi": (_i, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_ulonglong]),
+    "hpcgb200_smoother_init_jacobi": (_i, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_ulonglong, _i]),
     "hpcgb200_smoother_forward": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp]),
     "hpcgb200_smoother_configure": (_i, [_vp, _i]),
     "hpcgb200_smoother_loss_grad": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, ctypes.c_float, _i, _vp, _vp, _vp]),
@@ -60,7 +60,7 @@ SIGNATURES = {
                                      _vp, _vp]),
     "hpcgb200_make_training_pairs": (_i, [_i, _i, ctypes.c_ulonglong, _i, _vp, _vp, _vp, _d]),
     "hpcgb200_normal_rhs": (_i, [_ll, ctypes.c_ulonglong, _vp, _vp]),
-    "hpcgb200_problem_set_smoother": (_i, [_vp, _vp, _i]),
+    "hpcgb200_problem_set_smoother": (_i, [_vp, _vp, _i, _i]),
     "hpcgb200_problem_last_fallback": (_i, [_vp, _vp]),
     "hpcgb200_problem_create": (_i, [_i, _i, _i, _i, _vp]),
     "hpcgb200_problem_create_ex": (_i, [_i, _i, _i, _i, _i, _vp]),

@@ -30,7 +30,9 @@
 // is bounded.  On timeout the CTA records an error in *status, waits once more
 // (bounded) for its MMAs, leaves its loop as a whole block and still frees its
 // TMEM, so the context stays usable.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 
@@ -175,31 +177,126 @@ __device__ __forceinline__ uint4 pack_bf16x8(const float* v)
 __host__ __device__ constexpr uint32_t kmajor_off(int r, int c) { return (uint32_t)((r >> 3) * 256 + c * 128 + (r & 7) * 16); }
 
 // ------------------------------------------------------------ forward conv
+//
+// Warp-specialised persistent kernel, one CTA per SM:
+//   warp 0      TMA producer: for each brick, six tiled loads (three dx
+//               shifts x two 8-channel halves) of the halo'd brick into one of
+//               kStages shared-memory stages (zero fill outside the grid);
+//   warp 1      allocates TMEM and issues the brick's 27 x kTZ tcgen05.mma
+//               into one of two TMEM accumulators;
+//   warps 2-5   epilogue: tcgen05.ld of the finished accumulator, ReLU /
+//               mask / permuted scatter, global stores.
+// Stage and accumulator hand-offs are mbarriers (TMA complete_tx, MMA commit,
+// epilogue arrivals), so loads, MMAs and stores of consecutive bricks overlap.
 
-constexpr int kTX = 16, kTY = 8, kTZ = 2;
-constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2;
-constexpr int kCopyRows = kTX * kHY * kHZ;            // 640 rows per shifted copy
-constexpr int kRegion = kCopyRows * 16;               // one 8-channel half: 10240 B (the K-major LBO)
+#ifndef HB_CONV_TZ
+#define HB_CONV_TZ 4
+#endif
+#ifndef HB_CONV_STAGES
+#define HB_CONV_STAGES 2
+#endif
+#ifndef HB_CONV_CTAS
+#define HB_CONV_CTAS 1
+#endif
+constexpr int kTX = 16, kTY = 8, kTZ = HB_CONV_TZ;
+constexpr int kHY = kTY + 2, kHZ = kTZ + 2;
+constexpr int kCopyRows = kTX * kHY * kHZ;            // 960 rows per shifted copy
+constexpr int kRegion = kCopyRows * 16;               // one 8-channel half: 15360 B = one TMA box (the K-major LBO)
 constexpr int kCopyBytes = 2 * kRegion;
-constexpr int kStageBytes = 3 * kCopyBytes;           // 61440 B
-constexpr int kHaloItems = 2 * kHX * kHY * kHZ;       // 16-byte loads per brick: 1440
-constexpr int kConvThreads = 256;
-constexpr int kConvSmem = kStageBytes + kNetWeightTileBytes + 64 + 128;
+constexpr int kStageBytes = 3 * kCopyBytes;           // 92160 B
+constexpr int kStages = HB_CONV_STAGES;
+constexpr int kAccCols = kTZ * 16;                    // FP32 columns of one brick's accumulator
+constexpr int kTmemCols = 2 * kAccCols;               // double-buffered: 128 columns
+constexpr int kConvThreads = 192;
+constexpr int kEpiThreads = 128;
+constexpr int kConvSmem = kStages * kStageBytes + kNetWeightTileBytes + 256 + 1024;
 
 static_assert((kRegion >> 4) < (1 << 14), "LBO field");
 static_assert(kTX * kTY == 128, "one z plane of the brick is one 128-row M tile");
+static_assert(kStageBytes % 1024 == 0 && kRegion % 128 == 0, "stage alignment");
+static_assert(kConvSmem <= 227 * 1024, "shared memory per CTA");
+
+struct Brick
+{
+    int b, x0, y0, z0;
+};
+
+__device__ __forceinline__ Brick brick_of(const ConvGrid& g, long tile, int tx, int ty, long per_sample)
+{
+    Brick r;
+    r.b = (int)(tile / per_sample);
+    long t2 = tile - (long)r.b * per_sample;
+    const int bz = (int)(t2 / ((long)tx * ty));
+    t2 -= (long)bz * tx * ty;
+    const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
+    r.x0 = bx * kTX;
+    r.y0 = by * kTY;
+    r.z0 = bz * kTZ;
+    return r;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// Tiled 5-D TMA load (no multicast) completing on mbar.
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(mbar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+        : "memory");
+}
+
+// Bounded wait that also gives up when another role aborted.
+__device__ __forceinline__ bool role_wait(uint64_t* mbar, uint32_t parity, volatile int* abort_flag, int* status,
+                                          int code)
+{
+    const uint32_t a = smem_u32(mbar);
+    for(uint32_t i = 0; i < kSpinLimit; ++i)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if(done) return true;
+        if((i & 255) == 255 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    atomicExch(status, code);
+    return false;
+}
 
 template <int kOut>
-__global__ void __launch_bounds__(kConvThreads, 2)
-    k_conv16(ConvGrid g, const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wB, void* out,
+__global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
+    k_conv16(const __grid_constant__ CUtensorMap in_map, ConvGrid g, const __nv_bfloat16* __restrict__ wB, void* out,
              const __nv_bfloat16* __restrict__ act, PermMap pm, int* status)
 {
     extern __shared__ unsigned char smem_raw[];
-    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    unsigned char* sA = smem;
-    unsigned char* sW = smem + kStageBytes;
-    uint64_t* mbar = (uint64_t*)(sW + kNetWeightTileBytes);
-    uint32_t* tholder = (uint32_t*)(mbar + 1);
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sA = smem;                                   // kStages x kStageBytes
+    unsigned char* sW = smem + kStages * kStageBytes;           // weights
+    uint64_t* full = (uint64_t*)(sW + kNetWeightTileBytes);     // [kStages] TMA -> MMA
+    uint64_t* empty = full + kStages;                           // [kStages] MMA -> TMA
+    uint64_t* tfull = empty + kStages;                          // [2] MMA -> epilogue
+    uint64_t* tempty = tfull + 2;                               // [2] epilogue -> MMA
+    uint32_t* tholder = (uint32_t*)(tempty + 2);
+    volatile int* abort_flag = (volatile int*)(tholder + 1);
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -209,131 +306,180 @@ __global__ void __launch_bounds__(kConvThreads, 2)
 
     for(int i = tid; i < kNetWeightTileBytes / 16; i += kConvThreads)
         reinterpret_cast<uint4*>(sW)[i] = reinterpret_cast<const uint4*>(wB)[i];
-    if(tid == 0) mbar_init(mbar, 1);
-    if(warp == 0) tmem_alloc(tholder, 32);
+    if(tid == 0)
+    {
+        for(int s = 0; s < kStages; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for(int a = 0; a < 2; ++a)
+        {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], kEpiThreads);
+        }
+        *abort_flag = 0;
+    }
+    if(warp == 1) tmem_alloc(tholder, kTmemCols);
+    fence_async_smem();  // the weights are read by the tensor cores
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tholder;
-    constexpr uint32_t idesc = umma_idesc_bf16(128, 16, false, false);
-    uint32_t phase = 0;
 
-    for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    if(warp == 0 && lane == 0)
     {
-        const int b = (int)(tile / per_sample);
-        long t2 = tile - (long)b * per_sample;
-        const int bz = (int)(t2 / ((long)tx * ty));
-        t2 -= (long)bz * tx * ty;
-        const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
-        const int x0 = bx * kTX, y0 = by * kTY, z0 = bz * kTZ;
-        const __nv_bfloat16* inb = in + (long)b * g.nz * g.ny * g.nx * kNetCh;
-
-        // halo brick -> three dx-shifted copies (half-channel regions)
-        for(int it = tid; it < kHaloItems; it += kConvThreads)
+        // ---- TMA producer
+        long issued = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++issued)
         {
-            const int c8 = it / (kHX * kHY * kHZ);
-            const int q = it - c8 * (kHX * kHY * kHZ);
-            const int jx = q % kHX, rest = q / kHX;
-            const int ly = rest % kHY, lz = rest / kHY;
-            const int x = x0 + jx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)
-                v = __ldg(reinterpret_cast<const uint4*>(inb + (((long)z * g.ny + y) * g.nx + x) * kNetCh) + c8);
-            const int rowbase = (lz * kHY + ly) * kTX;
+            const int st = (int)(issued % kStages);
+            const uint32_t ph = (uint32_t)((issued / kStages) & 1);
+            if(!role_wait(&empty[st], ph ^ 1u, abort_flag, status, 3)) break;
+            const Brick bk = brick_of(g, tile, tx, ty, per_sample);
+            mbar_expect_tx(&full[st], 6u * kRegion);
+            unsigned char* dst = sA + st * kStageBytes;
 #pragma unroll
             for(int dxi = 0; dxi < 3; ++dxi)
+#pragma unroll
+                for(int c8 = 0; c8 < 2; ++c8)
+                    tma_load_5d(dst + dxi * kCopyBytes + c8 * kRegion, &in_map, c8 * 8, bk.x0 + dxi - 1, bk.y0 - 1,
+                                bk.z0 - 1, bk.b, &full[st]);
+        }
+        if(*abort_flag)
+        {
+            // let the loads already issued land before the CTA's shared memory goes away
+            for(long k = issued - kStages < 0 ? 0 : issued - kStages; k < issued; ++k)
             {
-                const int lx = jx - dxi;  // copy dx = dxi-1 holds point x0 + lx + dx at lx
-                if(lx >= 0 && lx < kTX)
-                    *reinterpret_cast<uint4*>(sA + dxi * kCopyBytes + c8 * kRegion + (rowbase + lx) * 16) = v;
+                uint32_t done = 0;
+                const uint32_t a = smem_u32(&full[k % kStages]);
+                for(uint32_t i = 0; i < kSpinLimit && !done; ++i)
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                        "selp.u32 %0, 1, 0, p;\n\t}\n"
+                        : "=r"(done)
+                        : "r"(a), "r"((uint32_t)((k / kStages) & 1))
+                        : "memory");
             }
         }
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if(tid == 0)
+    }
+    else if(warp == 1 && lane == 0)
+    {
+        // ---- MMA issuer
+        constexpr uint32_t idesc = umma_idesc_bf16(128, 16, false, false);
+        const uint64_t bd0 = umma_desc(smem_u32(sW), 128, 256);
+        long i = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
         {
-            const uint32_t a0 = smem_u32(sA), w0 = smem_u32(sW);
-#pragma unroll 1
+            const int st = (int)(i % kStages);
+            const uint32_t ph = (uint32_t)((i / kStages) & 1);
+            const int acc = (int)(i & 1);
+            const uint32_t aph = (uint32_t)((i >> 1) & 1);
+            if(!role_wait(&tempty[acc], aph ^ 1u, abort_flag, status, 4)) break;
+            if(!role_wait(&full[st], ph, abort_flag, status, 5)) break;
+            tc_fence_after();
+            // descriptors = base + compile-time offset (the 14-bit start field
+            // holds address / 16 and stays below 2^14 for any smem address)
+            const uint64_t ad0 = umma_desc(smem_u32(sA + st * kStageBytes), kRegion, 128);
+            const uint32_t d0 = tmem + (uint32_t)(acc * kAccCols);
+#pragma unroll
             for(int t = 0; t < 27; ++t)
             {
                 const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-                const uint64_t bd = umma_desc(w0 + t * 512, 128, 256);
 #pragma unroll
                 for(int mt = 0; mt < kTZ; ++mt)
                 {
                     const int row0 = ((mt + dz + 1) * kHY + (dy + 1)) * kTX;
-                    const uint64_t ad = umma_desc(a0 + (dx + 1) * kCopyBytes + row0 * 16, kRegion, 128);
-                    mma_bf16(tmem + mt * 16, ad, bd, idesc, t > 0 ? 1u : 0u);
+                    const uint64_t ad = ad0 + (uint64_t)(((dx + 1) * kCopyBytes + row0 * 16) >> 4);
+                    mma_bf16(d0 + mt * 16, ad, bd0 + (uint64_t)(t * 512 >> 4), idesc, t > 0 ? 1u : 0u);
                 }
             }
-            mma_commit(mbar);
+            mma_commit(&empty[st]);   // stage free once these MMAs have read it
+            mma_commit(&tfull[acc]);  // accumulator ready for the epilogue
         }
-        __syncwarp();
-        const bool done = mbar_wait(mbar, phase);
-        const bool ok = __syncthreads_and(done) != 0;
-        if(!ok)
+        if(*abort_flag && i > 0)
         {
-            if(tid == 0) atomicExch(status, 1);
-            if(!done) mbar_wait(mbar, phase);  // one more bounded chance for the MMAs in flight
-            break;
+            // MMAs in flight must finish before TMEM is released
+            const long k = i - 1;
+            uint32_t done = 0;
+            const uint32_t a = smem_u32(&tfull[k & 1]);
+            for(uint32_t j = 0; j < kSpinLimit && !done; ++j)
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(a), "r"((uint32_t)((k >> 1) & 1))
+                    : "memory");
         }
-        phase ^= 1u;
-        tc_fence_after();
-
-        const int qd = warp & 3, mt = warp >> 2;
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(mt * 16), v);
+    }
+    else if(warp >= 2)
+    {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        const int qd = warp & 3;
         const int m = qd * 32 + lane;
-        const int x = x0 + (m & 15), y = y0 + (m >> 4), z = z0 + mt;
-        if(x < g.nx && y < g.ny && z < g.nz)
+        long i = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
         {
-            const long p = (((long)b * g.nz + z) * g.ny + y) * g.nx + x;
-            if constexpr(kOut == kOutReluBf16 || kOut == kOutMaskBf16)
+            const int acc = (int)(i & 1);
+            const uint32_t aph = (uint32_t)((i >> 1) & 1);
+            if(!role_wait(&tfull[acc], aph, abort_flag, status, 6)) break;
+            tc_fence_after();
+            const Brick bk = brick_of(g, tile, tx, ty, per_sample);
+            const int x = bk.x0 + (m & 15), y = bk.y0 + (m >> 4);
+#pragma unroll 1
+            for(int mt = 0; mt < kTZ; ++mt)
             {
-                if constexpr(kOut == kOutReluBf16)
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(acc * kAccCols + mt * 16), v);
+                const int z = bk.z0 + mt;
+                if(x >= g.nx || y >= g.ny || z >= g.nz) continue;
+                const long p = (((long)bk.b * g.nz + z) * g.ny + y) * g.nx + x;
+                if constexpr(kOut == kOutReluBf16 || kOut == kOutMaskBf16)
                 {
+                    if constexpr(kOut == kOutReluBf16)
+                    {
 #pragma unroll
-                    for(int c = 0; c < 16; ++c) v[c] = v[c] > 0.f ? v[c] : 0.f;
+                        for(int c = 0; c < 16; ++c) v[c] = v[c] > 0.f ? v[c] : 0.f;
+                    }
+                    else
+                    {
+                        const uint4* ap = reinterpret_cast<const uint4*>(act + p * kNetCh);
+                        __align__(16) __nv_bfloat16 h[16];
+                        *reinterpret_cast<uint4*>(h) = ap[0];
+                        *reinterpret_cast<uint4*>(h + 8) = ap[1];
+#pragma unroll
+                        for(int c = 0; c < 16; ++c) v[c] = __bfloat162float(h[c]) > 0.f ? v[c] : 0.f;
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(out) + p * kNetCh);
+                    dst[0] = pack_bf16x8(v);
+                    dst[1] = pack_bf16x8(v + 8);
+                }
+                else if constexpr(kOut == kOutF32)
+                {
+                    float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + p * kNetCh);
+#pragma unroll
+                    for(int c = 0; c < 4; ++c)
+                        dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                }
+                else if constexpr(kOut == kOutF32C0)
+                {
+                    reinterpret_cast<float*>(out)[p] = v[0];
                 }
                 else
                 {
-                    const uint4* ap = reinterpret_cast<const uint4*>(act + p * kNetCh);
-                    __align__(16) __nv_bfloat16 h[16];
-                    *reinterpret_cast<uint4*>(h) = ap[0];
-                    *reinterpret_cast<uint4*>(h + 8) = ap[1];
-#pragma unroll
-                    for(int c = 0; c < 16; ++c) v[c] = __bfloat162float(h[c]) > 0.f ? v[c] : 0.f;
+                    float* xo = reinterpret_cast<float*>(out) + perm_row(pm, z, y, x);
+                    if constexpr(kOut == kOutPermSet) *xo = v[0];
+                    else *xo += v[0];
                 }
-                uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(out) + p * kNetCh);
-                dst[0] = pack_bf16x8(v);
-                dst[1] = pack_bf16x8(v + 8);
             }
-            else if constexpr(kOut == kOutF32)
-            {
-                float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + p * kNetCh);
-#pragma unroll
-                for(int c = 0; c < 4; ++c) dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
-            }
-            else if constexpr(kOut == kOutF32C0)
-            {
-                reinterpret_cast<float*>(out)[p] = v[0];
-            }
-            else
-            {
-                float* xo = reinterpret_cast<float*>(out) + perm_row(pm, z, y, x);
-                if constexpr(kOut == kOutPermSet) *xo = v[0];
-                else *xo += v[0];
-            }
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);
         }
-        tc_fence_before();
-        __syncthreads();  // TMEM read and staging consumed before the next brick
-        tc_fence_after();
     }
     tc_fence_before();
     __syncthreads();
-    if(warp == 0) tmem_free(tmem, 32);
+    tc_fence_after();
+    if(warp == 1) tmem_free(tmem, kTmemCols);
 }
 
 // ------------------------------------------------------------ weight gradient
@@ -419,15 +565,16 @@ __global__ void __launch_bounds__(kWgThreads) k_conv16_wgrad(ConvGrid g, const _
         tc_fence_after();
         if(tid == 0)
         {
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            const uint64_t ad0 = umma_desc(smem_u32(sA), 2048, 128);
+            const uint64_t bd0 = umma_desc(smem_u32(sB), 256, 128);
 #pragma unroll
             for(int s = 0; s < kWgK / 16; ++s)
             {
-                const uint64_t bd = umma_desc(b0 + s * 2 * 256, 256, 128);
+                const uint64_t bd = bd0 + (uint64_t)(s * 2 * 256 >> 4);
 #pragma unroll
                 for(int mt = 0; mt < 4; ++mt)
                 {
-                    const uint64_t ad = umma_desc(a0 + mt * kWgATile + s * 2 * 2048, 2048, 128);
+                    const uint64_t ad = ad0 + (uint64_t)((mt * kWgATile + s * 2 * 2048) >> 4);
                     mma_bf16(tmem + (uint32_t)(mt * 16), ad, bd, idesc, (first && s == 0) ? 0u : 1u);
                 }
             }
@@ -702,6 +849,45 @@ __global__ void __launch_bounds__(256) k_loss_grad(ConvGrid g, const float* __re
     if(threadIdx.x == 0) loss_partial[blockIdx.x] = acc;
 }
 
+// Projects the three layers' weights onto the odd-symmetric ("tied") form:
+// hidden channels k and k+8 are a +/- pair, so that the network is an odd
+// function of its input with one evaluation:
+//   w1[t][0][k+8] = -w1[t][0][k]; w2[t][i][j] = w2[t][i^8][j^8]; w3[t][j^8][0] = -w3[t][j][0].
+// Unused weights (layer 1 inputs >= 1, layer 3 outputs >= 1) are zeroed.
+__global__ void k_tie_odd(float* __restrict__ w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= kNetLayerWeights) return;
+    const int t = i / 256, a = (i / 16) % 16, b = i % 16;
+    float* w1 = w;
+    float* w2 = w + kNetLayerWeights;
+    float* w3 = w + 2 * kNetLayerWeights;
+    // each pair/quad is handled by its lowest index
+    if(a == 0 && b < 8)
+    {
+        const int k0 = (t * 16) * 16 + b, k1 = k0 + 8;
+        const float v = 0.5f * (w1[k0] - w1[k1]);
+        w1[k0] = v;
+        w1[k1] = -v;
+    }
+    if(a != 0) w1[i] = 0.f;
+    if(a < 8)
+    {
+        const int k0 = (t * 16 + a) * 16 + b, k1 = (t * 16 + (a ^ 8)) * 16 + (b ^ 8);
+        const float v = 0.5f * (w2[k0] + w2[k1]);
+        w2[k0] = v;
+        w2[k1] = v;
+    }
+    if(b == 0 && a < 8)
+    {
+        const int k0 = (t * 16 + a) * 16, k1 = (t * 16 + (a ^ 8)) * 16;
+        const float v = 0.5f * (w3[k0] - w3[k1]);
+        w3[k0] = v;
+        w3[k1] = -v;
+    }
+    if(b != 0) w3[i] = 0.f;
+}
+
 __global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ dw, float* __restrict__ m,
                        float* __restrict__ v, float lr, float beta1, float beta2, float eps, float c1, float c2)
 {
@@ -730,6 +916,34 @@ static int sm_count()
     return sms;
 }
 
+// Tensor map of a channel-last BF16 tensor [nb][nz][ny][nx][16] with the
+// brick box (8 channels, 16 x 10 x 6 points, 1 sample); the driver entry
+// point is looked up once through the runtime.
+static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if(!encode)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        HB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if(q != cudaDriverEntryPointSuccess || !fn)
+            return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[5] = {(cuuint64_t)kNetCh, (cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz,
+                                (cuuint64_t)g.nb};
+    const cuuint64_t row = (cuuint64_t)kNetCh * 2;
+    const cuuint64_t strides[4] = {row, row * g.nx, row * g.nx * g.ny, row * g.nx * g.ny * g.nz};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kTX, (cuuint32_t)kHY, (cuuint32_t)kHZ, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(in), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if(r != CUDA_SUCCESS) return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
 template <int kOut>
 static int conv_launch(const ConvGrid& g, const void* in, const void* wB, void* out, const void* act, const PermMap& pm,
                        int* status, cudaStream_t s)
@@ -740,10 +954,12 @@ static int conv_launch(const ConvGrid& g, const void* in, const void* wB, void* 
         HB_CUDA(cudaFuncSetAttribute(k_conv16<kOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
         attr = true;
     }
+    CUtensorMap map;
+    HB_RETURN_IF(conv_tensor_map(g, in, &map));
     const long tiles = (long)g.nb * ((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ);
-    const long cap = 2L * sm_count();
+    const long cap = (long)HB_CONV_CTAS * sm_count();
     const int grid = (int)(tiles < cap ? tiles : cap);
-    k_conv16<kOut><<<grid, kConvThreads, kConvSmem, s>>>(g, (const __nv_bfloat16*)in, (const __nv_bfloat16*)wB, out,
+    k_conv16<kOut><<<grid, kConvThreads, kConvSmem, s>>>(map, g, (const __nv_bfloat16*)wB, out,
                                                          (const __nv_bfloat16*)act, pm, status);
     HB_LAUNCHED();
     return 0;
@@ -897,6 +1113,13 @@ int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, float* d
     k_loss_diff<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, y, e, odd, d);
     HB_LAUNCHED();
     k_loss_grad<<<kLossBlocks, 256, 0, s>>>(g, d, wnorm, scale, kind, odd, (__nv_bfloat16*)G, loss_partial);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_tie_odd(float* w, cudaStream_t s)
+{
+    k_tie_odd<<<(kNetLayerWeights + 255) / 256, 256, 0, s>>>(w);
     HB_LAUNCHED();
     return 0;
 }

@@ -92,6 +92,11 @@ int loss_parts(long points);
 int launch_loss_grad(const ConvGrid& g, const float* y, const float* e, float* d, const float* wnorm, float scale,
                      int kind, int odd, void* G, float* loss_partial, cudaStream_t s);
 
+// Projects the weights (3 layers back to back) onto the tied odd form
+// (hidden channel k+8 = the negated twin of channel k): the network is then
+// an odd function of its input with a single evaluation.
+int launch_tie_odd(float* w, cudaStream_t s);
+
 // One Adam step on n parameters (bias-corrected, step t >= 1).
 int launch_adam(int n, float* w, const float* dw, float* m, float* v, float lr, float beta1, float beta2, float eps,
                 int t, cudaStream_t s);

@@ -100,6 +100,7 @@ struct LevelOpt
     // learned smoother (level 0 holds it for the hierarchy)
     struct Smoother* smoother = nullptr;
     int smoother_first_level = 2;
+    int smoother_coarse_steps = 1;     // learned Richardson steps x += N(r - A x) on the coarsest level
     int last_fallback_iter = 0;        // learned CG: iteration at which the last solve fell back (0: none)
     hb::PermMap pm{};                  // natural point -> permuted row (stencil levels)
 };

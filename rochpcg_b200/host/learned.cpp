@@ -41,8 +41,15 @@ Smoother::~Smoother()
         dfree(p);
 }
 
-void smoother_configure(Smoother& S, bool odd)
+void smoother_configure(Smoother& S, int symmetry, cudaStream_t s)
 {
+    const bool odd = symmetry == 1;
+    S.tied = symmetry == 2;
+    if(S.tied)
+    {
+        check(hb::launch_tie_odd(S.w, s));
+        S.tiles_stale = true;
+    }
     if(S.odd == odd) return;
     S.odd = odd;
     S.cap = 0;  // branch count changed: reallocate on next use
@@ -102,6 +109,7 @@ void smoother_reserve(Smoother& S, long points, bool training)
 void smoother_set_weights(Smoother& S, const float* host_w, cudaStream_t s)
 {
     HB_HOST_CUDA(cudaMemcpyAsync(S.w, host_w, sizeof(float) * kNetWeights, cudaMemcpyHostToDevice, s));
+    if(S.tied) check(hb::launch_tie_odd(S.w, s));
     S.tiles_stale = true;
     S.adam_t = 0;
     if(S.adam_m)
@@ -191,6 +199,7 @@ int smoother_adam(Smoother& S, float lr, float beta1, float beta2, float eps, cu
     if(!S.dw) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: no gradient computed yet");
     S.adam_t += 1;
     HB_RETURN_IF(hb::launch_adam(kNetWeights, S.w, S.dw, S.adam_m, S.adam_v, lr, beta1, beta2, eps, S.adam_t, s));
+    if(S.tied) HB_RETURN_IF(hb::launch_tie_odd(S.w, s));
     S.tiles_stale = true;
     return 0;
 }
@@ -219,18 +228,23 @@ int smoother_ready(const SparseMatrix& A, cudaStream_t s)
 }
 
 // FP32 V-cycle below level 0 with the learned levels (same recursion as mg_fp32).
-static int mg_fp32_learned(const SparseMatrix& A, int level, Smoother& S, int first, const float* r, float* x,
-                           cudaStream_t s)
+static int mg_fp32_learned(const SparseMatrix& A, int level, Smoother& S, int first, int coarse_steps, const float* r,
+                           float* x, cudaStream_t s)
 {
     const LevelOpt* o = opt(A);
     const bool learned = level >= first;
     if(learned) HB_RETURN_IF(smoother_level_apply(S, *o, r, x, false, s));
     else HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s));
-    if(!A.mgData) return 0;
+    if(!A.mgData)
+    {
+        // coarsest level: further learned Richardson steps x += N(r - A x)
+        for(int k = 1; learned && k < coarse_steps; ++k) HB_RETURN_IF(smoother_level_apply(S, *o, r, x, true, s));
+        return 0;
+    }
     const MGOpt* mo = mgopt(A);
     const int nc = A.Ac->localNumberOfRows;
     HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
-    HB_RETURN_IF(mg_fp32_learned(*A.Ac, level + 1, S, first, mo->rc32, mo->xc32, s));
+    HB_RETURN_IF(mg_fp32_learned(*A.Ac, level + 1, S, first, coarse_steps, mo->rc32, mo->xc32, s));
     HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
     if(learned) return smoother_level_apply(S, *o, r, x, true, s);
     return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
@@ -265,7 +279,7 @@ int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
         const MGOpt* mo = mgopt(A);
         const int nc = A.Ac->localNumberOfRows;
         HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
-        HB_RETURN_IF(mg_fp32_learned(*A.Ac, 1, S, first, mo->rc32, mo->xc32, s));
+        HB_RETURN_IF(mg_fp32_learned(*A.Ac, 1, S, first, o->smoother_coarse_steps, mo->rc32, mo->xc32, s));
         HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
         return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
     }
@@ -362,9 +376,10 @@ extern "C" int hpcgb200_smoother_get_weights(hpcgb200_smoother* h, float* host_w
     });
 }
 
-extern "C" int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsigned long long seed)
+extern "C" int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float noise, unsigned long long seed,
+                                             int twin)
 {
-    if(!host_w) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
+    if(!host_w || twin < 1 || twin > 15) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     constexpr int W = hb::kNetLayerWeights;
     Rng rng{seed};
     auto at = [](int tap, int ci, int co) { return (tap * 16 + ci) * 16 + co; };
@@ -375,13 +390,13 @@ extern "C" int hpcgb200_smoother_init_jacobi(float* host_w, float omega, float n
             const bool used = (l != 0 || ci == 0) && (l != 2 || co == 0);
             host_w[l * W + i] = used ? (float)(noise * (2.0 * rng.uniform() - 1.0)) : 0.f;
         }
-    // centre tap: channel 0 = relu(r), channel 1 = relu(-r), identity, out = omega (c0 - c1) / 26
+    // centre tap: channel 0 = relu(r), channel `twin` = relu(-r), identity, out = omega (c0 - c_twin) / 26
     host_w[0 * W + at(13, 0, 0)] += 1.f;
-    host_w[0 * W + at(13, 0, 1)] += -1.f;
+    host_w[0 * W + at(13, 0, twin)] += -1.f;
     host_w[1 * W + at(13, 0, 0)] += 1.f;
-    host_w[1 * W + at(13, 1, 1)] += 1.f;
+    host_w[1 * W + at(13, twin, twin)] += 1.f;
     host_w[2 * W + at(13, 0, 0)] += omega / 26.f;
-    host_w[2 * W + at(13, 1, 0)] += -omega / 26.f;
+    host_w[2 * W + at(13, twin, 0)] += -omega / 26.f;
     return 0;
 }
 
@@ -397,12 +412,13 @@ extern "C" int hpcgb200_smoother_forward(hpcgb200_smoother* h, int nb, int nz, i
     });
 }
 
-extern "C" int hpcgb200_smoother_configure(hpcgb200_smoother* h, int odd)
+extern "C" int hpcgb200_smoother_configure(hpcgb200_smoother* h, int symmetry)
 {
-    if(!h) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
+    if(!h || symmetry < 0 || symmetry > 2) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     return guarded([&] {
         HB_HOST_CUDA(cudaStreamSynchronize(h->stream));
-        smoother_configure(h->S, odd != 0);
+        smoother_configure(h->S, symmetry, h->stream);
+        HB_HOST_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     });
 }
@@ -574,11 +590,14 @@ extern "C" int hpcgb200_make_training_pairs(int fine_n, int level, unsigned long
     return rc;
 }
 
-extern "C" int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* h, int first_level)
+extern "C" int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* h, int first_level,
+                                             int coarse_steps)
 {
     if(!p) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     if(h && (first_level < 1 || first_level >= p->nlevels))
         return hb::record_error(HPCGB200_ERR_ARG, "first_level must be in 1..nlevels-1");
+    if(h && (coarse_steps < 1 || coarse_steps > 64))
+        return hb::record_error(HPCGB200_ERR_ARG, "coarse_steps must be in 1..64");
     return guarded([&] {
         LevelOpt* o = opt(p->A);
         if(!h)
@@ -604,6 +623,7 @@ extern "C" int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoot
         }
         o->smoother = &h->S;
         o->smoother_first_level = first_level;
+        o->smoother_coarse_steps = coarse_steps;
         return 0;
     });
 }

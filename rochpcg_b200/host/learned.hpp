@@ -15,6 +15,7 @@ struct Smoother
     unsigned char* wT = nullptr;   // 3 transposed-convolution tile sets
     bool tiles_stale = true;
     bool odd = false;              // evaluate (N(r) - N(-r)) / 2 (two branches as one batch)
+    bool tied = false;             // keep the weights in the tied odd form (one evaluation is odd)
 
     long cap = 0;                  // grid points the buffers hold (both branches when odd)
     long long epoch = 0;           // bumped when the activation buffers move
@@ -59,8 +60,9 @@ int smoother_forward(Smoother& S, const hb::ConvGrid& g, const float* r, float* 
 // the stencil A for kind 1) added to *loss_acc and its weight gradients into S.dw.
 int smoother_loss_grad(Smoother& S, const hb::ConvGrid& g, const float* r, const float* e, const float* wnorm,
                        float scale, int kind, cudaStream_t s);
-// Switches the odd evaluation (buffers are re-reserved on next use).
-void smoother_configure(Smoother& S, bool odd);
+// Symmetry of the network: 0 plain, 1 two-branch odd evaluation, 2 tied
+// odd weights (buffers are re-reserved on next use).
+void smoother_configure(Smoother& S, int symmetry, cudaStream_t s);
 int smoother_adam(Smoother& S, float lr, float beta1, float beta2, float eps, cudaStream_t s);
 // Reads and clears the device status word; nonzero: a tensor-core wait timed out.
 int smoother_status(Smoother& S, cudaStream_t s);

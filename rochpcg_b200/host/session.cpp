@@ -9,6 +9,7 @@
 
 #include "hpcg_b200.h"
 #include "internal.hpp"
+#include "learned.hpp"
 #include "problem.hpp"
 
 using namespace hpcg_b200;
@@ -493,6 +494,12 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
         else if(o == "symgs_zero") f = [&] { return ComputeSYMGSZeroGuess(A, r, z); };
         else if(o == "mg") f = [&] { return ComputeMG(A, r, z); };
         else if(o == "mg_mixed") f = [&] { return ComputeMG_Mixed(A, r, z); };
+        else if(o == "mg_learned")
+        {
+            if(!opt(A)->smoother) return hb::record_error(HPCGB200_ERR_ARG, "time_op: no smoother attached");
+            HB_RETURN_IF(smoother_ready(A, rt().stream));
+            f = [&] { return ComputeMG_Learned(A, r, z); };
+        }
         else if(o == "symgs32_sweep" || o == "spmv_stencil")
         {
             const LevelOpt* lo = opt(A);

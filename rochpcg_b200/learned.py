@@ -20,6 +20,7 @@ import numpy as np
 from ._lib import check, load
 
 WEIGHTS = 3 * 27 * 16 * 16
+PLAIN, ODD, TIED = 0, 1, 2
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "smoother_l23.npz")
 
 
@@ -38,12 +39,13 @@ def _stream() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def jacobi_weights(omega: float = 1.0, noise: float = 0.0, seed: int = 0) -> np.ndarray:
+def jacobi_weights(omega: float = 1.0, noise: float = 0.0, seed: int = 0, twin: int = 1) -> np.ndarray:
     """Weights whose network computes omega * r / 26 (a damped Jacobi step)
-    plus seeded uniform noise on the other used weights."""
+    plus seeded uniform noise on the other used weights; `twin` is the hidden
+    channel carrying relu(-r) (8 for the tied odd form)."""
     L = load()
     w = np.zeros(WEIGHTS, np.float32)
-    check(L, L.hpcgb200_smoother_init_jacobi(w.ctypes.data_as(ctypes.c_void_p), omega, noise, seed))
+    check(L, L.hpcgb200_smoother_init_jacobi(w.ctypes.data_as(ctypes.c_void_p), omega, noise, seed, twin))
     return w
 
 
@@ -82,21 +84,22 @@ def make_pairs(fine_n: int, level: int, first_seed: int, count: int, tol: float 
 class Smoother:
     """Device state of the conv-net smoother (weights, tiles, activations, Adam)."""
 
-    def __init__(self, weights: np.ndarray | None = None, odd: bool = False):
+    def __init__(self, weights: np.ndarray | None = None, symmetry: int = PLAIN):
         self.L = load()
         h = ctypes.c_void_p()
         check(self.L, self.L.hpcgb200_smoother_create(ctypes.byref(h)))
         self.h = h
         self.meta: dict = {}
-        self.odd = False
-        self.configure(odd)
+        self.symmetry = PLAIN
+        self.configure(symmetry)
         if weights is not None:
             self.set_weights(weights)
 
-    def configure(self, odd: bool):
-        """odd: evaluate (N(r) - N(-r)) / 2, an odd function of the residual."""
-        check(self.L, self.L.hpcgb200_smoother_configure(self.h, int(odd)))
-        self.odd = bool(odd)
+    def configure(self, symmetry: int):
+        """PLAIN: N(r); ODD: (N(r) - N(-r)) / 2; TIED: weights kept in the tied
+        odd form, so one evaluation is odd."""
+        check(self.L, self.L.hpcgb200_smoother_configure(self.h, int(symmetry)))
+        self.symmetry = int(symmetry)
 
     def close(self):
         if getattr(self, "h", None):
@@ -154,14 +157,14 @@ class Smoother:
     # -- weight files -------------------------------------------------------
     def save(self, path: str, **meta):
         w = self.get_weights()
-        meta = dict(meta, odd=self.odd, sha256=hashlib.sha256(w.tobytes()).hexdigest())
+        meta = dict(meta, symmetry=self.symmetry, sha256=hashlib.sha256(w.tobytes()).hexdigest())
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, w=w, meta=np.array(json.dumps(meta)))
 
     @classmethod
     def load(cls, path: str = DEFAULT_WEIGHTS) -> "Smoother":
         w, meta = read_weights(path)
-        s = cls(w, odd=bool(meta.get("odd", False)))
+        s = cls(w, symmetry=int(meta.get("symmetry", PLAIN)))
         s.meta = meta
         return s
 

@@ -50,7 +50,7 @@ def test_forward_matches_oracle(dims, nb, odd):
     rng = np.random.default_rng(1)
     per = int(np.prod(dims))
     w = LS.jacobi_weights(0.8, 0.1, 3)
-    S = LS.Smoother(w, odd=odd)
+    S = LS.Smoother(w, symmetry=LS.ODD if odd else LS.PLAIN)
     r = rng.standard_normal(nb * per).astype(np.float32)
     y = S.forward(dev(r), dims, nb)
     torch.cuda.synchronize()
@@ -73,7 +73,7 @@ def test_gradients_match_oracle(dims, nb, odd, kind):
     rng = np.random.default_rng(2)
     per = int(np.prod(dims))
     w = LS.jacobi_weights(0.8, 0.15, 5)
-    S = LS.Smoother(w, odd=odd)
+    S = LS.Smoother(w, symmetry=LS.ODD if odd else LS.PLAIN)
     r = rng.standard_normal(nb * per).astype(np.float32)
     e = (rng.standard_normal(nb * per) * 0.05).astype(np.float32)
     inv = LS.sample_norms(dev(e), dims, nb, kind)
@@ -163,3 +163,52 @@ def test_learned_cg_converges_and_falls_back():
     assert Pr.last_fallback() == 0
     assert r2["niters"] <= 2 * mixed["niters"]
     Pr.set_smoother(None)
+
+
+def test_tied_weights_make_an_odd_network():
+    dims = (12, 10, 16)
+    rng = np.random.default_rng(4)
+    S = LS.Smoother(LS.jacobi_weights(1.0, 0.1, 9, twin=8), symmetry=LS.TIED)
+    w = S.get_weights().reshape(3, 27, 16, 16)
+    # the projection holds: channel k+8 is the negated twin of channel k
+    assert np.array_equal(w[0, :, 0, 8:], -w[0, :, 0, :8])
+    assert np.array_equal(w[1, :, :8, :8], w[1, :, 8:, 8:]) and np.array_equal(w[1, :, :8, 8:], w[1, :, 8:, :8])
+    assert np.array_equal(w[2, :, 8:, 0], -w[2, :, :8, 0])
+    r = rng.standard_normal(int(np.prod(dims))).astype(np.float32)
+    y = S.forward(dev(r), dims).cpu().numpy()
+    ym = S.forward(dev(-r), dims).cpu().numpy()
+    assert np.linalg.norm(y + ym) <= 1e-2 * np.linalg.norm(y)
+    # training keeps the tied form
+    P = LS.make_pairs(32, 2, 1, 16, batch=8)
+    S.train([P], epochs=3, lr0=3e-3, lr1=1e-3, seed=2, kind=1)
+    w = S.get_weights().reshape(3, 27, 16, 16)
+    assert np.array_equal(w[0, :, 0, 8:], -w[0, :, 0, :8])
+    assert np.array_equal(w[2, :, 8:, 0], -w[2, :, :8, 0])
+
+
+def test_trained_weights_gain_over_untrained_and_report_vs_symgs():
+    """What training buys: the committed network (trained on the device by the
+    library's own kernels) against the same network at its initialisation (a
+    damped Jacobi step), on held-out pairs and inside the learned V-cycle; the
+    plain SymGS V-cycle is the method without the network and is reported."""
+    S = LS.Smoother.load()
+    meta = S.meta
+    init = LS.Smoother(LS.jacobi_weights(1.0, 0.02, 0), symmetry=S.symmetry)
+    held = LS.make_pairs(64, 2, 300001, 16)
+    inv = LS.sample_norms(held.e, held.dims, held.count, 1)
+    l_tr, _ = S.loss_grad(held.r, held.e, inv, held.dims, held.count, 1.0 / held.count, 1)
+    l_in, _ = init.loss_grad(held.r, held.e, inv, held.dims, held.count, 1.0 / held.count, 1)
+    assert l_tr < 0.5 * l_in, (l_tr, l_in)  # energy-norm error of N(r) vs the exact correction
+    P = R.Problem(128, 128, 128)
+    P.set_rhs(normal_rhs(P.rows[0], 9999))
+    mixed = P.cg(1000, 1e-9, mode=R.MODE_MIXED)
+    P.set_smoother(init, 2)
+    untrained = P.cg(1000, 1e-9, mode=R.MODE_LEARNED)
+    P.set_smoother(S, 2)
+    trained = P.cg(1000, 1e-9, mode=R.MODE_LEARNED)
+    assert trained["normr"] / trained["normr0"] <= 1e-9 and P.true_residual() <= 2e-9
+    assert trained["niters"] < untrained["niters"], (trained["niters"], untrained["niters"])
+    print(f"\nlearned smoother at 128^3: trained {trained['niters']} it, untrained {untrained['niters']} it, "
+          f"SymGS V-cycle {mixed['niters']} it; held-out energy error {l_tr:.4f} vs {l_in:.4f}; "
+          f"256^3 record: {meta['cg']['learned_iters']} vs {meta['cg']['mixed_iters']} it")
+    P.set_smoother(None)
