@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256"],
+                    help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--learned-nx", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
@@ -533,8 +535,32 @@ def run_mixed_only(args, R, barrier):
     return 0
 
 
+def run_profile_case(case: str) -> int:
+    """Small fixed workloads for ncu captures (see profiles/)."""
+    import torch
+
+    import rochpcg_b200 as R
+
+    torch.cuda.set_device(0)
+    if case == "conv":
+        # layer-2 convolution at MG level 2 of 256^3 (64^3 points, both odd branches)
+        print(json.dumps(conv_kernel_timing(2, 64, reps=2)))
+    elif case == "sweep128":
+        P = R.Problem(128)
+        print(json.dumps({"symgs_sweep_ms": P.time_op("symgs_sweep", 2)}))
+    else:
+        from rochpcg_b200 import learned as LS
+
+        P = R.Problem(256)
+        P.set_smoother(LS.Smoother.load(), 2)
+        print(json.dumps({"mg_learned_ms": P.time_op("mg_learned", 2), "mg_mixed_ms": P.time_op("mg_mixed", 2)}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        return run_profile_case(args.profile_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
