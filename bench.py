@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
     ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256"],
                     help="run one small case for a profiler and exit (no JSON line)")
+    ap.add_argument("--largest", action="store_true",
+                    help="also run configs[4]: 560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs")
     ap.add_argument("--learned-nx", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
@@ -352,6 +354,8 @@ def run_ours(args):
     if not args.no_learned:
         learned = learned_comparison(args, R, barrier)
 
+    largest = largest_comparison(args, R, barrier) if args.largest else None
+
     # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -380,7 +384,7 @@ def run_ours(args):
             "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m,
                     "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err},
             "roofline": roofline, "kernels": extra_kernels, "cpu_baseline": cpu, "mixed": mixed,
-            "learned": learned,
+            "learned": learned, "largest": largest,
             "gpu_launches": launches, "clocks": clocks,
         }
         print(json.dumps(line))
@@ -514,6 +518,51 @@ def learned_comparison(args, R, barrier, steps=2):
     res["grid"] = [n, n, n]
     res["rhs"] = "N(0,1) i.i.d., seed 9999"
     return res
+
+
+def largest_comparison(args, R, barrier):
+    """560 x 560 x 280 (87.8M rows), FP64 outer CG with the FP32
+    V-cycle and the learned level-2/3 smoother, against plain mixed and FP64,
+    for b ~ N(0,1) seed 7 and for the generated b (exact solution ones), all to
+    args.tol verified in FP64; fine-level bandwidth from the HPCG byte model
+    with the mixed path's element sizes."""
+    from rochpcg_b200 import learned as LS
+    from rochpcg_b200.rhs import normal_rhs
+
+    Q = R.Problem(560, 560, 280)
+    f, bytes64 = Q.model()
+    m = Q.rows[0]
+    S = LS.Smoother.load()
+    out = {"grid": [560, 560, 280], "rows": m}
+    for rhs in ("seed7", "ones"):
+        Q.set_rhs(normal_rhs(m, 7) if rhs == "seed7" else None)
+        res = {}
+        for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED), ("learned", R.MODE_LEARNED)):
+            if mode == R.MODE_LEARNED:
+                Q.set_smoother(S, 2)
+            Q.cg(args.max_iter, args.tol, mode=mode)  # warm-up
+            barrier()
+            r = Q.cg(args.max_iter, args.tol, mode=mode)
+            res[name] = {"time_to_1e-9_s": r["seconds"], "iterations": r["niters"],
+                         "rel_residual_fp64_true": Q.true_residual(),
+                         "gflops_hpcg_model": f * r["niters"] / r["seconds"] / 1e9}
+            if mode == R.MODE_FP64:
+                res[name]["model_GBps"] = bytes64 * r["niters"] / r["seconds"] / 1e9
+            if mode == R.MODE_LEARNED:
+                res[name]["fallback_iteration"] = Q.last_fallback()
+                Q.set_smoother(None)
+        res["speedup_learned_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
+        res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
+        out[rhs] = res
+    # fine-level FP32 sweep of the mixed path, timed alone
+    rows_c = m // 8
+    sw = Q.time_op("symgs32_sweep", 10)
+    out["fine_level_k32_sweep"] = {"ms": sw, "GBps": (rows_c * 12 + (m - rows_c) * 4) / (sw * 1e-3) / 1e9}
+    sw64 = Q.time_op("symgs_sweep", 10)
+    out["fine_level_k_symgs_sweep_fp64"] = {"ms": sw64, "GBps": (rows_c * (27 * 12 + 3 * 8) + (m - rows_c) * 8)
+                                            / (sw64 * 1e-3) / 1e9}
+    Q.close()
+    return out
 
 
 def measured_bf16_peak():

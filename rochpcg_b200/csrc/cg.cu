@@ -71,7 +71,11 @@ __global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const double* __rest
 {
     const int i = blockIdx.x * kBS + threadIdx.x;
     if(i >= n) return;
-    if(st->k == 1) p[i] = fma(0.0, z[i], z[i]);     // WAXPBY(1, z, 0, z)
+    // first iteration, and the first one after the learned smoother fell
+    // back: p = z (a restart: the old directions belong to the other
+    // preconditioner)
+    const bool restart = st->k == 1 || (st->fallback_iter > 0 && st->k == st->fallback_iter + 1);
+    if(restart) p[i] = fma(0.0, z[i], z[i]);         // WAXPBY(1, z, 0, z)
     else p[i] = fma(st->beta, p[i], z[i]);          // WAXPBY(1, z, beta, p)
 }
 

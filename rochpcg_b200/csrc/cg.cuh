@@ -20,7 +20,7 @@ struct CGState
     int flexible;         // 1: Polak-Ribiere beta (flexible CG); 0: Fletcher-Reeves as the reference
     int status;           // nonzero: a device-side check failed
     int net;              // learned smoother: 0 not used, 1 active, 2 failed to reduce normr (fell back)
-    int fallback_iter;    // iteration at which it failed (0: never)
+    int fallback_iter;    // iteration at which it failed (0: never); the next iteration restarts p = z
     int pad;
     double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
 };
