@@ -5,6 +5,7 @@
 // rounding sequence is exactly the ELL sweep's).
 #include <algorithm>
 #include <array>
+#include <utility>
 
 #include "mixed.cuh"
 
@@ -316,74 +317,350 @@ __global__ void __launch_bounds__(kBS32) k32_prolong(int nc, const int* __restri
 }
 
 // ----------------------------------------------------- FP64 stencil SpMV
+//
+// One launch for all colours: a block owns a natural-order tile of
+// 32 x 8 x 4 points, stages p on the tile and its one-point halo (34 x 10 x 6
+// doubles, 16 KB) in shared memory with coalesced loads from the colour
+// bricks, and computes every row of the tile from there.  Each warp holds
+// rows of one parity class (= one colour), so the row's ELL slot order --
+// that colour's order, read from a per-block table -- is warp-uniform, and
+// the sum is formed exactly like the ELL SpMV: sum = fma(a_ii, x_i, sum) at
+// the diagonal slot, sum - x_col (= fma(-1, x_col, sum)) at the others, absent
+// neighbours (+0.0 in the halo) leave it unchanged.  Bitwise equal to
+// k_spmv on the same matrix.
 
-// ELL: sum = fma(a, x_col, sum) per existing slot from 0.0, a = -1 off the
-// diagonal: fma(-1, x, s) == s - x, and an absent slot is s - (+0.0) == s.
-template <bool kEven>
-__device__ __forceinline__ double spmv64_row(const ColorLaunch& c, const StencilLevel& L, const BrickRow& b,
-                                             const double* __restrict__ diag, const double* __restrict__ x)
+constexpr int kT64X = 32, kT64Y = 8, kT64Z = 4;
+constexpr int kH64X = kT64X + 2, kH64Y = kT64Y + 2, kH64Z = kT64Z + 2;
+constexpr int kT64Threads = kT64X * kT64Y * kT64Z;  // 1024: 8 parity classes x 128 rows
+constexpr int kH64Points = kH64X * kH64Y * kH64Z;   // 2040
+
+__device__ __forceinline__ int natural_to_row(const StencilLevel& L, int z, int y, int x)
 {
-    double val[27];
-    gather<kOff, kEven>(L, c, b, x, 0.0, val);
-    const double d = diag[b.row];
-    const double xr = x[b.row];
-    double sum = 0.0;
+    const int v = L.color_of_par[((x & 1) << 2) | ((y & 1) << 1) | (z & 1)];
+    return L.offsets[v] + ((z >> 1) * L.by[v] + (y >> 1)) * L.bx[v] + (x >> 1);
+}
+
+inline dim3 tile64_grid(const StencilLevel& L)
+{
+    return dim3((unsigned)((L.nx + kT64X - 1) / kT64X), (unsigned)((L.ny + kT64Y - 1) / kT64Y),
+                (unsigned)((L.nz + kT64Z - 1) / kT64Z));
+}
+
+constexpr int kT64Loads = (kH64Points + kT64Threads - 1) / kT64Threads;  // halo values per thread: 2
+// Shared-memory layout of the staged tile: split by parity class into eight
+// sub-bricks of (34/2) x (10/2) x (6/2) points, so the rows of one class that a
+// warp holds (every other x) read consecutive doubles -- no bank conflicts.
+constexpr int kSbX = kH64X / 2, kSbY = kH64Y / 2, kSbZ = kH64Z / 2, kSbN = kSbX * kSbY * kSbZ;
+static_assert(kSbN * 8 == kH64Points, "sub-bricks cover the halo'd tile");
+
+// Halo coordinates (h = natural - tile origin + 1; origins are even) -> slot.
+__host__ __device__ constexpr int sub_index(int hx, int hy, int hz)
+{
+    const int par = (((hx + 1) & 1) << 2) | (((hy + 1) & 1) << 1) | ((hz + 1) & 1);
+    return par * kSbN + ((hz >> 1) * kSbY + (hy >> 1)) * kSbX + (hx >> 1);
+}
+
+struct Tile64
+{
+    int x0, y0, z0;
+};
+
+__device__ __forceinline__ Tile64 tile64_of(const StencilLevel& L, int tile)
+{
+    const int tx = (L.nx + kT64X - 1) / kT64X, ty = (L.ny + kT64Y - 1) / kT64Y;
+    const int bz = tile / (tx * ty), rem = tile - bz * tx * ty;
+    const int by = rem / tx, bx = rem - by * tx;
+    return Tile64{bx * kT64X, by * kT64Y, bz * kT64Z};
+}
+
+// This thread's halo values and its row's diagonal for tile t (loads only).
+__device__ __forceinline__ void tile64_load(const StencilLevel& L, const Tile64& t, int tid, int cls_x, int cls_y,
+                                            int cls_z, const double* __restrict__ p,
+                                            const double* __restrict__ diag, double (&hv)[kT64Loads], double& dv)
+{
 #pragma unroll
-    for(int j = 0; j < 27; ++j)
+    for(int k = 0; k < kT64Loads; ++k)
     {
-        if(j == c.tb.dp) sum = fma(d, xr, sum);
-        sum = sum - val[j];
+        const int e = tid + k * kT64Threads;
+        hv[k] = 0.0;
+        if(e < kH64Points)
+        {
+            const int hx = e % kH64X, hy = (e / kH64X) % kH64Y, hz = e / (kH64X * kH64Y);
+            const int x = t.x0 + hx - 1, y = t.y0 + hy - 1, z = t.z0 + hz - 1;
+            if(x >= 0 && x < L.nx && y >= 0 && y < L.ny && z >= 0 && z < L.nz) hv[k] = p[natural_to_row(L, z, y, x)];
+        }
     }
-    return sum;
+    const int x = t.x0 + cls_x, y = t.y0 + cls_y, z = t.z0 + cls_z;
+    dv = (x < L.nx && y < L.ny && z < L.nz) ? diag[natural_to_row(L, z, y, x)] : 0.0;
 }
 
-template <bool kEven>
-__global__ void __launch_bounds__(kBrickThreads) k64_spmv_color(const ColorLaunch c, const StencilLevel L,
-                                                                const double* __restrict__ diag,
-                                                                const double* __restrict__ x, double* __restrict__ y)
+// Persistent: a block walks tiles blockIdx.x, +gridDim.x, ...; the next
+// tile's loads are issued before the current tile is computed.
+template <bool kPap>
+__global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_tile(const StencilLevel L, const double* __restrict__ diag,
+                                                                const double* __restrict__ p,
+                                                                double* __restrict__ Ap, CGState* st,
+                                                                double* partial, unsigned int* ticket)
 {
-    const BrickRow b = brick_row(c, blockIdx.z);
-    if(!b.in) return;
-    y[b.row] = spmv64_row<kEven>(c, L, b, diag, x);
-}
-
-// Ap = A p on one colour and its blocks' partial sums of p.Ap into
-// partial[base + block].  The launch of the last colour (`finalize`) also
-// sums every partial of every colour launch (earlier launches are complete:
-// same stream) in index order and forms alpha = rtz / pAp.
-template <bool kEven>
-__global__ void __launch_bounds__(kBrickThreads) k64_pap_color(const ColorLaunch c, const StencilLevel L,
-                                                               const double* __restrict__ diag,
-                                                               const double* __restrict__ p, double* __restrict__ Ap,
-                                                               CGState* st, double* partial, int base, int total,
-                                                               unsigned int* ticket, int finalize)
-{
+    __shared__ double s_p[kH64Points];
+    __shared__ short s_delta[8][27];
+    __shared__ int s_dp[8];
     __shared__ double red[32];
     __shared__ bool last;
-    const BrickRow b = brick_row(c, blockIdx.z);
-    double s = 0.0;
-    if(b.in)
+    const int tid = threadIdx.x;
+    const int ntiles = ((L.nx + kT64X - 1) / kT64X) * ((L.ny + kT64Y - 1) / kT64Y) * ((L.nz + kT64Z - 1) / kT64Z);
+
+    // slot order of each parity class (its colour's ELL order) as offsets
+    // between sub-brick slots (the same for every point of the class)
+    if(tid < 8 * 27)
     {
-        const double sum = spmv64_row<kEven>(c, L, b, diag, p);
-        Ap[b.row] = sum;
-        s = sum * p[b.row];
+        const int cls = tid / 27, j = tid - cls * 27;
+        const unsigned e = L.tab[L.color_of_par[cls]].nb[j];
+        const int dx = (int)(e & 3) - 1, dy = (int)((e >> 2) & 3) - 1, dz = (int)((e >> 4) & 3) - 1;
+        const int hx = ((cls >> 2) & 1) + 1, hy = ((cls >> 1) & 1) + 1, hz = (cls & 1) + 1;
+        s_delta[cls][j] = (short)(sub_index(hx + dx, hy + dy, hz + dz) - sub_index(hx, hy, hz));
+        if(j == 0) s_dp[cls] = L.tab[L.color_of_par[cls]].dp;
     }
+    // thread -> (parity class, point of that class in the tile)
+    const int cls = tid >> 7, i = tid & 127;
+    const int lx = 2 * (i & 15) + ((cls >> 2) & 1);
+    const int ly = 2 * ((i >> 4) & 3) + ((cls >> 1) & 1);
+    const int lz = 2 * (i >> 6) + (cls & 1);
+    const int c = sub_index(lx + 1, ly + 1, lz + 1);
+
+    double hv[kT64Loads], dv = 0.0;
+    int tile = blockIdx.x;
+    if(tile < ntiles) tile64_load(L, tile64_of(L, tile), tid, lx, ly, lz, p, diag, hv, dv);
+    double s = 0.0;
+    for(; tile < ntiles; tile += gridDim.x)
+    {
+        const Tile64 t = tile64_of(L, tile);
+        __syncthreads();  // previous tile's reads of s_p are done
+#pragma unroll
+        for(int k = 0; k < kT64Loads; ++k)
+        {
+            const int e = tid + k * kT64Threads;
+            if(e < kH64Points) s_p[sub_index(e % kH64X, (e / kH64X) % kH64Y, e / (kH64X * kH64Y))] = hv[k];
+        }
+        const double d = dv;
+        __syncthreads();
+        if(tile + (int)gridDim.x < ntiles)
+            tile64_load(L, tile64_of(L, tile + gridDim.x), tid, lx, ly, lz, p, diag, hv, dv);
+        const int x = t.x0 + lx, y = t.y0 + ly, z = t.z0 + lz;
+        if(x < L.nx && y < L.ny && z < L.nz)
+        {
+            const double xr = s_p[c];
+            const int dp = s_dp[cls];
+            double sum = 0.0;
+#pragma unroll
+            for(int j = 0; j < 27; ++j)
+            {
+                if(j == dp) sum = fma(d, xr, sum);
+                else sum = sum - s_p[c + s_delta[cls][j]];
+            }
+            Ap[natural_to_row(L, z, y, x)] = sum;
+            if(kPap) s = fma(sum, xr, s);
+        }
+    }
+    if(!kPap) return;
     s = block_sum(s, red);
-    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    const int tid = block_tid();
-    if(tid == 0) partial[base + bid] = s;
-    if(!finalize) return;
     if(tid == 0)
     {
+        partial[blockIdx.x] = s;
         __threadfence();
-        last = atomicAdd(ticket, 1u) == nblocks - 1;
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if(!last) return;
     __threadfence();
     double acc = 0.0;
-    for(int i = tid; i < total; i += (int)kBrickThreads) acc += __ldcg(&partial[i]);
+    for(int k = tid; k < (int)gridDim.x; k += kT64Threads) acc += __ldcg(&partial[k]);
+    acc = block_sum(acc, red);
+    if(tid == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
+
+// ---- specialisation for the colouring the reference's JPL rounds produce
+// (parity class -> colour 7,2,3,6,5,4,1,0 on every grid it was run on): the
+// slot order of each class is a compile-time list, so the 27 neighbour reads
+// use immediate offsets and the staging needs no per-element divisions.
+// Levels with any other colour map take k64_spmv_tile.
+constexpr int kCanonColor[8] = {7, 2, 3, 6, 5, 4, 1, 0};
+
+struct CanonSlots
+{
+    int delta[27];  // sub-brick slot offset of ELL slot j for a point of the class
+    int dp;         // slot of the diagonal
+};
+
+__host__ __device__ constexpr CanonSlots canon_slots(int cls)
+{
+    CanonSlots r{};
+    int key[27] = {}, dxs[27] = {}, dys[27] = {}, dzs[27] = {};
+    int k = 0;
+    for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy)
+            for(int dx = -1; dx <= 1; ++dx)
+            {
+                const int col = kCanonColor[cls ^ (((dx & 1) << 2) | ((dy & 1) << 1) | (dz & 1))];
+                key[k] = ((col * 3 + (dz + 1)) * 3 + (dy + 1)) * 3 + (dx + 1);  // (colour, dz, dy, dx) order
+                dxs[k] = dx;
+                dys[k] = dy;
+                dzs[k] = dz;
+                ++k;
+            }
+    for(int a = 1; a < 27; ++a)
+        for(int b = a; b > 0 && key[b - 1] > key[b]; --b)
+        {
+            int t = key[b]; key[b] = key[b - 1]; key[b - 1] = t;
+            t = dxs[b]; dxs[b] = dxs[b - 1]; dxs[b - 1] = t;
+            t = dys[b]; dys[b] = dys[b - 1]; dys[b - 1] = t;
+            t = dzs[b]; dzs[b] = dzs[b - 1]; dzs[b - 1] = t;
+        }
+    const int hx = ((cls >> 2) & 1) + 1, hy = ((cls >> 1) & 1) + 1, hz = (cls & 1) + 1;
+    for(int j = 0; j < 27; ++j)
+    {
+        r.delta[j] = sub_index(hx + dxs[j], hy + dys[j], hz + dzs[j]) - sub_index(hx, hy, hz);
+        if(dxs[j] == 0 && dys[j] == 0 && dzs[j] == 0) r.dp = j;
+    }
+    return r;
+}
+
+template <int kCls>
+struct Canon
+{
+    static constexpr CanonSlots s = canon_slots(kCls);
+};
+
+template <int kCls, int J>
+__device__ __forceinline__ void canon_step(double& sum, const double* sp, int c, double d, double xr)
+{
+    constexpr int delta = Canon<kCls>::s.delta[J];
+    if constexpr(J == Canon<kCls>::s.dp) sum = fma(d, xr, sum);
+    else sum = sum - sp[c + delta];
+}
+
+template <int kCls, int... J>
+__device__ __forceinline__ double canon_row(const double* sp, int c, double d, double xr,
+                                            std::integer_sequence<int, J...>)
+{
+    double sum = 0.0;
+    (canon_step<kCls, J>(sum, sp, c, d, xr), ...);  // slots in ELL order, left to right
+    return sum;
+}
+
+constexpr int kHaloLines = kH64Y * kH64Z;  // 60 lines of 34 points
+
+template <bool kPap>
+__global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_canon(const StencilLevel L, const double* __restrict__ diag,
+                                                                 const double* __restrict__ p,
+                                                                 double* __restrict__ Ap, CGState* st,
+                                                                 double* partial, unsigned int* ticket)
+{
+    __shared__ double s_p[kH64Points];
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tx = (L.nx + kT64X - 1) / kT64X, ty = (L.ny + kT64Y - 1) / kT64Y;
+    const int ntiles = tx * ty * ((L.nz + kT64Z - 1) / kT64Z);
+    const int cls = tid >> 7, i = tid & 127;
+    const int lx = 2 * (i & 15) + ((cls >> 2) & 1);
+    const int ly = 2 * ((i >> 4) & 3) + ((cls >> 1) & 1);
+    const int lz = 2 * (i >> 6) + (cls & 1);
+    const int c = sub_index(lx + 1, ly + 1, lz + 1);
+    const int vown = L.color_of_par[cls];
+
+    // halo line q of this warp = warp + 32 q; lane covers hx = lane and lane + 32
+    double hv[2][2], dv = 0.0;
+    auto load = [&](int tile) {
+        const int bz = tile / (tx * ty), rem = tile - bz * tx * ty, by = rem / tx, bx = rem - by * tx;
+        const int x0 = bx * kT64X, y0 = by * kT64Y, z0 = bz * kT64Z;
+#pragma unroll
+        for(int q = 0; q < 2; ++q)
+        {
+            const int line = warp + 32 * q;
+            hv[q][0] = hv[q][1] = 0.0;
+            if(line >= kHaloLines) continue;
+            const int hy = line % kH64Y, hz = line / kH64Y;
+            const int y = y0 + hy - 1, z = z0 + hz - 1;
+            if(y < 0 || y >= L.ny || z < 0 || z >= L.nz) continue;
+            const int pe = ((y & 1) << 1) | (z & 1);
+            const int ve = L.color_of_par[pe], vo = L.color_of_par[4 | pe];
+            const int be = L.offsets[ve] + ((z >> 1) * L.by[ve] + (y >> 1)) * L.bx[ve];
+            const int bo = L.offsets[vo] + ((z >> 1) * L.by[vo] + (y >> 1)) * L.bx[vo];
+#pragma unroll
+            for(int a = 0; a < 2; ++a)
+            {
+                const int hx = lane + 32 * a;
+                const int x = x0 + hx - 1;
+                if(hx < kH64X && x >= 0 && x < L.nx) hv[q][a] = p[((x & 1) ? bo : be) + (x >> 1)];
+            }
+        }
+        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+        dv = (x < L.nx && y < L.ny && z < L.nz)
+                 ? diag[L.offsets[vown] + ((z >> 1) * L.by[vown] + (y >> 1)) * L.bx[vown] + (x >> 1)]
+                 : 0.0;
+    };
+
+    int tile = blockIdx.x;
+    if(tile < ntiles) load(tile);
+    double s = 0.0;
+    for(; tile < ntiles; tile += gridDim.x)
+    {
+        const int bz = tile / (tx * ty), rem = tile - bz * tx * ty, by = rem / tx, bx = rem - by * tx;
+        const int x = bx * kT64X + lx, y = by * kT64Y + ly, z = bz * kT64Z + lz;
+        __syncthreads();  // previous tile's reads of s_p are done
+#pragma unroll
+        for(int q = 0; q < 2; ++q)
+        {
+            const int line = warp + 32 * q;
+            if(line >= kHaloLines) continue;
+            const int hy = line % kH64Y, hz = line / kH64Y;
+#pragma unroll
+            for(int a = 0; a < 2; ++a)
+                if(lane + 32 * a < kH64X) s_p[sub_index(lane + 32 * a, hy, hz)] = hv[q][a];
+        }
+        const double d = dv;
+        __syncthreads();
+        if(tile + (int)gridDim.x < ntiles) load(tile + gridDim.x);
+        if(x < L.nx && y < L.ny && z < L.nz)
+        {
+            const double xr = s_p[c];
+            double sum;
+            using Seq = std::make_integer_sequence<int, 27>;
+            switch(cls)
+            {
+                case 0: sum = canon_row<0>(s_p, c, d, xr, Seq{}); break;
+                case 1: sum = canon_row<1>(s_p, c, d, xr, Seq{}); break;
+                case 2: sum = canon_row<2>(s_p, c, d, xr, Seq{}); break;
+                case 3: sum = canon_row<3>(s_p, c, d, xr, Seq{}); break;
+                case 4: sum = canon_row<4>(s_p, c, d, xr, Seq{}); break;
+                case 5: sum = canon_row<5>(s_p, c, d, xr, Seq{}); break;
+                case 6: sum = canon_row<6>(s_p, c, d, xr, Seq{}); break;
+                default: sum = canon_row<7>(s_p, c, d, xr, Seq{}); break;
+            }
+            Ap[L.offsets[vown] + ((z >> 1) * L.by[vown] + (y >> 1)) * L.bx[vown] + (x >> 1)] = sum;
+            if(kPap) s = fma(sum, xr, s);
+        }
+    }
+    if(!kPap) return;
+    s = block_sum(s, red);
+    if(tid == 0)
+    {
+        partial[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(int k = tid; k < (int)gridDim.x; k += kT64Threads) acc += __ldcg(&partial[k]);
     acc = block_sum(acc, red);
     if(tid == 0)
     {
@@ -537,46 +814,42 @@ int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc
     return 0;
 }
 
-size_t stencil_pap_partials(const StencilLevel& L)
+// Persistent grid: two 1024-thread blocks per SM (148 SMs on B200), never more
+// blocks than tiles.
+static int tile64_blocks(const StencilLevel& L)
 {
-    size_t n = 0;
-    for(int v = 0; v < L.ncolors; ++v)
-    {
-        const dim3 g = brick_grid(color_launch(L, v));
-        n += (size_t)g.x * g.y * g.z;
-    }
-    return n;
+    const dim3 g = tile64_grid(L);
+    const long tiles = (long)g.x * g.y * g.z;
+    return (int)(tiles < 2 * 148 ? tiles : 2 * 148);
+}
+
+size_t stencil_pap_partials(const StencilLevel& L) { return (size_t)tile64_blocks(L); }
+
+static bool canonical_colours(const StencilLevel& L)
+{
+    for(int q = 0; q < 8; ++q)
+        if(L.color_of_par[q] != kCanonColor[q]) return false;
+    return true;
 }
 
 int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s)
 {
-    for(int v = 0; v < L.ncolors; ++v)
-    {
-        const ColorLaunch c = color_launch(L, v);
-        if(L.even) k64_spmv_color<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, diag, x, y);
-        else k64_spmv_color<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, diag, x, y);
-        HB_LAUNCHED();
-    }
+    if(canonical_colours(L))
+        k64_spmv_canon<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+    else
+        k64_spmv_tile<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+    HB_LAUNCHED();
     return 0;
 }
 
 int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
-    const int total = (int)stencil_pap_partials(L);
-    int base = 0;
-    for(int v = 0; v < L.ncolors; ++v)
-    {
-        const ColorLaunch c = color_launch(L, v);
-        const dim3 g = brick_grid(c);
-        const int fin = v == L.ncolors - 1;
-        if(L.even)
-            k64_pap_color<true><<<g, dim3(32, 8), 0, s>>>(c, L, diag, p, Ap, st, partial, base, total, ticket, fin);
-        else
-            k64_pap_color<false><<<g, dim3(32, 8), 0, s>>>(c, L, diag, p, Ap, st, partial, base, total, ticket, fin);
-        HB_LAUNCHED();
-        base += (int)(g.x * g.y * g.z);
-    }
+    if(canonical_colours(L))
+        k64_spmv_canon<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
+    else
+        k64_spmv_tile<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
+    HB_LAUNCHED();
     return 0;
 }
 

@@ -58,7 +58,7 @@ def test_mixed_test_symmetry_and_test_cg():
     assert t["count_fail"] == 0, t
 
 
-@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32), (24, 40, 56), (72, 40, 48)])
 def test_stencil_spmv_equals_ell_spmv_bitwise(dims):
     """The mixed path's implicit FP64 operator is the ELL operator, bit for bit."""
     P, O = problems(*dims)
