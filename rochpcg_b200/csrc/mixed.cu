@@ -491,6 +491,7 @@ __global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_tile(const StencilLev
 // use immediate offsets and the staging needs no per-element divisions.
 // Levels with any other colour map take k64_spmv_tile.
 constexpr int kCanonColor[8] = {7, 2, 3, 6, 5, 4, 1, 0};
+static_assert(((0x01456327u >> 0) & 15u) == 7 && ((0x01456327u >> 28) & 15u) == 0, "packed canonical colours");
 
 struct CanonSlots
 {
@@ -670,6 +671,219 @@ __global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_canon(const StencilLe
     }
 }
 
+
+// ---- plane march (canonical colouring): a block owns a 64 x 4 column of the
+// grid and walks a chunk of z planes with a ring of four staged planes
+// (66 x 6 doubles each, halo included, x split by parity so a warp's reads
+// are consecutive).  Per step it stores the prefetched plane z+2, issues the
+// loads of plane z+3, computes the rows of plane z with the compile-time slot
+// order, and synchronises once.  Each warp holds one x parity and one y row,
+// so the parity class (= colour) of its rows is warp-uniform.
+constexpr int kMX = 64, kMY = 4, kMZ = 16;                 // column, z chunk
+constexpr int kMThreads = (kMX / 2) * 2 * kMY;             // 256: (32 lanes) x (2 x-parities) x (4 rows)
+constexpr int kPX = kMX + 2, kPY = kMY + 2;                // staged plane 66 x 6
+constexpr int kPXh = kPX / 2;                              // 33 per x parity
+constexpr int kPlane = kPX * kPY;                          // 396
+constexpr int kMLoads = (kPlane + kMThreads - 1) / kMThreads;  // 2 per thread
+
+// Plane slot of halo coordinates (hx = x - x0 + 1, hy = y - y0 + 1; x0, y0 even).
+__host__ __device__ constexpr int plane_slot(int hx, int hy) { return (hy * 2 + ((hx + 1) & 1)) * kPXh + (hx >> 1); }
+
+struct MarchSlots
+{
+    int off[27];  // plane-slot offset of slot j (same plane index layout for every dz)
+    int dz[27];   // plane of slot j relative to the row's plane
+    int dp;
+};
+
+__host__ __device__ constexpr MarchSlots march_slots(int cls)
+{
+    MarchSlots r{};
+    int key[27] = {}, dxs[27] = {}, dys[27] = {}, dzs[27] = {};
+    int k = 0;
+    for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy)
+            for(int dx = -1; dx <= 1; ++dx)
+            {
+                const int col = kCanonColor[cls ^ (((dx & 1) << 2) | ((dy & 1) << 1) | (dz & 1))];
+                key[k] = ((col * 3 + (dz + 1)) * 3 + (dy + 1)) * 3 + (dx + 1);
+                dxs[k] = dx;
+                dys[k] = dy;
+                dzs[k] = dz;
+                ++k;
+            }
+    for(int a = 1; a < 27; ++a)
+        for(int b = a; b > 0 && key[b - 1] > key[b]; --b)
+        {
+            int t = key[b]; key[b] = key[b - 1]; key[b - 1] = t;
+            t = dxs[b]; dxs[b] = dxs[b - 1]; dxs[b - 1] = t;
+            t = dys[b]; dys[b] = dys[b - 1]; dys[b - 1] = t;
+            t = dzs[b]; dzs[b] = dzs[b - 1]; dzs[b - 1] = t;
+        }
+    // any point of the class: x parity (cls>>2)&1, y parity (cls>>1)&1 (x0, y0 even)
+    const int hx = ((cls >> 2) & 1) + 1, hy = ((cls >> 1) & 1) + 1;
+    for(int j = 0; j < 27; ++j)
+    {
+        r.off[j] = plane_slot(hx + dxs[j], hy + dys[j]) - plane_slot(hx, hy);
+        r.dz[j] = dzs[j];
+        if(dxs[j] == 0 && dys[j] == 0 && dzs[j] == 0) r.dp = j;
+    }
+    return r;
+}
+
+template <int kCls>
+struct MarchTab
+{
+    static constexpr MarchSlots s = march_slots(kCls);
+};
+
+template <int kCls, int J>
+__device__ __forceinline__ void march_step(double& sum, const double* pm, const double* p0, const double* pp, double d,
+                                           double xr)
+{
+    constexpr int off = MarchTab<kCls>::s.off[J];
+    constexpr int dz = MarchTab<kCls>::s.dz[J];
+    if constexpr(J == MarchTab<kCls>::s.dp) sum = fma(d, xr, sum);
+    else sum = sum - (dz < 0 ? pm : (dz == 0 ? p0 : pp))[off];
+}
+
+template <int kCls, int... J>
+__device__ __forceinline__ double march_row(const double* pm, const double* p0, const double* pp, double d, double xr,
+                                            std::integer_sequence<int, J...>)
+{
+    double sum = 0.0;
+    (march_step<kCls, J>(sum, pm, p0, pp, d, xr), ...);  // slots in ELL order, left to right
+    return sum;
+}
+
+// Colour-permuted row of natural (x, y, z) for the canonical colouring.
+__device__ __forceinline__ int canon_row_of(const StencilLevel& L, int x, int y, int z)
+{
+    // kCanonColor packed in nibbles (parity class 0 in the lowest)
+    const int v = (int)((0x01456327u >> (4 * (((x & 1) << 2) | ((y & 1) << 1) | (z & 1)))) & 15u);
+    return L.offsets[v] + ((z >> 1) * L.by[v] + (y >> 1)) * L.bx[v] + (x >> 1);
+}
+
+template <bool kPap>
+__global__ void __launch_bounds__(kMThreads) k64_spmv_march(const StencilLevel L, const double* __restrict__ diag,
+                                                            const double* __restrict__ p, double* __restrict__ Ap,
+                                                            CGState* st, double* partial, unsigned int* ticket)
+{
+    __shared__ double ring[4][kPlane];
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, zb = blockIdx.z * kMZ;
+    const int ze = zb + kMZ < L.nz ? zb + kMZ : L.nz;
+
+    // this thread's staged positions (fixed for every plane) and whether they exist
+    int hxs[kMLoads], hys[kMLoads];
+    bool inxy[kMLoads];
+#pragma unroll
+    for(int k = 0; k < kMLoads; ++k)
+    {
+        const int e = tid + k * kMThreads;
+        hxs[k] = e % kPX;
+        hys[k] = e / kPX;
+        const int x = x0 + hxs[k] - 1, y = y0 + hys[k] - 1;
+        inxy[k] = e < kPlane && x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+    }
+    auto load_plane = [&](int z, double (&v)[kMLoads]) {
+#pragma unroll
+        for(int k = 0; k < kMLoads; ++k)
+        {
+            v[k] = 0.0;
+            if(inxy[k] && z >= 0 && z < L.nz) v[k] = p[canon_row_of(L, x0 + hxs[k] - 1, y0 + hys[k] - 1, z)];
+        }
+    };
+    auto store_plane = [&](int z, const double (&v)[kMLoads]) {
+        double* dst = ring[(z + 4) & 3];
+#pragma unroll
+        for(int k = 0; k < kMLoads; ++k)
+            if(tid + k * kMThreads < kPlane) dst[plane_slot(hxs[k], hys[k])] = v[k];
+    };
+
+    // own column: warp -> (x parity, row); lane -> x
+    const int px = warp & 1, ly = warp >> 1;
+    const int lx = 2 * lane + px;
+    const int x = x0 + lx, y = y0 + ly;
+    const bool mine = x < L.nx && y < L.ny;
+    const int c = plane_slot(lx + 1, ly + 1);
+
+    double hv[kMLoads];
+    load_plane(zb - 1, hv);
+    store_plane(zb - 1, hv);
+    load_plane(zb, hv);
+    store_plane(zb, hv);
+    load_plane(zb + 1, hv);
+    store_plane(zb + 1, hv);
+    load_plane(zb + 2, hv);
+    double dv = (mine && zb < ze) ? diag[canon_row_of(L, x, y, zb)] : 0.0;
+    __syncthreads();
+    double s = 0.0;
+    for(int z = zb; z < ze; ++z)
+    {
+        store_plane(z + 2, hv);  // ring slot of plane z-2: free since the last step
+        const double d = dv;
+        if(z + 1 < ze)
+        {
+            load_plane(z + 3, hv);
+            dv = mine ? diag[canon_row_of(L, x, y, z + 1)] : 0.0;
+        }
+        if(mine)
+        {
+            const double* pm = ring[(z + 3) & 3];
+            const double* p0 = ring[(z + 4) & 3];
+            const double* pp = ring[(z + 5) & 3];
+            const double xr = p0[c];
+            double sum;
+            using Seq = std::make_integer_sequence<int, 27>;
+            switch((px << 2) | ((ly & 1) << 1) | (z & 1))
+            {
+                case 0: sum = march_row<0>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 1: sum = march_row<1>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 2: sum = march_row<2>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 3: sum = march_row<3>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 4: sum = march_row<4>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 5: sum = march_row<5>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 6: sum = march_row<6>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                default: sum = march_row<7>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+            }
+            Ap[canon_row_of(L, x, y, z)] = sum;
+            if(kPap) s = fma(sum, xr, s);
+        }
+        __syncthreads();  // plane z+2 stored, plane z-1 no longer read
+    }
+    if(!kPap) return;
+    s = block_sum(s, red);
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    if(tid == 0)
+    {
+        partial[bid] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == nblocks - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(int k = tid; k < (int)nblocks; k += kMThreads) acc += __ldcg(&partial[k]);
+    acc = block_sum(acc, red);
+    if(tid == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
+inline dim3 march_grid(const StencilLevel& L)
+{
+    return dim3((unsigned)((L.nx + kMX - 1) / kMX), (unsigned)((L.ny + kMY - 1) / kMY),
+                (unsigned)((L.nz + kMZ - 1) / kMZ));
+}
+
 // ------------------------------------------------------------ set-up kernels
 
 __global__ void k_diag32(int m, const double* __restrict__ diag, float* __restrict__ d32, float* __restrict__ inv32)
@@ -823,7 +1037,12 @@ static int tile64_blocks(const StencilLevel& L)
     return (int)(tiles < 2 * 148 ? tiles : 2 * 148);
 }
 
-size_t stencil_pap_partials(const StencilLevel& L) { return (size_t)tile64_blocks(L); }
+size_t stencil_pap_partials(const StencilLevel& L)
+{
+    const dim3 g = march_grid(L);
+    const size_t march = (size_t)g.x * g.y * g.z;
+    return march > (size_t)tile64_blocks(L) ? march : (size_t)tile64_blocks(L);
+}
 
 static bool canonical_colours(const StencilLevel& L)
 {
@@ -835,7 +1054,7 @@ static bool canonical_colours(const StencilLevel& L)
 int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s)
 {
     if(canonical_colours(L))
-        k64_spmv_canon<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+        k64_spmv_march<false><<<march_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
     else
         k64_spmv_tile<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
     HB_LAUNCHED();
@@ -846,7 +1065,7 @@ int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, cons
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
     if(canonical_colours(L))
-        k64_spmv_canon<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
+        k64_spmv_march<true><<<march_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
     else
         k64_spmv_tile<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
     HB_LAUNCHED();
