@@ -316,6 +316,163 @@ __global__ void __launch_bounds__(kBS32) k32_prolong(int nc, const int* __restri
     xf[inj_f[ic]] += xc[inj_c[ic]];
 }
 
+
+// ------------------------------------------------ 4-row vector sweeps (even grids)
+//
+// When every colour brick's x extent is a multiple of 4 (and hence every
+// colour's offset), a thread updates four consecutive rows of a brick line.
+// Their neighbours in any slot are four consecutive floats of the neighbour's
+// brick: one aligned float4 when the slot's column offset is a multiple of 4,
+// two otherwise -- instead of four scalar gathers.  Each row keeps the ELL
+// slot order and the -0.0f no-op for missing neighbours, so results are the
+// same bits as the one-row kernels above.
+constexpr int kV4X = 8, kV4Y = 32;  // block: 8 x 32 threads, 32 rows x 32 lines of a brick plane
+
+inline bool vec4_ok(const StencilLevel& L)
+{
+    if(!L.even) return false;
+    for(int v = 0; v < L.ncolors; ++v)
+        if(L.bx[v] % 4 || L.offsets[v] % 4) return false;
+    return true;
+}
+
+inline dim3 brick_grid4(const ColorLaunch& c)
+{
+    return dim3((unsigned)((c.bx + 4 * kV4X - 1) / (4 * kV4X)), (unsigned)((c.by + kV4Y - 1) / kV4Y), (unsigned)c.bz);
+}
+
+struct Rows4
+{
+    int row0;
+    bool in;
+    unsigned mask[4];
+    bool fast;
+};
+
+__device__ __forceinline__ Rows4 rows4(const ColorLaunch& c, int kz)
+{
+    Rows4 b;
+    const int kx0 = (blockIdx.x * kV4X + threadIdx.x) * 4;
+    const int ky = blockIdx.y * kV4Y + threadIdx.y;
+    b.in = kx0 < c.bx && ky < c.by && kz < c.bz;  // bx % 4 == 0: all four rows or none
+    const int iy = 2 * ky + ((c.par >> 1) & 1), iz = 2 * kz + (c.par & 1);
+    unsigned any = 0;
+#pragma unroll
+    for(int r = 0; r < 4; ++r)
+    {
+        const int ix = 2 * (kx0 + r) + ((c.par >> 2) & 1);
+        b.mask[r] = b.in ? face_mask(c, ix, iy, iz) : 0u;
+        any |= b.mask[r];
+    }
+    b.fast = __all_sync(0xffffffffu, any == 0u);
+    b.row0 = c.off + (kz * c.by + ky) * c.bx + kx0;
+    return b;
+}
+
+__device__ __forceinline__ float4 ld4(const float* x, int i, int m)
+{
+    return (i >= 0 && i + 4 <= m) ? *reinterpret_cast<const float4*>(x + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// x[base .. base+3]; s = base & 3 is the same for every thread of the launch.
+__device__ __forceinline__ void load4(const float* x, int base, int m, int s, float (&v)[4])
+{
+    if(s == 0)
+    {
+        const float4 a = ld4(x, base, m);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        return;
+    }
+    const int lo = base - s;
+    const float4 a = ld4(x, lo, m), b = ld4(x, lo + 4, m);
+    if(s == 1) { v[0] = a.y; v[1] = a.z; v[2] = a.w; v[3] = b.x; }
+    else if(s == 2) { v[0] = a.z; v[1] = a.w; v[2] = b.x; v[3] = b.y; }
+    else { v[0] = a.w; v[1] = b.x; v[2] = b.y; v[3] = b.z; }
+}
+
+template <int kSel>
+__device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b, const float* x, int m,
+                                           float (&sum)[4])
+{
+#pragma unroll
+    for(int j = 0; j < 27; ++j)
+    {
+        if(!selected<kSel>(j, c.tb.dp)) continue;
+        float v[4];
+        load4(x, b.row0 + c.tb.delta[j], m, c.tb.delta[j] & 3, v);
+        if(b.fast)
+        {
+#pragma unroll
+            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + v[r];
+        }
+        else
+        {
+#pragma unroll
+            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & c.tb.bmask[j]) ? -0.0f : v[r]);
+        }
+    }
+}
+
+template <bool kFromDouble>
+__global__ void __launch_bounds__(kV4X * kV4Y) k32v_fwd0(const ColorLaunch c, const StencilLevel L,
+                                                         const float* __restrict__ inv_diag32,
+                                                         const double* __restrict__ r64, float* __restrict__ r32,
+                                                         float* x)
+{
+    const Rows4 b = rows4(c, blockIdx.z);
+    if(!b.in) return;
+    float sum[4];
+    if(kFromDouble)
+    {
+        const double2 a = *reinterpret_cast<const double2*>(r64 + b.row0);
+        const double2 a2 = *reinterpret_cast<const double2*>(r64 + b.row0 + 2);
+        sum[0] = (float)a.x; sum[1] = (float)a.y; sum[2] = (float)a2.x; sum[3] = (float)a2.y;
+        *reinterpret_cast<float4*>(r32 + b.row0) = make_float4(sum[0], sum[1], sum[2], sum[3]);
+    }
+    else
+    {
+        const float4 a = *reinterpret_cast<const float4*>(r32 + b.row0);
+        sum[0] = a.x; sum[1] = a.y; sum[2] = a.z; sum[3] = a.w;
+    }
+    if(c.tb.dp > 0) add_slots4<kBefore>(c, b, x, L.m, sum);
+    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
+    *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
+}
+
+__global__ void __launch_bounds__(kV4X * kV4Y) k32v_bwd0(const ColorLaunch c, const StencilLevel L,
+                                                         const float* __restrict__ diag32,
+                                                         const float* __restrict__ inv_diag32, float* x)
+{
+    const Rows4 b = rows4(c, blockIdx.z);
+    if(!b.in) return;
+    const float4 xv = *reinterpret_cast<const float4*>(x + b.row0);
+    const float4 dv = *reinterpret_cast<const float4*>(diag32 + b.row0);
+    float sum[4] = {__fmul_rn(xv.x, dv.x), __fmul_rn(xv.y, dv.y), __fmul_rn(xv.z, dv.z), __fmul_rn(xv.w, dv.w)};
+    add_slots4<kAfter>(c, b, x, L.m, sum);
+    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
+    *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
+}
+
+__global__ void __launch_bounds__(kV4X * kV4Y) k32v_sweep(const ColorLaunch c, const StencilLevel L,
+                                                          const float* __restrict__ inv_diag32,
+                                                          const float* __restrict__ r, float* x,
+                                                          double* __restrict__ z64)
+{
+    const Rows4 b = rows4(c, blockIdx.z);
+    if(!b.in) return;
+    const float4 rv = *reinterpret_cast<const float4*>(r + b.row0);
+    float sum[4] = {rv.x, rv.y, rv.z, rv.w};
+    add_slots4<kOff>(c, b, x, L.m, sum);
+    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
+    const float4 xn = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
+    *reinterpret_cast<float4*>(x + b.row0) = xn;
+    if(z64)
+    {
+        *reinterpret_cast<double2*>(z64 + b.row0) = make_double2((double)xn.x, (double)xn.y);
+        *reinterpret_cast<double2*>(z64 + b.row0 + 2) = make_double2((double)xn.z, (double)xn.w);
+    }
+}
+
 // ----------------------------------------------------- FP64 stencil SpMV
 //
 // One launch for all colours: a block owns a natural-order tile of
@@ -964,13 +1121,19 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
                         float* r32, float* x, cudaStream_t s)
 {
     const int n = L.ncolors;
-    const dim3 t(32, 8);
+    const dim3 t(32, 8), t4(kV4X, kV4Y);
+    const bool vec = vec4_ok(L);
     for(int v = 0; v < n; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const dim3 g = brick_grid(c);
-        if(L.even)
+        if(vec)
+        {
+            if(r64) k32v_fwd0<true><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else k32v_fwd0<false><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+        }
+        else if(L.even)
         {
             if(r64) k32_fwd0<true, true><<<g, t, 0, s>>>(c, L, inv_diag32, r64, r32, x);
             else k32_fwd0<true, false><<<g, t, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
@@ -986,7 +1149,8 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
+        if(vec) k32v_bwd0<<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        else if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         HB_LAUNCHED();
     }
@@ -997,10 +1161,12 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
                    cudaStream_t s)
 {
     const int n = L.ncolors;
+    const bool vec = vec4_ok(L);
     auto sweep = [&](int v, double* z) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
+        if(vec) k32v_sweep<<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+        else if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         else k32_sweep<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         HB_LAUNCHED();
         return 0;
