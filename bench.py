@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
-    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256"],
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256", "mixed320"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--largest", action="store_true",
                     help="also run configs[4]: 560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs")
@@ -597,6 +597,10 @@ def run_profile_case(case: str) -> int:
     elif case == "sweep128":
         P = R.Problem(128)
         print(json.dumps({"symgs_sweep_ms": P.time_op("symgs_sweep", 2)}))
+    elif case == "mixed320":
+        # one mixed V-cycle + one stencil SpMV at 320^3 (eager launches)
+        P = R.Problem(320)
+        print(json.dumps({"mg_mixed_ms": P.time_op("mg_mixed", 1), "spmv_stencil_ms": P.time_op("spmv_stencil", 1)}))
     else:
         from rochpcg_b200 import learned as LS
 

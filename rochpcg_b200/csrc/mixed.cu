@@ -390,25 +390,40 @@ __device__ __forceinline__ void load4(const float* x, int base, int m, int s, fl
     else { v[0] = a.w; v[1] = b.x; v[2] = b.y; v[3] = b.z; }
 }
 
+#ifndef HB_V4_GROUP
+#define HB_V4_GROUP 3
+#endif
+constexpr int kV4Group = HB_V4_GROUP;  // slots whose loads are issued together before their in-order adds
+
 template <int kSel>
 __device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b, const float* x, int m,
                                            float (&sum)[4])
 {
 #pragma unroll
-    for(int j = 0; j < 27; ++j)
+    for(int g = 0; g < 27; g += kV4Group)
     {
-        if(!selected<kSel>(j, c.tb.dp)) continue;
-        float v[4];
-        load4(x, b.row0 + c.tb.delta[j], m, c.tb.delta[j] & 3, v);
-        if(b.fast)
-        {
+        float v[kV4Group][4];
 #pragma unroll
-            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + v[r];
+        for(int k = 0; k < kV4Group; ++k)
+        {
+            const int j = g + k;
+            if(j < 27 && selected<kSel>(j, c.tb.dp)) load4(x, b.row0 + c.tb.delta[j], m, c.tb.delta[j] & 3, v[k]);
         }
-        else
-        {
 #pragma unroll
-            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & c.tb.bmask[j]) ? -0.0f : v[r]);
+        for(int k = 0; k < kV4Group; ++k)
+        {
+            const int j = g + k;
+            if(j >= 27 || !selected<kSel>(j, c.tb.dp)) continue;
+            if(b.fast)
+            {
+#pragma unroll
+                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + v[k][r];
+            }
+            else
+            {
+#pragma unroll
+                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & c.tb.bmask[j]) ? -0.0f : v[k][r]);
+            }
         }
     }
 }
