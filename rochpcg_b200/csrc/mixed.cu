@@ -390,27 +390,28 @@ __device__ __forceinline__ void load4(const float* x, int base, int m, int s, fl
     else { v[0] = a.w; v[1] = b.x; v[2] = b.y; v[3] = b.z; }
 }
 
-#ifndef HB_V4_GROUP
-#define HB_V4_GROUP 3
-#endif
-constexpr int kV4Group = HB_V4_GROUP;  // slots whose loads are issued together before their in-order adds
+// Slots whose loads are issued together before their in-order adds: 3 on
+// large levels (keeps registers low, occupancy high), all 27 on small levels
+// (few threads: one round trip instead of nine).
+constexpr int kV4GroupLarge = 3, kV4GroupSmall = 27;
+constexpr int kV4SmallRows = 1 << 17;  // rows per colour below which a level counts as small
 
-template <int kSel>
+template <int kSel, int kGroup>
 __device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b, const float* x, int m,
                                            float (&sum)[4])
 {
 #pragma unroll
-    for(int g = 0; g < 27; g += kV4Group)
+    for(int g = 0; g < 27; g += kGroup)
     {
-        float v[kV4Group][4];
+        float v[kGroup][4];
 #pragma unroll
-        for(int k = 0; k < kV4Group; ++k)
+        for(int k = 0; k < kGroup; ++k)
         {
             const int j = g + k;
             if(j < 27 && selected<kSel>(j, c.tb.dp)) load4(x, b.row0 + c.tb.delta[j], m, c.tb.delta[j] & 3, v[k]);
         }
 #pragma unroll
-        for(int k = 0; k < kV4Group; ++k)
+        for(int k = 0; k < kGroup; ++k)
         {
             const int j = g + k;
             if(j >= 27 || !selected<kSel>(j, c.tb.dp)) continue;
@@ -428,7 +429,7 @@ __device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b,
     }
 }
 
-template <bool kFromDouble>
+template <bool kFromDouble, int kG>
 __global__ void __launch_bounds__(kV4X * kV4Y) k32v_fwd0(const ColorLaunch c, const StencilLevel L,
                                                          const float* __restrict__ inv_diag32,
                                                          const double* __restrict__ r64, float* __restrict__ r32,
@@ -449,11 +450,12 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_fwd0(const ColorLaunch c, co
         const float4 a = *reinterpret_cast<const float4*>(r32 + b.row0);
         sum[0] = a.x; sum[1] = a.y; sum[2] = a.z; sum[3] = a.w;
     }
-    if(c.tb.dp > 0) add_slots4<kBefore>(c, b, x, L.m, sum);
+    if(c.tb.dp > 0) add_slots4<kBefore, kG>(c, b, x, L.m, sum);
     const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
     *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
 }
 
+template <int kG>
 __global__ void __launch_bounds__(kV4X * kV4Y) k32v_bwd0(const ColorLaunch c, const StencilLevel L,
                                                          const float* __restrict__ diag32,
                                                          const float* __restrict__ inv_diag32, float* x)
@@ -463,11 +465,12 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_bwd0(const ColorLaunch c, co
     const float4 xv = *reinterpret_cast<const float4*>(x + b.row0);
     const float4 dv = *reinterpret_cast<const float4*>(diag32 + b.row0);
     float sum[4] = {__fmul_rn(xv.x, dv.x), __fmul_rn(xv.y, dv.y), __fmul_rn(xv.z, dv.z), __fmul_rn(xv.w, dv.w)};
-    add_slots4<kAfter>(c, b, x, L.m, sum);
+    add_slots4<kAfter, kG>(c, b, x, L.m, sum);
     const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
     *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
 }
 
+template <int kG>
 __global__ void __launch_bounds__(kV4X * kV4Y) k32v_sweep(const ColorLaunch c, const StencilLevel L,
                                                           const float* __restrict__ inv_diag32,
                                                           const float* __restrict__ r, float* x,
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_sweep(const ColorLaunch c, c
     if(!b.in) return;
     const float4 rv = *reinterpret_cast<const float4*>(r + b.row0);
     float sum[4] = {rv.x, rv.y, rv.z, rv.w};
-    add_slots4<kOff>(c, b, x, L.m, sum);
+    add_slots4<kOff, kG>(c, b, x, L.m, sum);
     const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
     const float4 xn = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
     *reinterpret_cast<float4*>(x + b.row0) = xn;
@@ -486,6 +489,55 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_sweep(const ColorLaunch c, c
         *reinterpret_cast<double2*>(z64 + b.row0) = make_double2((double)xn.x, (double)xn.y);
         *reinterpret_cast<double2*>(z64 + b.row0 + 2) = make_double2((double)xn.z, (double)xn.w);
     }
+}
+
+// Restriction on the 4-row layout: the injected fine points are the parity-0
+// colour's brick, whose brick-local index is the coarse natural index, so
+// rc[inj_c[row - off]] = (rf - A xf)[row] with the same per-row arithmetic as
+// k32_restrict (slot order, fmaf(-a_ii, x_i, .) at the diagonal slot).
+template <int kG>
+__global__ void __launch_bounds__(kV4X * kV4Y) k32v_restrict(const ColorLaunch c, const StencilLevel L,
+                                                             const int* __restrict__ inj_c,
+                                                             const float* __restrict__ diag32,
+                                                             const float* __restrict__ rf, const float* __restrict__ xf,
+                                                             float* __restrict__ rc)
+{
+    const Rows4 b = rows4(c, blockIdx.z);
+    if(!b.in) return;
+    const float4 rv = *reinterpret_cast<const float4*>(rf + b.row0);
+    float sum[4] = {rv.x, rv.y, rv.z, rv.w};
+    // slots before the diagonal, fmaf(-a_ii, x_i, .) at it, slots after it
+    add_slots4<kBefore, kG>(c, b, xf, L.m, sum);
+    const float4 xv = *reinterpret_cast<const float4*>(xf + b.row0);
+    const float4 dv = *reinterpret_cast<const float4*>(diag32 + b.row0);
+    sum[0] = fmaf(-dv.x, xv.x, sum[0]);
+    sum[1] = fmaf(-dv.y, xv.y, sum[1]);
+    sum[2] = fmaf(-dv.z, xv.z, sum[2]);
+    sum[3] = fmaf(-dv.w, xv.w, sum[3]);
+    add_slots4<kAfter, kG>(c, b, xf, L.m, sum);
+    const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
+    rc[ic.x] = sum[0];
+    rc[ic.y] = sum[1];
+    rc[ic.z] = sum[2];
+    rc[ic.w] = sum[3];
+}
+
+// xf[row] += xc[inj_c[row - off]] over the parity-0 colour's brick.
+__global__ void __launch_bounds__(kV4X * kV4Y) k32v_prolong(const ColorLaunch c, const int* __restrict__ inj_c,
+                                                            const float* __restrict__ xc, float* __restrict__ xf)
+{
+    const int kx0 = (blockIdx.x * kV4X + threadIdx.x) * 4;
+    const int ky = blockIdx.y * kV4Y + threadIdx.y;
+    const int kz = blockIdx.z;
+    if(!(kx0 < c.bx && ky < c.by && kz < c.bz)) return;
+    const int row0 = c.off + (kz * c.by + ky) * c.bx + kx0;
+    const int4 ic = *reinterpret_cast<const int4*>(inj_c + (row0 - c.off));
+    float4 x = *reinterpret_cast<const float4*>(xf + row0);
+    x.x += xc[ic.x];
+    x.y += xc[ic.y];
+    x.z += xc[ic.z];
+    x.w += xc[ic.w];
+    *reinterpret_cast<float4*>(xf + row0) = x;
 }
 
 // ----------------------------------------------------- FP64 stencil SpMV
@@ -1138,15 +1190,21 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     const int n = L.ncolors;
     const dim3 t(32, 8), t4(kV4X, kV4Y);
     const bool vec = vec4_ok(L);
+    const bool small = L.m / 8 < kV4SmallRows;
     for(int v = 0; v < n; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const dim3 g = brick_grid(c);
-        if(vec)
+        if(vec && small)
         {
-            if(r64) k32v_fwd0<true><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
-            else k32v_fwd0<false><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+            if(r64) k32v_fwd0<true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else k32v_fwd0<false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+        }
+        else if(vec)
+        {
+            if(r64) k32v_fwd0<true, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else k32v_fwd0<false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
         }
         else if(L.even)
         {
@@ -1164,7 +1222,8 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(vec) k32v_bwd0<<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        if(vec && small) k32v_bwd0<kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        else if(vec) k32v_bwd0<kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
         else if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         HB_LAUNCHED();
@@ -1177,10 +1236,14 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
 {
     const int n = L.ncolors;
     const bool vec = vec4_ok(L);
+    const bool small = L.m / 8 < kV4SmallRows;
     auto sweep = [&](int v, double* z) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(vec) k32v_sweep<<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+        if(vec && small)
+            k32v_sweep<kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+        else if(vec)
+            k32v_sweep<kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
         else if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         else k32_sweep<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         HB_LAUNCHED();
@@ -1196,15 +1259,25 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
                       const float* rf, const float* xf, float* rc, cudaStream_t s)
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
-    if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
+    const bool vec = vec4_ok(Lf) && nc == c.bx * c.by * c.bz;
+    if(vec && Lf.m / 8 < kV4SmallRows)
+        k32v_restrict<kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+    else if(vec)
+        k32v_restrict<kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+    else if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     else k32_restrict<false><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     HB_LAUNCHED();
     return 0;
 }
 
-int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf, cudaStream_t s)
+int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf,
+                     cudaStream_t s)
 {
-    k32_prolong<<<nblk(nc), kBS32, 0, s>>>(nc, inj_f, inj_c, xc, xf);
+    const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
+    if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
+        k32v_prolong<<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
+    else
+        k32_prolong<<<nblk(nc), kBS32, 0, s>>>(nc, inj_f, inj_c, xc, xf);
     HB_LAUNCHED();
     return 0;
 }

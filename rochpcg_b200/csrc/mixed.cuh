@@ -71,8 +71,9 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
 // rc[inj_c[i]] = rf[inj_f[i]] - (A xf)[inj_f[i]].
 int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* diag32,
                       const float* rf, const float* xf, float* rc, cudaStream_t s);
-// xf[inj_f[i]] += xc[inj_c[i]].
-int launch32_prolong(int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf, cudaStream_t s);
+// xf[inj_f[i]] += xc[inj_c[i]] (Lf: the fine level).
+int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf,
+                     cudaStream_t s);
 
 // FP64 y = A x on the implicit stencil (bitwise equal to the ELL SpMV: same
 // slot order, fma(-1, x, s) == s - x, fma(a_ii, x_i, s) on the diagonal).

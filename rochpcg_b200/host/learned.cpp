@@ -245,7 +245,7 @@ static int mg_fp32_learned(const SparseMatrix& A, int level, Smoother& S, int fi
     const int nc = A.Ac->localNumberOfRows;
     HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
     HB_RETURN_IF(mg_fp32_learned(*A.Ac, level + 1, S, first, coarse_steps, mo->rc32, mo->xc32, s));
-    HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
+    HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
     if(learned) return smoother_level_apply(S, *o, r, x, true, s);
     return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
 }
@@ -280,7 +280,7 @@ int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
         const int nc = A.Ac->localNumberOfRows;
         HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
         HB_RETURN_IF(mg_fp32_learned(*A.Ac, 1, S, first, o->smoother_coarse_steps, mo->rc32, mo->xc32, s));
-        HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
+        HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
         return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
     }
     catch(const Error& e)

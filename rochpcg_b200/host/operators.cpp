@@ -131,7 +131,7 @@ int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s)
     const int nc = A.Ac->localNumberOfRows;
     HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
     HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
-    HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
+    HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
     return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
 }
 
@@ -155,7 +155,7 @@ int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x)
         const int nc = A.Ac->localNumberOfRows;
         HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
         HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
-        HB_RETURN_IF(hb::launch32_prolong(nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
+        HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
         return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
     });
 }
