@@ -19,8 +19,11 @@ def gold(name):
     return np.load(os.path.join(GOLD, name))
 
 
-@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32), (24, 40, 56), (56, 56, 40)])
 def test_cg_history_matches_oracle(dims):
+    """(24, 40, 56) and (56, 56, 40) have odd coarse levels (3x5x7, 7x7x5):
+    colour sizes and offsets by value (the reference fills them in JPL round
+    order, which disagrees with its colour-sorted permutation there)."""
     P, O = problems(*dims)
     r = P.cg(50, 0.0)
     o = O.cg(50, 0.0)

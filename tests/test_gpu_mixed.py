@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 FLT_OVER_DBL = np.finfo(np.float32).eps / np.finfo(np.float64).eps
 
 
-@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 32), (64, 64, 64), (24, 40, 56), (56, 56, 40)])
 def test_mixed_vcycle_bitwise(dims):
     import rochpcg_b200 as R
 
