@@ -378,6 +378,93 @@ int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter
  * (the V-cycle with the attached learned smoother). */
 int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
 
+/* ---------------------------------------------- reference routines (natural order)
+ * The benchmark's `_ref` kernels on the generated row-major arrays (natural
+ * row order, 27 slots per row, nonzero counts as signed char, the diagonal's
+ * slot per row), device pointers, nx*ny*nz rows.  Results equal those of the
+ * sequential C loops bit for bit (products and sums rounded separately). */
+/* src/ComputeSPMV_ref.cpp:48-75: y = A x. */
+int hpcgb200_ref_spmv(int nx, int ny, int nz, const int* mtx_ind, const double* values,
+                      const signed char* nnz_in_row, const double* x, double* y, void* stream);
+/* src/ComputeSYMGS_ref.cpp:51-104: one forward and one backward natural-order
+ * Gauss-Seidel sweep on x (in place), run as 2 * (nx + 2 ny + 4 nz - 6)
+ * wavefront launches. */
+int hpcgb200_ref_symgs(int nx, int ny, int nz, const int* mtx_ind, const double* values,
+                       const signed char* nnz_in_row, const int* diag_slot, const double* r, double* x,
+                       void* stream);
+/* src/CG_ref.cpp:60-160 on a problem created with
+ * HPCGB200_FLAG_KEEP_GENERATED: the reference CG in natural order from x = 0
+ * on the problem's b (un-permuted), with ComputeMG_ref as preconditioner when
+ * precond != 0.  Overwrites the problem's x with the natural-order result
+ * (hpcgb200_problem_get_x does not apply to it). */
+int hpcgb200_problem_cg_ref(hpcgb200_problem* p, int max_iter, double tol, int precond, int* niters,
+                            double* normr, double* normr0, double* seconds);
+
+/* src/ComputeMG_ref.cpp on a problem created with HPCGB200_FLAG_KEEP_GENERATED:
+ * z = M^-1 r for natural-order device vectors r, z of level 0 (the V-cycle
+ * of the reference CG: natural-order SymGS, injection, 1 pre / 1 post step). */
+int hpcgb200_problem_mg_ref(hpcgb200_problem* p, const double* r_natural, double* z_natural);
+
+/* --------------------------------------------------- benchmark protocol
+ * src/main.cpp:174-563 with src/ReportResults.cpp: set-up, CheckProblem,
+ * reference SpMV+MG timing, the 50-iteration reference CG residual,
+ * OptimizeProblem, TestCG, TestSymmetry, the optimized CG set-up run, timed
+ * CG sets for running_time seconds, TestNorms and the report (a JSON
+ * document with the sections and field names of the reference's YAML).  One
+ * rank; the reference phases run on the device in natural order. */
+#define HPCGB200_BENCH_MAX_LEVELS 8
+typedef struct hpcgb200_benchmark_params
+{
+    int nx, ny, nz;       /* local = global grid; a dimension < 16 is raised as src/init.cpp:150-159 does */
+    int running_time;     /* seconds of timed CG sets (--rt=); 0 selects the QuickPath */
+    int verify;           /* 1: reference phases and validation; 0: ref tolerance = tol (--tol=) */
+    double tol;
+    int mode;             /* HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED */
+} hpcgb200_benchmark_params;
+
+typedef struct hpcgb200_benchmark_result
+{
+    /* filled by hpcgb200_benchmark_run: the inputs of the report */
+    int nx, ny, nz, mode, verify, quick_path;
+    int levels;
+    long long rows[HPCGB200_BENCH_MAX_LEVELS];
+    long long nonzeros[HPCGB200_BENCH_MAX_LEVELS];
+    int presmoother_steps, postsmoother_steps;
+    double times[10];              /* the driver's times[]: 0 timed CG sets, 1 DDOT, 2 WAXPBY, 3 SpMV,
+                                      5 MG, 7 optimization, 8 reference SpMV+MG per call, 9 setup */
+    double optimize_problem_bytes; /* device bytes OptimizeProblem allocates */
+    long long check_problem_errors;
+    int ref_max_iters, ref_niters;
+    double ref_tolerance;          /* normr/normr0 after the reference CG (or params.tol) */
+    int opt_max_iters;             /* iterations per timed set */
+    int opt_setup_niters;          /* iterations the set-up run needed to reach ref_tolerance */
+    int tolerance_failures, err_count, global_failure;
+    double opt_worst_time;
+    int cg_sets;
+    int testcg_count_pass, testcg_count_fail;
+    int testcg_expected_niters_no_prec, testcg_expected_niters_prec;
+    int testcg_niters_max_no_prec, testcg_niters_max_prec;
+    double depsym_spmv, depsym_mg;
+    int symmetry_count_fail;
+    double norms_mean, norms_variance;
+    int norms_pass;
+    /* filled by hpcgb200_benchmark_report */
+    double fnops, frefnops;
+    double gflops_raw, gflops_convergence, gflops_final, gflops_hpcg24;
+    double gbs_raw, gbs_final;
+    double memory_total_gb;
+    int valid;
+} hpcgb200_benchmark_result;
+
+/* Runs the whole protocol on the current device and fills *result (then
+ * calls hpcgb200_benchmark_report without a buffer). */
+int hpcgb200_benchmark_run(const hpcgb200_benchmark_params* params, hpcgb200_benchmark_result* result);
+/* Host only (no device needed): the derived figures of src/ReportResults.cpp
+ * :134-195,396-460 from the inputs in *result, and the report as JSON into
+ * json[capacity] (NUL-terminated; *length = bytes without the NUL, also when
+ * json is NULL or too small, which returns HPCGB200_ERR_WORKSPACE). */
+int hpcgb200_benchmark_report(hpcgb200_benchmark_result* result, char* json, size_t capacity, size_t* length);
+
 #ifdef __cplusplus
 }
 #endif

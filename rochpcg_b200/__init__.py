@@ -162,6 +162,21 @@ class Problem:
                                                          ctypes.byref(sec)))
         return dict(niters=it.value, normr=nr.value, normr0=nr0.value, seconds=sec.value)
 
+    def cg_ref(self, max_iter: int, tol: float, precond: bool = True) -> dict:
+        """The benchmark's reference CG (src/CG_ref.cpp) in natural order on the
+        device; needs a problem created with keep_generated=True.  Leaves x in
+        natural order."""
+        it = ctypes.c_int()
+        nr, nr0, sec = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(self.L, self.L.hpcgb200_problem_cg_ref(self.h, max_iter, tol, int(precond), ctypes.byref(it),
+                                                     ctypes.byref(nr), ctypes.byref(nr0), ctypes.byref(sec)))
+        return dict(niters=it.value, normr=nr.value, normr0=nr0.value, seconds=sec.value)
+
+    def mg_ref(self, r_ptr: int, z_ptr: int) -> None:
+        """z = M^-1 r with the reference V-cycle (src/ComputeMG_ref.cpp), natural
+        order, device pointers; needs keep_generated=True."""
+        check(self.L, self.L.hpcgb200_problem_mg_ref(self.h, ctypes.c_void_p(r_ptr), ctypes.c_void_p(z_ptr)))
+
     def true_residual(self) -> float:
         """||b - A x|| / ||b|| of the current solution, computed in FP64."""
         rel = ctypes.c_double()

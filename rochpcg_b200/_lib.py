@@ -77,6 +77,12 @@ SIGNATURES = {
     "hpcgb200_problem_cg": (_i, [_vp, _i, _i, _d, _i, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_problem_solve_host": (_i, [_vp, _i, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp]),
     "hpcgb200_problem_true_residual": (_i, [_vp, _vp]),
+    "hpcgb200_problem_cg_ref": (_i, [_vp, _i, _d, _i, _vp, _vp, _vp, _vp]),
+    "hpcgb200_problem_mg_ref": (_i, [_vp, _vp, _vp]),
+    "hpcgb200_ref_spmv": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hpcgb200_ref_symgs": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hpcgb200_benchmark_run": (_i, [_vp, _vp]),
+    "hpcgb200_benchmark_report": (_i, [_vp, _vp, _sz, _vp]),
     "hpcgb200_problem_kernels_per_iteration": (_i, [_vp, _i, _i, _vp]),
     "hpcgb200_problem_test_cg": (_i, [_vp, _i, _vp, _vp, _vp]),
     "hpcgb200_problem_test_symmetry": (_i, [_vp, _i, _vp, _vp, _vp]),

@@ -225,6 +225,25 @@ int TestSymmetry_B200(SparseMatrix& A, Vector& b, Vector& xexact, TestSymmetryDa
                       MGPrecision prec);
 int TestNorms(TestNormsData& testnorms_data);
 
+// -------------------------------------------------- reference routines
+// The benchmark's `_ref` routines (src/*_ref.cpp, src/CheckProblem.cpp) on
+// the device: natural row order on the generated row-major arrays, so they
+// apply between GenerateCoarseProblem and OptimizeProblem (or later on a
+// hierarchy that keeps its generated arrays).  SpMV and SymGS results equal
+// the sequential C loops bit for bit.
+int ComputeSPMV_ref(const SparseMatrix& A, Vector& x, Vector& y);
+int ComputeSYMGS_ref(const SparseMatrix& A, const Vector& r, Vector& x);
+int ComputeMG_ref(const SparseMatrix& A, const Vector& r, Vector& x);
+int ComputeRestriction_ref(const SparseMatrix& A, const Vector& rf);
+int ComputeProlongation_ref(const SparseMatrix& Af, Vector& xf);
+int ComputeDotProduct_ref(local_int_t n, const Vector& x, const Vector& y, double& result, double& time_allreduce);
+int ComputeWAXPBY_ref(local_int_t n, double alpha, const Vector& x, double beta, const Vector& y, Vector& w);
+int CG_ref(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const int max_iter, const double tolerance,
+           int& niters, double& normr, double& normr0, double* times, bool doPreconditioning, bool verbose);
+// CheckProblem as a count: rows whose entries, b, x or xexact differ from the
+// generated stencil problem, plus one if the nonzero total disagrees.
+long long CheckProblem_B200(const SparseMatrix& A, const Vector* b, const Vector* x, const Vector* xexact);
+
 // HPCG flop / memory-traffic model per CG iteration (src/ReportResults.cpp:
 // 134-195 with numberOfCgSets = 1, optMaxIters = 1, preamble excluded).
 struct HpcgModel

@@ -19,6 +19,7 @@ extern bool g_keep_generated;
 }
 
 
+
 namespace {
 
 MGPrecision prec_of(int mode)
@@ -341,6 +342,55 @@ extern "C" int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const 
         HB_HOST_CUDA(cudaStreamSynchronize(s));
         if(seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return 0;
+    });
+}
+
+// src/CG_ref.cpp on the problem's generated arrays (kept with
+// HPCGB200_FLAG_KEEP_GENERATED): b is brought back to natural order, x is
+// left in natural order.
+extern "C" int hpcgb200_problem_cg_ref(hpcgb200_problem* p, int max_iter, double tol, int precond, int* niters,
+                                       double* normr, double* normr0, double* seconds)
+{
+    if(!p || !niters || !normr || !normr0) return hb::record_error(HPCGB200_ERR_ARG, "null argument");
+    if(max_iter < 0 || max_iter > 1000000) return hb::record_error(HPCGB200_ERR_ARG, "max_iter out of range");
+    return guarded([&] {
+        const int m = p->A.localNumberOfRows;
+        Vector bn;
+        CudaInitializeVector(bn, m);
+        int rc = 0;
+        try
+        {
+            check(hpcgb200_unpermute_vector(m, p->A.perm, p->b.d_values, bn.d_values, rt().stream));
+            CudaZeroVector(p->x);
+            double times[10] = {0};
+            rc = CG_ref(p->A, p->data, bn, p->x, max_iter, tol, *niters, *normr, *normr0, times, precond != 0, false);
+            if(seconds) *seconds = times[0];
+        }
+        catch(...)
+        {
+            CudaDeleteVector(bn);
+            throw;
+        }
+        CudaDeleteVector(bn);
+        return rc;
+    });
+}
+
+// src/ComputeMG_ref.cpp on the problem's generated arrays: z = M^-1 r with
+// r and z natural-order device vectors of level 0.
+extern "C" int hpcgb200_problem_mg_ref(hpcgb200_problem* p, const double* r_natural, double* z_natural)
+{
+    if(!p || !r_natural || !z_natural || r_natural == z_natural)
+        return hb::record_error(HPCGB200_ERR_ARG, "need distinct device vectors r and z");
+    return guarded([&] {
+        const int m = p->A.localNumberOfRows;
+        Vector r, z;
+        r.localLength = z.localLength = m;
+        r.d_values = const_cast<double*>(r_natural);
+        z.d_values = z_natural;
+        const int rc = ComputeMG_ref(p->A, r, z);
+        HB_HOST_CUDA(cudaStreamSynchronize(rt().stream));
+        return rc;
     });
 }
 

@@ -1,0 +1,156 @@
+"""The benchmark protocol on the GPU: the reference routines in natural order
+(SpMV, SymGS, V-cycle) bit for bit against the reference's own CPU code
+(oracle/_ref) and its golden fixtures, the reference CG's 50-iteration
+residual, and whole protocol runs (QuickPath) against the reference's
+iteration bounds.
+
+Tolerances: the reference CG sums its dot products in an OpenMP order and
+ours in a fixed block order, so its residuals agree to a relative 1e-6 where
+they are well above rounding (64^3: 1.1e-11 after 50 iterations); at 32^3 the
+50-iteration residual is at the rounding floor (5.8e-21 to 1.0e-20 with the
+thread count) and only its magnitude is checked."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import rochpcg_b200 as R
+from rochpcg_b200 import benchmark as B
+from oracle.oracle import RefProblem
+from gpu_util import host, sync, to_dev
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def ref_spmv(P, level, x):
+    nx, ny, nz = P.dims[level]
+    xd = to_dev(x)
+    yd = torch.empty_like(xd)
+    torch.cuda.synchronize()
+    rc = P.L.hpcgb200_ref_spmv(nx, ny, nz, ctypes.c_void_p(P.device_ptr("mtx_ind", level)),
+                               ctypes.c_void_p(P.device_ptr("values", level)),
+                               ctypes.c_void_p(P.device_ptr("nnz_in_row", level)), ctypes.c_void_p(xd.data_ptr()),
+                               ctypes.c_void_p(yd.data_ptr()), ctypes.c_void_p(P.stream_handle))
+    assert rc == 0
+    sync(P)
+    return host(yd)
+
+
+def ref_symgs(P, level, r, x0):
+    nx, ny, nz = P.dims[level]
+    rd, xd = to_dev(r), to_dev(x0.copy())
+    torch.cuda.synchronize()
+    rc = P.L.hpcgb200_ref_symgs(nx, ny, nz, ctypes.c_void_p(P.device_ptr("mtx_ind", level)),
+                                ctypes.c_void_p(P.device_ptr("values", level)),
+                                ctypes.c_void_p(P.device_ptr("nnz_in_row", level)),
+                                ctypes.c_void_p(P.device_ptr("diag_slot", level)), ctypes.c_void_p(rd.data_ptr()),
+                                ctypes.c_void_p(xd.data_ptr()), ctypes.c_void_p(P.stream_handle))
+    assert rc == 0
+    sync(P)
+    return host(xd)
+
+
+def test_ref_kernels_equal_golden_fixtures():
+    g = golden("ref_16x16x16.npz")
+    P = R.Problem(16, 16, 16, keep_generated=True)
+    assert np.array_equal(ref_spmv(P, 0, g["spmv_x"]), g["spmv_y"])
+    assert np.array_equal(ref_symgs(P, 0, g["symgs_r"], np.zeros(P.rows[0])), g["symgs_x"])
+    P.close()
+
+
+@pytest.mark.parametrize("dims", [(16, 24, 32), (24, 40, 56)])
+def test_ref_kernels_equal_reference_on_every_level(dims):
+    P = R.Problem(*dims, keep_generated=True)
+    Q = RefProblem(*dims)
+    rng = np.random.default_rng(5)
+    for l in range(4):
+        m = P.rows[l]
+        x = rng.uniform(-1, 1, m)
+        r = rng.uniform(-1, 1, m)
+        assert np.array_equal(ref_spmv(P, l, x), Q.spmv(l, x)), l
+        assert np.array_equal(ref_symgs(P, l, r, x), Q.symgs(l, r, x)), l
+    P.close()
+
+
+@pytest.mark.parametrize("dims", [(32, 32, 32), (24, 40, 56)])
+def test_ref_vcycle_equals_reference(dims):
+    P = R.Problem(*dims, keep_generated=True)
+    Q = RefProblem(*dims)
+    r = np.random.default_rng(6).uniform(-1, 1, P.rows[0])
+    rd = to_dev(r)
+    zd = torch.empty_like(rd)
+    torch.cuda.synchronize()
+    P.mg_ref(rd.data_ptr(), zd.data_ptr())
+    sync(P)
+    assert np.array_equal(host(zd), Q.mg(r))
+    P.close()
+
+
+def test_ref_cg_residual_matches_reference():
+    g = golden("ref_64x64x64.npz")
+    P = R.Problem(64, 64, 64, keep_generated=True)
+    out = P.cg_ref(50, 0.0)
+    assert out["niters"] == 50
+    assert out["normr0"] == pytest.approx(float(g["cg50_normr0"]), rel=1e-13)
+    assert out["normr"] / out["normr0"] == pytest.approx(float(g["cg50_normr"]) / float(g["cg50_normr0"]), rel=1e-6)
+    # to 1e-9: the reference's own iteration count
+    out = P.cg_ref(500, 1e-9)
+    assert out["niters"] == int(g["cg1e9_niters"])
+    P.close()
+    g32 = golden("ref_32x32x32.npz")
+    P = R.Problem(32, 32, 32, keep_generated=True)
+    out = P.cg_ref(50, 0.0)
+    assert out["normr0"] == pytest.approx(float(g32["cg50_normr0"]), rel=1e-13)
+    assert out["normr"] / out["normr0"] < 1e-19
+    P.close()
+
+
+@pytest.mark.parametrize("n,bound", [(32, 53), (64, 50)])
+def test_protocol_quickpath_valid(n, bound):
+    """QuickPath run of the whole protocol; the optimized CG must reach the
+    reference residual within the reference's check_niter bound
+    (test_rochpcg.cpp:88-119)."""
+    res, rep = B.run(n, n, n, running_time=0, verify=True)
+    assert res["check_problem_errors"] == 0
+    assert res["ref_niters"] == 50
+    assert res["tolerance_failures"] == 0 and res["err_count"] == 0
+    assert res["opt_setup_niters"] <= bound
+    assert res["opt_max_iters"] == max(50, res["opt_setup_niters"])
+    assert res["cg_sets"] == 1 and res["quick_path"] == 1
+    assert res["testcg_count_fail"] == 0 and res["symmetry_count_fail"] == 0 and res["norms_pass"] == 1
+    assert res["valid"] == 1
+    assert rep["Final Summary"]["HPCG result is VALID with a GFLOP/s rating of"] == pytest.approx(res["gflops_final"])
+    assert rep["Linear System Information"]["Number of Equations"] == n ** 3
+    assert res["times"][0] > 0 and res["times"][7] > 0 and res["times"][8] > 0 and res["times"][9] > 0
+    if n == 64:
+        g = golden("ref_64x64x64.npz")
+        assert res["ref_tolerance"] == pytest.approx(float(g["cg50_normr"]) / float(g["cg50_normr0"]), rel=1e-6)
+
+
+def test_protocol_with_given_tolerance_and_timed_sets():
+    res, rep = B.run(32, 32, 32, running_time=1, verify=False, tol=1e-6)
+    assert res["ref_tolerance"] == 1e-6 and res["ref_niters"] == 0
+    assert res["opt_max_iters"] == 50           # reaching 1e-6 takes fewer than 50 iterations
+    assert res["cg_sets"] >= 2 and res["times"][0] >= 1.0
+    assert res["norms_pass"] == 1 and res["valid"] == 1
+    assert rep["Reproducibility Information"]["Scaled residual variance"] < 1e-6
+
+
+def test_protocol_small_dimensions_raised():
+    res, _ = B.run(8, 24, 4, running_time=0, verify=False, tol=1e-3)
+    assert (res["nx"], res["ny"], res["nz"]) == (24, 24, 24)
+
+
+def test_protocol_mixed_mode():
+    res, rep = B.run(32, 32, 32, running_time=0, verify=True, mode=R.MODE_MIXED)
+    assert res["tolerance_failures"] == 0 and res["opt_setup_niters"] <= 53
+    assert res["valid"] == 1
+    assert "Mixed precision" in rep["Final Summary"]
