@@ -404,7 +404,8 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
     Q.set_rhs(normal_rhs(Q.rows[0], 0))
     f3, _ = Q.model()
     res = {}
-    for name, mode in (("fp64", R.MODE_FP64), ("mixed", R.MODE_MIXED)):
+    hists = {}
+    for name, mode in (("fp64", R.MODE_FP64), ("fp64_stencil", R.MODE_FP64_STENCIL), ("mixed", R.MODE_MIXED)):
         for _ in range(warmup):
             Q.cg(args.max_iter, args.tol, mode=mode)
         barrier()
@@ -412,12 +413,17 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
         for _ in range(steps):
             r3 = Q.cg(args.max_iter, args.tol, mode=mode)
             ts.append(r3["seconds"])
+        hists[name] = r3["hist"]
         res[name] = {"time_to_1e-9_s": min(ts), "iterations": r3["niters"],
                      "rel_residual_recurrence": r3["normr"] / r3["normr0"],
                      "rel_residual_fp64_true": Q.true_residual(),
                      "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9,
                      "kernels_per_iteration": Q.kernels_per_iteration(mode)}
     res["speedup_mixed_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["mixed"]["time_to_1e-9_s"]
+    # FP64 on the implicit stencil: the FP64 residual history bit for bit, no matrix reads
+    res["speedup_fp64_stencil_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["fp64_stencil"]["time_to_1e-9_s"]
+    res["fp64_stencil_history_bitwise_equal"] = bool(len(hists["fp64"]) == len(hists["fp64_stencil"]) and
+                                                     (hists["fp64"] == hists["fp64_stencil"]).all())
     # level-0 kernels of the mixed path, timed alone (CUDA events)
     m3 = Q.rows[0]
     rows_c = m3 // 8
@@ -428,7 +434,8 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
     res["kernels"] = {"k32_sweep_ms": sw, "k32_sweep_GBps": sw_bytes / (sw * 1e-3) / 1e9,
                       "k32_sweep_algorithmic_bytes": sw_bytes,
                       "k64_spmv_stencil_ms": sp, "k64_spmv_stencil_GBps": sp_bytes / (sp * 1e-3) / 1e9,
-                      "mg_mixed_ms": Q.time_op("mg_mixed", 5), "mg_fp64_ms": Q.time_op("mg", 3)}
+                      "mg_mixed_ms": Q.time_op("mg_mixed", 5), "mg_fp64_ms": Q.time_op("mg", 3),
+                      "mg_fp64_stencil_ms": Q.time_op("mg_stencil", 5)}
     res["grid"] = [n3, n3, n3]
     res["rhs"] = "N(0,1) i.i.d., seed 0 (SplitMix64 + Box-Muller, natural row order)"
     Q.close()

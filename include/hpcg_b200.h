@@ -212,6 +212,9 @@ typedef struct hpcgb200_problem hpcgb200_problem;
 #define HPCGB200_MODE_LEARNED 2 /* as MIXED, with the attached learned smoother on the coarse levels
                                    (flexible CG; falls back to MIXED once an iteration does not
                                    reduce the FP64 residual) */
+#define HPCGB200_MODE_FP64_STENCIL 3 /* FP64 as HPCGB200_MODE_FP64, V-cycle and SpMV on the implicit stencil:
+                                        the same residual history bit for bit, no matrix reads (needs the
+                                        27-point stencil in parity colouring, like MIXED) */
 
 int hpcgb200_problem_create(int nx, int ny, int nz, int nlevels, hpcgb200_problem** out);
 /* flags: HPCGB200_FLAG_KEEP_GENERATED keeps the row-major generated arrays
@@ -375,7 +378,8 @@ int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter
  * (one full-row color sweep, averaged over the 15 of a SymGS step),
  * "symgs","symgs_zero","mg","mg_mixed", "symgs32_sweep" (one FP32 implicit
  * colour sweep, averaged over a SymGS step), "spmv_stencil", "mg_learned"
- * (the V-cycle with the attached learned smoother). */
+ * (the V-cycle with the attached learned smoother), "mg_stencil" (the FP64
+ * V-cycle on the implicit stencil). */
 int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
 
 /* ---------------------------------------------- reference routines (natural order)
@@ -419,7 +423,7 @@ typedef struct hpcgb200_benchmark_params
     int running_time;     /* seconds of timed CG sets (--rt=); 0 selects the QuickPath */
     int verify;           /* 1: reference phases and validation; 0: ref tolerance = tol (--tol=) */
     double tol;
-    int mode;             /* HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED */
+    int mode;             /* HPCGB200_MODE_FP64, HPCGB200_MODE_MIXED or HPCGB200_MODE_FP64_STENCIL */
 } hpcgb200_benchmark_params;
 
 typedef struct hpcgb200_benchmark_result

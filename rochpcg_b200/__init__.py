@@ -23,6 +23,7 @@ from ._lib import LIB_PATH, load, HpcgError, check  # noqa: F401
 MODE_FP64 = 0
 MODE_MIXED = 1
 MODE_LEARNED = 2
+MODE_FP64_STENCIL = 3  # FP64 results of MODE_FP64 bit for bit, V-cycle and SpMV on the implicit stencil
 FLAG_KEEP_GENERATED = 1
 
 _FIELD_DTYPES = {

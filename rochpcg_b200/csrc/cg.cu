@@ -126,6 +126,38 @@ __global__ void __launch_bounds__(kBS) k_cg_spmv_pap(int m, ColorChunks cc, cons
     }
 }
 
+// The reduction half of k_cg_spmv_pap on a stored Ap: same chunk -> row map,
+// same per-block tree, same last-block sum.
+__global__ void __launch_bounds__(kBS) k_cg_pap_chunks(ColorChunks cc, const double* __restrict__ p,
+                                                       const double* __restrict__ Ap, CGState* st, double* partial,
+                                                       unsigned int* ticket)
+{
+    __shared__ double red[32];
+    __shared__ bool last;
+    double s = 0.0;
+    int row;
+    if(cc.row_of(blockIdx.x, threadIdx.x, row)) s = Ap[row] * p[row];
+    s = block_sum(s, red);
+    if(threadIdx.x == 0)
+    {
+        partial[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(unsigned i = threadIdx.x; i < gridDim.x; i += kBS) acc += __ldcg(&partial[i]);
+    acc = block_sum(acc, red);
+    if(threadIdx.x == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
 __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const double* __restrict__ p,
                                                                  const double* __restrict__ Ap,
                                                                  double* __restrict__ r, double* __restrict__ x,
@@ -225,6 +257,15 @@ int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const d
                        double* Ap, CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
     k_cg_spmv_pap<<<cc.nchunks(), kBS, 0, s>>>(m, cc, ell_col, ell_val, p, Ap, st, partial, ticket);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const double* Ap, CGState* st,
+                         double* partial, unsigned int* ticket, cudaStream_t s)
+{
+    (void)m;
+    k_cg_pap_chunks<<<cc.nchunks(), kBS, 0, s>>>(cc, p, Ap, st, partial, ticket);
     HB_LAUNCHED();
     return 0;
 }

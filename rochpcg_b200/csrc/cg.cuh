@@ -39,6 +39,11 @@ int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cud
 // sums, `ticket` must start at zero and is left at zero.
 int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
                        double* Ap, CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
+// pAp = p.Ap and alpha from a precomputed Ap, summed with exactly the block
+// partition and order of launch_cg_spmv_pap (same partials, same final sum),
+// so a solve whose SpMV runs elsewhere keeps the ELL solve's scalars bit for bit.
+int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const double* Ap, CGState* st,
+                         double* partial, unsigned int* ticket, cudaStream_t s);
 // r -= alpha Ap, normr = ||r||, x += alpha p, history; then (own 1-thread
 // kernel) k++ and the loop condition (k <= max_iter && normr/normr0 > tol)
 // written to `cond` (a graph conditional handle; 0 = none).  While the

@@ -369,41 +369,82 @@ __device__ __forceinline__ Rows4 rows4(const ColorLaunch& c, int kz)
     return b;
 }
 
-__device__ __forceinline__ float4 ld4(const float* x, int i, int m)
+// Four consecutive values of a brick line: one float4, or two double2 for
+// the FP64 V-cycle (32 bytes, 16-byte aligned halves).
+template <typename T>
+struct Quad;
+template <>
+struct Quad<float>
 {
-    return (i >= 0 && i + 4 <= m) ? *reinterpret_cast<const float4*>(x + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    static __device__ __forceinline__ void load(const float* p, float (&v)[4])
+    {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    static __device__ __forceinline__ void store(float* p, const float (&v)[4])
+    {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+template <>
+struct Quad<double>
+{
+    static __device__ __forceinline__ void load(const double* p, double (&v)[4])
+    {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        const double2 b = *reinterpret_cast<const double2*>(p + 2);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    static __device__ __forceinline__ void store(double* p, const double (&v)[4])
+    {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+    }
+};
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return fma(a, b, c); }
+
+template <typename T>
+__device__ __forceinline__ void ld4(const T* x, int i, int m, T (&v)[4])
+{
+    if(i >= 0 && i + 4 <= m) Quad<T>::load(x + i, v);
+    else v[0] = v[1] = v[2] = v[3] = T(0);
 }
 
 // x[base .. base+3]; s = base & 3 is the same for every thread of the launch.
-__device__ __forceinline__ void load4(const float* x, int base, int m, int s, float (&v)[4])
+template <typename T>
+__device__ __forceinline__ void load4(const T* x, int base, int m, int s, T (&v)[4])
 {
     if(s == 0)
     {
-        const float4 a = ld4(x, base, m);
-        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        ld4(x, base, m, v);
         return;
     }
     const int lo = base - s;
-    const float4 a = ld4(x, lo, m), b = ld4(x, lo + 4, m);
-    if(s == 1) { v[0] = a.y; v[1] = a.z; v[2] = a.w; v[3] = b.x; }
-    else if(s == 2) { v[0] = a.z; v[1] = a.w; v[2] = b.x; v[3] = b.y; }
-    else { v[0] = a.w; v[1] = b.x; v[2] = b.y; v[3] = b.z; }
+    T a[4], b[4];
+    ld4(x, lo, m, a);
+    ld4(x, lo + 4, m, b);
+    if(s == 1) { v[0] = a[1]; v[1] = a[2]; v[2] = a[3]; v[3] = b[0]; }
+    else if(s == 2) { v[0] = a[2]; v[1] = a[3]; v[2] = b[0]; v[3] = b[1]; }
+    else { v[0] = a[3]; v[1] = b[0]; v[2] = b[1]; v[3] = b[2]; }
 }
 
 // Slots whose loads are issued together before their in-order adds: 3 on
-// large levels (keeps registers low, occupancy high), all 27 on small levels
-// (few threads: one round trip instead of nine).
-constexpr int kV4GroupLarge = 3, kV4GroupSmall = 27;
+// large levels (keeps registers low, occupancy high), all 27 (FP32) or 9
+// (FP64) on small levels (few threads: fewer round trips).
+constexpr int kV4GroupLarge = 3, kV4GroupSmall = 27, kV4GroupSmall64 = 9;
 constexpr int kV4SmallRows = 1 << 17;  // rows per colour below which a level counts as small
 
-template <int kSel, int kGroup>
-__device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b, const float* x, int m,
-                                           float (&sum)[4])
+template <int kSel, int kGroup, typename T>
+__device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b, const T* x, int m, T (&sum)[4])
 {
 #pragma unroll
     for(int g = 0; g < 27; g += kGroup)
     {
-        float v[kGroup][4];
+        T v[kGroup][4];
 #pragma unroll
         for(int k = 0; k < kGroup; ++k)
         {
@@ -423,97 +464,108 @@ __device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b,
             else
             {
 #pragma unroll
-                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & c.tb.bmask[j]) ? -0.0f : v[k][r]);
+                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & c.tb.bmask[j]) ? T(-0.0) : v[k][r]);
             }
         }
     }
 }
 
-template <bool kFromDouble, int kG>
-__global__ void __launch_bounds__(kV4X * kV4Y) k32v_fwd0(const ColorLaunch c, const StencilLevel L,
-                                                         const float* __restrict__ inv_diag32,
-                                                         const double* __restrict__ r64, float* __restrict__ r32,
-                                                         float* x)
+// Zero-guess forward sweep of one colour.  FP32 with kFromDouble: r comes in
+// FP64 (the CG residual) and its float copy is stored for the later sweeps.
+template <typename T, bool kFromDouble, int kG>
+__global__ void __launch_bounds__(kV4X * kV4Y) kv_fwd0(const ColorLaunch c, const StencilLevel L,
+                                                       const T* __restrict__ inv_diag, const double* __restrict__ r64,
+                                                       T* __restrict__ r, T* x)
 {
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
-    float sum[4];
-    if(kFromDouble)
+    T sum[4];
+    if constexpr(kFromDouble)
     {
-        const double2 a = *reinterpret_cast<const double2*>(r64 + b.row0);
-        const double2 a2 = *reinterpret_cast<const double2*>(r64 + b.row0 + 2);
-        sum[0] = (float)a.x; sum[1] = (float)a.y; sum[2] = (float)a2.x; sum[3] = (float)a2.y;
-        *reinterpret_cast<float4*>(r32 + b.row0) = make_float4(sum[0], sum[1], sum[2], sum[3]);
+        double a[4];
+        Quad<double>::load(r64 + b.row0, a);
+#pragma unroll
+        for(int q = 0; q < 4; ++q) sum[q] = (T)a[q];
+        Quad<T>::store(r + b.row0, sum);
     }
     else
     {
-        const float4 a = *reinterpret_cast<const float4*>(r32 + b.row0);
-        sum[0] = a.x; sum[1] = a.y; sum[2] = a.z; sum[3] = a.w;
+        Quad<T>::load(r + b.row0, sum);
     }
     if(c.tb.dp > 0) add_slots4<kBefore, kG>(c, b, x, L.m, sum);
-    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
-    *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
+    T inv[4], out[4];
+    Quad<T>::load(inv_diag + b.row0, inv);
+#pragma unroll
+    for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
+    Quad<T>::store(x + b.row0, out);
 }
 
-template <int kG>
-__global__ void __launch_bounds__(kV4X * kV4Y) k32v_bwd0(const ColorLaunch c, const StencilLevel L,
-                                                         const float* __restrict__ diag32,
-                                                         const float* __restrict__ inv_diag32, float* x)
+template <typename T, int kG>
+__global__ void __launch_bounds__(kV4X * kV4Y) kv_bwd0(const ColorLaunch c, const StencilLevel L,
+                                                       const T* __restrict__ diag, const T* __restrict__ inv_diag, T* x)
 {
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
-    const float4 xv = *reinterpret_cast<const float4*>(x + b.row0);
-    const float4 dv = *reinterpret_cast<const float4*>(diag32 + b.row0);
-    float sum[4] = {__fmul_rn(xv.x, dv.x), __fmul_rn(xv.y, dv.y), __fmul_rn(xv.z, dv.z), __fmul_rn(xv.w, dv.w)};
+    T xv[4], dv[4], sum[4];
+    Quad<T>::load(x + b.row0, xv);
+    Quad<T>::load(diag + b.row0, dv);
+#pragma unroll
+    for(int q = 0; q < 4; ++q) sum[q] = mul_rn(xv[q], dv[q]);
     add_slots4<kAfter, kG>(c, b, x, L.m, sum);
-    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
-    *reinterpret_cast<float4*>(x + b.row0) = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
+    T inv[4], out[4];
+    Quad<T>::load(inv_diag + b.row0, inv);
+#pragma unroll
+    for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
+    Quad<T>::store(x + b.row0, out);
 }
 
-template <int kG>
-__global__ void __launch_bounds__(kV4X * kV4Y) k32v_sweep(const ColorLaunch c, const StencilLevel L,
-                                                          const float* __restrict__ inv_diag32,
-                                                          const float* __restrict__ r, float* x,
-                                                          double* __restrict__ z64)
+// Full sweep of one colour; FP32 with z64: also the FP64 copy of the new x.
+template <typename T, int kG>
+__global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, const StencilLevel L,
+                                                        const T* __restrict__ inv_diag, const T* __restrict__ r, T* x,
+                                                        double* __restrict__ z64)
 {
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
-    const float4 rv = *reinterpret_cast<const float4*>(r + b.row0);
-    float sum[4] = {rv.x, rv.y, rv.z, rv.w};
+    T sum[4];
+    Quad<T>::load(r + b.row0, sum);
     add_slots4<kOff, kG>(c, b, x, L.m, sum);
-    const float4 inv = *reinterpret_cast<const float4*>(inv_diag32 + b.row0);
-    const float4 xn = make_float4(sum[0] * inv.x, sum[1] * inv.y, sum[2] * inv.z, sum[3] * inv.w);
-    *reinterpret_cast<float4*>(x + b.row0) = xn;
-    if(z64)
+    T inv[4], out[4];
+    Quad<T>::load(inv_diag + b.row0, inv);
+#pragma unroll
+    for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
+    Quad<T>::store(x + b.row0, out);
+    if constexpr(sizeof(T) == 4)
     {
-        *reinterpret_cast<double2*>(z64 + b.row0) = make_double2((double)xn.x, (double)xn.y);
-        *reinterpret_cast<double2*>(z64 + b.row0 + 2) = make_double2((double)xn.z, (double)xn.w);
+        if(z64)
+        {
+            const double zo[4] = {(double)out[0], (double)out[1], (double)out[2], (double)out[3]};
+            Quad<double>::store(z64 + b.row0, zo);
+        }
     }
 }
 
 // Restriction on the 4-row layout: the injected fine points are the parity-0
 // colour's brick, whose brick-local index is the coarse natural index, so
 // rc[inj_c[row - off]] = (rf - A xf)[row] with the same per-row arithmetic as
-// k32_restrict (slot order, fmaf(-a_ii, x_i, .) at the diagonal slot).
-template <int kG>
-__global__ void __launch_bounds__(kV4X * kV4Y) k32v_restrict(const ColorLaunch c, const StencilLevel L,
-                                                             const int* __restrict__ inj_c,
-                                                             const float* __restrict__ diag32,
-                                                             const float* __restrict__ rf, const float* __restrict__ xf,
-                                                             float* __restrict__ rc)
+// the ELL restriction (slot order, fma(-a_ii, x_i, .) at the diagonal slot).
+template <typename T, int kG>
+__global__ void __launch_bounds__(kV4X * kV4Y) kv_restrict(const ColorLaunch c, const StencilLevel L,
+                                                           const int* __restrict__ inj_c, const T* __restrict__ diag,
+                                                           const T* __restrict__ rf, const T* __restrict__ xf,
+                                                           T* __restrict__ rc)
 {
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
-    const float4 rv = *reinterpret_cast<const float4*>(rf + b.row0);
-    float sum[4] = {rv.x, rv.y, rv.z, rv.w};
-    // slots before the diagonal, fmaf(-a_ii, x_i, .) at it, slots after it
+    T sum[4];
+    Quad<T>::load(rf + b.row0, sum);
+    // slots before the diagonal, fma(-a_ii, x_i, .) at it, slots after it
     add_slots4<kBefore, kG>(c, b, xf, L.m, sum);
-    const float4 xv = *reinterpret_cast<const float4*>(xf + b.row0);
-    const float4 dv = *reinterpret_cast<const float4*>(diag32 + b.row0);
-    sum[0] = fmaf(-dv.x, xv.x, sum[0]);
-    sum[1] = fmaf(-dv.y, xv.y, sum[1]);
-    sum[2] = fmaf(-dv.z, xv.z, sum[2]);
-    sum[3] = fmaf(-dv.w, xv.w, sum[3]);
+    T xv[4], dv[4];
+    Quad<T>::load(xf + b.row0, xv);
+    Quad<T>::load(diag + b.row0, dv);
+#pragma unroll
+    for(int q = 0; q < 4; ++q) sum[q] = fma_rn(-dv[q], xv[q], sum[q]);
     add_slots4<kAfter, kG>(c, b, xf, L.m, sum);
     const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
     rc[ic.x] = sum[0];
@@ -523,8 +575,9 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_restrict(const ColorLaunch c
 }
 
 // xf[row] += xc[inj_c[row - off]] over the parity-0 colour's brick.
-__global__ void __launch_bounds__(kV4X * kV4Y) k32v_prolong(const ColorLaunch c, const int* __restrict__ inj_c,
-                                                            const float* __restrict__ xc, float* __restrict__ xf)
+template <typename T>
+__global__ void __launch_bounds__(kV4X * kV4Y) kv_prolong(const ColorLaunch c, const int* __restrict__ inj_c,
+                                                          const T* __restrict__ xc, T* __restrict__ xf)
 {
     const int kx0 = (blockIdx.x * kV4X + threadIdx.x) * 4;
     const int ky = blockIdx.y * kV4Y + threadIdx.y;
@@ -532,12 +585,13 @@ __global__ void __launch_bounds__(kV4X * kV4Y) k32v_prolong(const ColorLaunch c,
     if(!(kx0 < c.bx && ky < c.by && kz < c.bz)) return;
     const int row0 = c.off + (kz * c.by + ky) * c.bx + kx0;
     const int4 ic = *reinterpret_cast<const int4*>(inj_c + (row0 - c.off));
-    float4 x = *reinterpret_cast<const float4*>(xf + row0);
-    x.x += xc[ic.x];
-    x.y += xc[ic.y];
-    x.z += xc[ic.z];
-    x.w += xc[ic.w];
-    *reinterpret_cast<float4*>(xf + row0) = x;
+    T x[4];
+    Quad<T>::load(xf + row0, x);
+    x[0] += xc[ic.x];
+    x[1] += xc[ic.y];
+    x[2] += xc[ic.z];
+    x[3] += xc[ic.w];
+    Quad<T>::store(xf + row0, x);
 }
 
 // ----------------------------------------------------- FP64 stencil SpMV
@@ -1198,13 +1252,13 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         const dim3 g = brick_grid(c);
         if(vec && small)
         {
-            if(r64) k32v_fwd0<true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
-            else k32v_fwd0<false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+            if(r64) kv_fwd0<float, true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else kv_fwd0<float, false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
         }
         else if(vec)
         {
-            if(r64) k32v_fwd0<true, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
-            else k32v_fwd0<false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+            if(r64) kv_fwd0<float, true, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
+            else kv_fwd0<float, false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
         }
         else if(L.even)
         {
@@ -1222,8 +1276,8 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(vec && small) k32v_bwd0<kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
-        else if(vec) k32v_bwd0<kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        if(vec && small) kv_bwd0<float, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        else if(vec) kv_bwd0<float, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
         else if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         HB_LAUNCHED();
@@ -1241,9 +1295,9 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
         if(vec && small)
-            k32v_sweep<kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+            kv_sweep<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
         else if(vec)
-            k32v_sweep<kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+            kv_sweep<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
         else if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         else k32_sweep<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         HB_LAUNCHED();
@@ -1261,9 +1315,9 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     const bool vec = vec4_ok(Lf) && nc == c.bx * c.by * c.bz;
     if(vec && Lf.m / 8 < kV4SmallRows)
-        k32v_restrict<kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+        kv_restrict<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
     else if(vec)
-        k32v_restrict<kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+        kv_restrict<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
     else if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     else k32_restrict<false><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     HB_LAUNCHED();
@@ -1275,9 +1329,93 @@ int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
-        k32v_prolong<<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
+        kv_prolong<float><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
     else
         k32_prolong<<<nblk(nc), kBS32, 0, s>>>(nc, inj_f, inj_c, xc, xf);
+    HB_LAUNCHED();
+    return 0;
+}
+
+// ------------------------------------------ FP64 V-cycle on the implicit stencil
+// The same 4-row kernels in double precision: each row performs the ELL
+// kernels' operations in the same order (sum + x == fma(1, x, sum) per
+// off-diagonal slot, x * (1/a_ii), x_i * a_ii rounded then the later slots,
+// fma(-a_ii, x_i, .) in the restriction), so the results are the FP64 ELL
+// V-cycle's bits without reading the matrix.
+
+bool stencil_vec4(const StencilLevel& L) { return vec4_ok(L); }
+
+int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double* inv_diag, const double* r,
+                         double* x, cudaStream_t s)
+{
+    if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
+    const dim3 t4(kV4X, kV4Y);
+    const bool small = L.m / 8 < kV4SmallRows;
+    for(int v = 0; v < L.ncolors; ++v)
+    {
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
+        const ColorLaunch c = color_launch(L, v);
+        if(small)
+            kv_fwd0<double, false, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
+                                                                                const_cast<double*>(r), x);
+        else
+            kv_fwd0<double, false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
+                                                                              const_cast<double*>(r), x);
+        HB_LAUNCHED();
+    }
+    for(int v = L.ncolors - 2; v >= 0; --v)
+    {
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
+        const ColorLaunch c = color_launch(L, v);
+        if(small) kv_bwd0<double, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
+        else kv_bwd0<double, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
+        HB_LAUNCHED();
+    }
+    return 0;
+}
+
+int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double* r, double* x, cudaStream_t s)
+{
+    if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
+    const bool small = L.m / 8 < kV4SmallRows;
+    auto sweep = [&](int v) -> int {
+        if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
+        const ColorLaunch c = color_launch(L, v);
+        if(small)
+            kv_sweep<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
+                                                                                        nullptr);
+        else
+            kv_sweep<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
+                                                                                      nullptr);
+        HB_LAUNCHED();
+        return 0;
+    };
+    for(int v = 0; v < L.ncolors; ++v) HB_RETURN_IF(sweep(v));
+    for(int v = L.ncolors - 2; v >= 0; --v) HB_RETURN_IF(sweep(v));
+    return 0;
+}
+
+int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const double* diag, const double* rf,
+                       const double* xf, double* rc, cudaStream_t s)
+{
+    const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
+    if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
+        return record_error(HPCGB200_ERR_ARG, "FP64 stencil restriction: colour bricks not 4-aligned");
+    if(Lf.m / 8 < kV4SmallRows)
+        kv_restrict<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
+                                                                                       rc);
+    else
+        kv_restrict<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf, rc);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch64v_prolong(const StencilLevel& Lf, int nc, const int* inj_c, const double* xc, double* xf, cudaStream_t s)
+{
+    const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
+    if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
+        return record_error(HPCGB200_ERR_ARG, "FP64 stencil prolongation: colour bricks not 4-aligned");
+    kv_prolong<double><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
     HB_LAUNCHED();
     return 0;
 }

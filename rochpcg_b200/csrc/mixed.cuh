@@ -75,6 +75,18 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
 int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* xc, float* xf,
                      cudaStream_t s);
 
+// FP64 V-cycle pieces on the implicit stencil, bitwise equal to the ELL
+// kernels (launch_symgs_zero, launch_symgs, launch_restrict, launch_prolong);
+// they need stencil_vec4(L): every colour brick's x extent and offset a
+// multiple of 4 (else HPCGB200_ERR_ARG).
+bool stencil_vec4(const StencilLevel& L);
+int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double* inv_diag, const double* r,
+                         double* x, cudaStream_t s);
+int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double* r, double* x, cudaStream_t s);
+int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const double* diag, const double* rf,
+                       const double* xf, double* rc, cudaStream_t s);
+int launch64v_prolong(const StencilLevel& Lf, int nc, const int* inj_c, const double* xc, double* xf, cudaStream_t s);
+
 // FP64 y = A x on the implicit stencil (bitwise equal to the ELL SpMV: same
 // slot order, fma(-1, x, s) == s - x, fma(a_ii, x_i, s) on the diagonal).
 int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s);

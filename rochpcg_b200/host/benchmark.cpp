@@ -230,8 +230,11 @@ extern "C" int hpcgb200_benchmark_report(hpcgb200_benchmark_result* R, char* jso
     J.text("HPCG-Benchmark version", "3.1");
     J.open("Implementation");
     J.text("Name", "rochpcg_b200 (B200, sm_100a)");
-    J.text("Precision", R->mode == HPCGB200_MODE_MIXED ? "mixed: FP64 CG, FP32 V-cycle on the implicit stencil"
-                                                       : "FP64");
+    J.text("Precision", R->mode == HPCGB200_MODE_MIXED
+                            ? "mixed: FP64 CG, FP32 V-cycle on the implicit stencil"
+                            : (R->mode == HPCGB200_MODE_FP64_STENCIL
+                                   ? "FP64 on the implicit stencil (the ELL path's results, no matrix reads)"
+                                   : "FP64"));
     J.boolean("Reference phases run", R->verify != 0);
     J.close();
     J.open("Machine Summary");
@@ -438,12 +441,14 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     if(d[0] % div || d[1] % div || d[2] % div)
         return hb::record_error(HPCGB200_ERR_ARG, "dimensions must be divisible by %d", div);
     if((long long)d[0] * d[1] * d[2] > 0x7fffffffLL) return hb::record_error(HPCGB200_ERR_ARG, "grid exceeds 2^31 rows");
-    if(P.mode != HPCGB200_MODE_FP64 && P.mode != HPCGB200_MODE_MIXED)
-        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED");
+    if(P.mode != HPCGB200_MODE_FP64 && P.mode != HPCGB200_MODE_MIXED && P.mode != HPCGB200_MODE_FP64_STENCIL)
+        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64, _MIXED or _FP64_STENCIL");
     const bool verify = P.verify != 0;
     const bool quickPath = P.running_time == 0;
-    const MGPrecision prec = P.mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32 : MGPrecision::FP64;
-    const bool flexible = prec != MGPrecision::FP64;
+    const MGPrecision prec = P.mode == HPCGB200_MODE_MIXED
+                                 ? MGPrecision::FP32
+                                 : (P.mode == HPCGB200_MODE_FP64_STENCIL ? MGPrecision::FP64_STENCIL : MGPrecision::FP64);
+    const bool flexible = needs_flexible(prec);
     R.nx = d[0];
     R.ny = d[1];
     R.nz = d[2];

@@ -45,6 +45,7 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     if(precond)
     {
         if(prec == MGPrecision::FP64) HB_RETURN_IF(ComputeMG(A, data.r, data.z));
+        else if(prec == MGPrecision::FP64_STENCIL) HB_RETURN_IF(ComputeMG_Stencil(A, data.r, data.z));
         else if(prec == MGPrecision::FP32) HB_RETURN_IF(ComputeMG_Mixed(A, data.r, data.z));
         else HB_RETURN_IF(ComputeMG_Learned(A, data.r, data.z));
     }
@@ -56,7 +57,15 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     }
     HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
     HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
-    if(prec != MGPrecision::FP64)
+    if(prec == MGPrecision::FP64_STENCIL)
+    {
+        // the implicit-stencil product, then p.Ap with the ELL kernel's partition: the FP64 path's scalars
+        const LevelOpt* o = opt(A);
+        HB_RETURN_IF(hb::launch64_spmv_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, s));
+        HB_RETURN_IF(hb::launch_cg_pap_chunks(n, o->cc, data.p.d_values, data.Ap.d_values, st, o->spmv_partial,
+                                              o->spmv_ticket, s));
+    }
+    else if(prec != MGPrecision::FP64)
     {
         // mixed path: the FP64 operator on the implicit stencil (bitwise equal to the ELL product)
         const LevelOpt* o = opt(A);
@@ -239,7 +248,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             for(const SparseMatrix* M = &A; M; M = M->Ac)
                 if(!opt(*M) || !opt(*M)->stencil_ok)
                     return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
-                                            "mixed CG needs the 27-point stencil in parity colouring on every level");
+                                            "stencil CG needs the 27-point stencil in parity colouring on every level");
             check(hb::launch64_spmv_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, s));
         }
         else

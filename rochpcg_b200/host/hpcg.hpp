@@ -149,8 +149,12 @@ enum class MGPrecision
 {
     FP64 = 0,    // the reference's optimized path, FP64 ELL
     FP32 = 1,    // FP32 vectors + FP32 accumulation, implicit stencil values
-    LEARNED = 2  // FP32 V-cycle whose coarse levels use the learned conv-net smoother
+    LEARNED = 2,  // FP32 V-cycle whose coarse levels use the learned conv-net smoother
+    FP64_STENCIL = 3  // FP64 V-cycle and SpMV on the implicit stencil: the FP64 path's bits, no matrix reads
 };
+
+// Preconditioners that need flexible (Polak-Ribiere) CG.
+inline bool needs_flexible(MGPrecision p) { return p == MGPrecision::FP32 || p == MGPrecision::LEARNED; }
 
 // ---------------------------------------------------------------- runtime
 // One stream and one reduction workspace per process, like the reference's
@@ -206,6 +210,11 @@ int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x);
 // and post-smoothing SymGS (x = N(r); ...; x += N(r - A x)) and the coarsest
 // solve.  Nonlinear and non-symmetric: use it inside flexible CG.
 int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x);
+// ComputeMG on the implicit stencil (no reference counterpart): the same
+// operations in the same order as ComputeMG, so z is bitwise the same, with
+// no matrix reads on levels whose colour bricks are 4-aligned (the others
+// use the ELL kernels).
+int ComputeMG_Stencil(const SparseMatrix& A, const Vector& r, Vector& x);
 
 // --------------------------------------------------------------- solver
 int CG(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const int max_iter, const double tolerance,

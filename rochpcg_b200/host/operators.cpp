@@ -160,6 +160,54 @@ int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x)
     });
 }
 
+namespace {
+
+bool stencil_vec_level(const SparseMatrix& A)
+{
+    const LevelOpt* o = opt(A);
+    return o && o->stencil_ok && hb::stencil_vec4(o->st);
+}
+
+// ComputeMG's recursion (1 zero-guess pre-smoothing step, fused restriction,
+// coarse solve, prolongation, 1 post-smoothing step) per level on the
+// implicit-stencil kernels or, where the bricks are not 4-aligned, the ELL ones.
+int mg64_stencil(const SparseMatrix& A, const double* r, double* x, cudaStream_t s)
+{
+    const LevelOpt* o = opt(A);
+    const bool vec = stencil_vec_level(A);
+    if(vec) HB_RETURN_IF(hb::launch64v_symgs_zero(o->st, o->diag, A.inv_diag, r, x, s));
+    else
+        HB_RETURN_IF(hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets,
+                                           A.ell_col_ind, A.ell_val, A.diag_idx, o->diag, A.inv_diag, r, x, s));
+    if(!A.mgData) return 0;
+    const MGOpt* mo = mgopt(A);
+    const int nc = A.Ac->localNumberOfRows;
+    double* rc = A.mgData->rc->d_values;
+    double* xc = A.mgData->xc->d_values;
+    if(vec) HB_RETURN_IF(hb::launch64v_restrict(o->st, nc, mo->inj_c, o->diag, r, x, rc, s));
+    else
+        HB_RETURN_IF(hb::launch_restrict(nc, mo->inj_f, mo->inj_c, A.localNumberOfRows, A.ell_col_ind, A.ell_val, r, x,
+                                         rc, s));
+    HB_RETURN_IF(mg64_stencil(*A.Ac, rc, xc, s));
+    if(vec) HB_RETURN_IF(hb::launch64v_prolong(o->st, nc, mo->inj_c, xc, x, s));
+    else HB_RETURN_IF(hb::launch_prolong(nc, mo->inj_f, mo->inj_c, xc, x, s));
+    if(vec) return hb::launch64v_symgs(o->st, A.inv_diag, r, x, s);
+    return hb::launch_symgs(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind, A.ell_val,
+                            A.inv_diag, r, x, s);
+}
+
+}  // namespace
+
+int ComputeMG_Stencil(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] {
+        for(const SparseMatrix* M = &A; M; M = M->Ac)
+            if(M->mgData && (M->mgData->numberOfPresmootherSteps != 1 || M->mgData->numberOfPostsmootherSteps != 1))
+                return hb::record_error(HPCGB200_ERR_ARG, "stencil V-cycle: 1 pre- and 1 post-smoothing step only");
+        return mg64_stencil(A, r.d_values, x.d_values, rt().stream);
+    });
+}
+
 // src/ComputeDotProduct.cpp:189-238 (blocking, like the reference).
 int ComputeDotProduct(local_int_t n, const Vector& x, const Vector& y, double& result, double& time_allreduce,
                       bool& isOptimized)

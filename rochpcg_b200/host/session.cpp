@@ -24,14 +24,25 @@ namespace {
 
 MGPrecision prec_of(int mode)
 {
-    return mode == HPCGB200_MODE_MIXED ? MGPrecision::FP32
-                                       : (mode == HPCGB200_MODE_LEARNED ? MGPrecision::LEARNED : MGPrecision::FP64);
+    switch(mode)
+    {
+    case HPCGB200_MODE_MIXED: return MGPrecision::FP32;
+    case HPCGB200_MODE_LEARNED: return MGPrecision::LEARNED;
+    case HPCGB200_MODE_FP64_STENCIL: return MGPrecision::FP64_STENCIL;
+    default: return MGPrecision::FP64;
+    }
 }
 
 bool mode_ok(int mode)
 {
-    return mode == HPCGB200_MODE_FP64 || mode == HPCGB200_MODE_MIXED || mode == HPCGB200_MODE_LEARNED;
+    return mode == HPCGB200_MODE_FP64 || mode == HPCGB200_MODE_MIXED || mode == HPCGB200_MODE_LEARNED ||
+           mode == HPCGB200_MODE_FP64_STENCIL;
 }
+
+bool flexible_of(int mode) { return needs_flexible(prec_of(mode)); }
+
+// modes TestCG / TestSymmetry run with (the learned V-cycle is not symmetric)
+bool test_mode_ok(int mode) { return mode_ok(mode) && mode != HPCGB200_MODE_LEARNED; }
 
 template <typename F>
 int guarded(F&& f)
@@ -315,7 +326,7 @@ extern "C" int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, 
     return guarded([&] {
         CudaZeroVector(p->x);
         return run_cg(p->A, p->data, p->b, p->x, max_iter, tol, *niters, *normr, *normr0, precond != 0, prec_of(mode),
-                      mode != HPCGB200_MODE_FP64, normr_hist, seconds);
+                      flexible_of(mode), normr_hist, seconds);
     });
 }
 
@@ -335,7 +346,7 @@ extern "C" int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const 
         check(hpcgb200_permute_vector(m, p->A.perm, tmp, p->b.d_values, s));
         HB_HOST_CUDA(cudaMemsetAsync(p->x.d_values, 0, sizeof(double) * m, s));
         int r = run_cg(p->A, p->data, p->b, p->x, max_iter, tol, *niters, *normr, *normr0, true, prec_of(mode),
-                       mode != HPCGB200_MODE_FP64, nullptr, nullptr);
+                       flexible_of(mode), nullptr, nullptr);
         if(r) return r;
         check(hpcgb200_unpermute_vector(m, p->A.perm, p->x.d_values, tmp, s));
         HB_HOST_CUDA(cudaMemcpyAsync(x_natural, tmp, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
@@ -417,7 +428,7 @@ extern "C" int hpcgb200_problem_kernels_per_iteration(hpcgb200_problem* p, int m
     if(!p || !kernels) return hb::record_error(HPCGB200_ERR_ARG, "null argument");
     if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     return guarded([&] {
-        *kernels = iteration_kernels(p->A, p->data, p->b, p->x, precond != 0, prec_of(mode), mode != HPCGB200_MODE_FP64);
+        *kernels = iteration_kernels(p->A, p->data, p->b, p->x, precond != 0, prec_of(mode), flexible_of(mode));
         return 0;
     });
 }
@@ -426,8 +437,8 @@ extern "C" int hpcgb200_problem_test_cg(hpcgb200_problem* p, int mode, int* out_
                                         int* count_fail)
 {
     if(!p) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
-    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED)
-        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED");
+    if(!test_mode_ok(mode))
+        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64, _MIXED or _FP64_STENCIL");
     TestCGData d{};
     const int rc = TestCG_B200(p->A, p->data, p->b, p->x, d, prec_of(mode));
     if(out_niters)
@@ -441,8 +452,8 @@ extern "C" int hpcgb200_problem_test_symmetry(hpcgb200_problem* p, int mode, dou
                                               double* residual_inf)
 {
     if(!p) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
-    if(mode != HPCGB200_MODE_FP64 && mode != HPCGB200_MODE_MIXED)
-        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64 or HPCGB200_MODE_MIXED");
+    if(!test_mode_ok(mode))
+        return hb::record_error(HPCGB200_ERR_ARG, "mode must be HPCGB200_MODE_FP64, _MIXED or _FP64_STENCIL");
     TestSymmetryData d{};
     const int rc = TestSymmetry_B200(p->A, p->b, p->xexact, d, prec_of(mode));
     if(depsym_spmv) *depsym_spmv = d.depsym_spmv;
@@ -498,7 +509,9 @@ extern "C" int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* 
 {
     if(!p || !r || !x) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     Vector rv = wrap(r, p->A.localNumberOfRows), xv = wrap(x, p->A.localNumberOfRows);
+    if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     if(mode == HPCGB200_MODE_LEARNED) return ComputeMG_Learned(p->A, rv, xv);
+    if(mode == HPCGB200_MODE_FP64_STENCIL) return ComputeMG_Stencil(p->A, rv, xv);
     return mode == HPCGB200_MODE_MIXED ? ComputeMG_Mixed(p->A, rv, xv) : ComputeMG(p->A, rv, xv);
 }
 
@@ -544,6 +557,7 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
         else if(o == "symgs_zero") f = [&] { return ComputeSYMGSZeroGuess(A, r, z); };
         else if(o == "mg") f = [&] { return ComputeMG(A, r, z); };
         else if(o == "mg_mixed") f = [&] { return ComputeMG_Mixed(A, r, z); };
+        else if(o == "mg_stencil") f = [&] { return ComputeMG_Stencil(A, r, z); };
         else if(o == "mg_learned")
         {
             if(!opt(A)->smoother) return hb::record_error(HPCGB200_ERR_ARG, "time_op: no smoother attached");

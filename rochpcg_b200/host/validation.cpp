@@ -63,7 +63,7 @@ int TestCG_B200(SparseMatrix& A, CGData& data, Vector& b, Vector& x, TestCGData&
             {
                 CudaZeroVector(x);
                 rc = CG_B200(A, data, b, x, maxIters, tolerance, niters, normr, normr0, nullptr, k == 1, prec,
-                             prec != MGPrecision::FP64, nullptr);
+                             needs_flexible(prec), nullptr);
                 d.niters[k * 2 + i] = niters;
                 if(niters <= expected) ++d.count_pass;
                 else ++d.count_fail;
@@ -129,7 +129,9 @@ int TestSymmetry_B200(SparseMatrix& A, Vector& b, Vector& xexact, TestSymmetryDa
 
     // x'M^{-1}y vs y'M^{-1}x
     auto mg = [&](const Vector& r, Vector& z) {
-        return prec == MGPrecision::FP64 ? ComputeMG(A, r, z) : ComputeMG_Mixed(A, r, z);
+        if(prec == MGPrecision::FP64) return ComputeMG(A, r, z);
+        if(prec == MGPrecision::FP64_STENCIL) return ComputeMG_Stencil(A, r, z);
+        return ComputeMG_Mixed(A, r, z);
     };
     ierr |= mg(y_ncol, z_ncol);
     double xtMinvy = 0.0;
@@ -140,7 +142,7 @@ int TestSymmetry_B200(SparseMatrix& A, Vector& b, Vector& xexact, TestSymmetryDa
     d.depsym_mg = std::fabs((long double)(xtMinvy - ytMinvx)) / ((xNorm2 * ANorm * yNorm2 + yNorm2 * ANorm * xNorm2) * (DBL_EPSILON));
     // an FP32 V-cycle is symmetric to single-precision rounding: the same
     // departure (still reported in DBL_EPSILON units) is judged at FLT_EPSILON
-    const double mg_limit = prec == MGPrecision::FP64 ? 1.0 : (double)FLT_EPSILON / DBL_EPSILON;
+    const double mg_limit = needs_flexible(prec) ? (double)FLT_EPSILON / DBL_EPSILON : 1.0;
     if(d.depsym_mg > mg_limit) ++d.count_fail;
 
     // ||A xexact - b||_inf, twice (src/TestSymmetry.cpp:150-160)
