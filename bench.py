@@ -13,9 +13,15 @@ device time).  The same line carries:
                the measured HBM copy bandwidth
   cpu_baseline the reference's own CPU path (CG_ref, OpenMP) on a bounded
                sample, timed on this machine's host cores
+  fp64_stencil the same 256^3 solve with the V-cycle and SpMV on the implicit
+               stencil (HPCGB200_MODE_FP64_STENCIL): the FP64 residual history
+               bit for bit without matrix reads
   mixed        FP64-outer / FP32 V-cycle solve at 320^3 with b ~ N(0,1)
-               (seed 0) vs the FP64 path on the same system, both verified
-               with an FP64 true residual
+               (seed 0) vs the FP64 path (ELL and implicit) on the same
+               system, all verified with an FP64 true residual
+  learned      the learned coarse-level smoother vs SymGS at 256^3
+               (b ~ N(0,1), seed 9999), with the tcgen05 conv kernel's
+               tensor roofline
 
 `--impl reference` times the reference's CPU CG_ref on this machine instead.
 Under torchrun (N>1) every rank solves its own local problem (HPCG weak
@@ -341,6 +347,19 @@ def run_ours(args):
     spmv_bytes = m * (27 * 12 + 8 + 8)
     extra_kernels = {"spmv_GBps": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "spmv_ms": spmv_ms,
                      "mg_ms": P.time_op("mg", 5)}
+
+    # ---- the same solve on the implicit stencil: FP64 history bit for bit, no matrix reads
+    stencil = None
+    if P.stencil_ok(0):
+        P.cg(args.max_iter, args.tol, mode=R.MODE_FP64_STENCIL)
+        barrier()
+        s_runs = [P.cg(args.max_iter, args.tol, mode=R.MODE_FP64_STENCIL) for _ in range(args.steps)]
+        s_min = min(r["seconds"] for r in s_runs)
+        stencil = {"time_to_solution_s": s_min, "iterations": s_runs[-1]["niters"],
+                   "gflops_hpcg_model": flops_it * s_runs[-1]["niters"] / s_min / 1e9,
+                   "history_bitwise_equal_to_fp64": bool(np.array_equal(s_runs[-1]["hist"], runs[-1]["hist"])),
+                   "speedup_vs_fp64_ell": ms_step * 1e-3 / s_min,
+                   "mg_ms": P.time_op("mg_stencil", 5)}
     P.close()
     del P
 
@@ -383,7 +402,8 @@ def run_ours(args):
             "model_GBps": world * bytes_it * iters / (ms_step * 1e-3) / 1e9,
             "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m,
                     "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err},
-            "roofline": roofline, "kernels": extra_kernels, "cpu_baseline": cpu, "mixed": mixed,
+            "roofline": roofline, "kernels": extra_kernels, "fp64_stencil": stencil, "cpu_baseline": cpu,
+            "mixed": mixed,
             "learned": learned, "largest": largest,
             "gpu_launches": launches, "clocks": clocks,
         }
