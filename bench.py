@@ -243,25 +243,60 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------------ rank plumbing
+# One process per GPU; every rank solves its own local problem (replicas, no
+# collective on the data path); the only collectives are the barriers around
+# the timed region and the max of the timings.
+
+def ranks() -> tuple[int, int, int]:
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def init_dist(world: int, local: int, backend: str, timeout_s: int = 600):
+    """torch.distributed for world > 1 (nccl on the GPUs, gloo in the CPU
+    tests), else None.  MASTER_ADDR / MASTER_PORT come from the launcher."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    kw = {}
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        kw["device_id"] = torch.device("cuda", local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+    return dist
+
+
+def max_over(dist, v: float, device: str) -> float:
+    """max of v over all ranks (v itself without a process group)."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gflops(world: int, flops_per_iter: float, iters: int, seconds_per_step: float) -> float:
+    """Whole-job GFLOP/s: every rank solves its own problem of the same size in
+    the (max-over-ranks) step time."""
+    return world * flops_per_iter * iters / seconds_per_step / 1e9
+
+
 # ------------------------------------------------------------------ our arm
 
 def run_ours(args):
     import torch
     import rochpcg_b200 as R
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    else:
+    world, rank, local = ranks()
+    dist = init_dist(world, local, "nccl")
+    if dist is None:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
@@ -271,11 +306,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over(dist, v, "cuda")
 
     if args.mixed_only:
         return run_mixed_only(args, R, barrier)
@@ -304,7 +335,7 @@ def run_ours(args):
     ms_total = max_over_ranks(e0.elapsed_time(e1))
     iters = runs[-1]["niters"]
     ms_step = ms_total / args.steps
-    value = world * flops_it * iters / (ms_step * 1e-3) / 1e9
+    value = job_gflops(world, flops_it, iters, ms_step * 1e-3)
     rel = runs[-1]["normr"] / runs[-1]["normr0"]
     true_rel = P.true_residual()
     kpi = P.kernels_per_iteration(R.MODE_FP64)
@@ -329,7 +360,7 @@ def run_ours(args):
         re = P.solve_host(b_host, x_host, 1000, args.tol)
     barrier()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
-    e2e_val = world * flops_it * re["niters"] / e2e_s / 1e9
+    e2e_val = job_gflops(world, flops_it, re["niters"], e2e_s)
     x_err = float(torch.max(torch.abs(x_host - 1.0)))
 
     # ---- dominant kernel: level-0 full SymGS colour sweep
