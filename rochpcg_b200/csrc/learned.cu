@@ -790,6 +790,157 @@ __global__ void k_odd_natural(long n, const float* __restrict__ y, float* __rest
     if(p < n) out[p] = 0.5f * (y[p] - y[p + n]);
 }
 
+// ------------------------------------------- layers 1 and 3 on the CUDA cores
+// Layer 1 has one real input channel and layer 3 one real output channel, so
+// 15/16 of their tensor-core MMA work multiplies zeros.  For evaluation they
+// run here instead, in FP32 with the BF16-rounded weights: layer 1 fused with
+// the odd pair (the second branch's pre-activation is exactly -z), layer 3
+// fused with the odd combination and the scatter into the level vector.
+
+// Bf16 scalar field of a level: r, or the residual r - A x (k_embed_level's
+// channel 0 without the 15 zero channels and the negated copy).
+__global__ void k_embed_scalar_level(PermMap pm, int nz, int ny, int nx, const float* __restrict__ r,
+                                     const float* __restrict__ x, const float* __restrict__ diag32,
+                                     __nv_bfloat16* __restrict__ s1)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= (long)nz * ny * nx) return;
+    const int z = (int)(p / ((long)ny * nx));
+    const long rem = p - (long)z * ny * nx;
+    const int y = (int)(rem / nx), xx = (int)(rem - (long)y * nx);
+    const int row = perm_row(pm, z, y, xx);
+    float v = r[row];
+    if(x)
+    {
+        float off = 0.f;
+#pragma unroll
+        for(int t = 0; t < 27; ++t)
+        {
+            const int z2 = z + t / 9 - 1, y2 = y + (t / 3) % 3 - 1, x2 = xx + t % 3 - 1;
+            if(t != 13 && z2 >= 0 && z2 < nz && y2 >= 0 && y2 < ny && x2 >= 0 && x2 < nx)
+                off += x[perm_row(pm, z2, y2, x2)];
+        }
+        v = v - (diag32[row] * x[row] - off);
+    }
+    s1[p] = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ float in_value(const __nv_bfloat16* v, long q) { return __bfloat162float(v[q]); }
+__device__ __forceinline__ float in_value(const float* v, long q) { return __bfloat162float(__float2bfloat16_rn(v[q])); }
+
+// a1[p] = bf16(relu(z)), z[co] = sum_t w1[t][0][co] in[p + t]; with kPair also
+// a1[p + n] = bf16(relu(-z)) (the branch of -in).  nb samples back to back.
+template <bool kPair, typename Tin>
+__global__ void __launch_bounds__(256) k_layer1_direct(ConvGrid g, const Tin* __restrict__ in,
+                                                       const float* __restrict__ w1, __nv_bfloat16* __restrict__ a1)
+{
+    __shared__ float w[27 * kNetCh];
+    for(int i = threadIdx.x; i < 27 * kNetCh; i += blockDim.x)
+        w[i] = __bfloat162float(__float2bfloat16_rn(w1[(i / kNetCh) * kNetCh * kNetCh + (i % kNetCh)]));
+    __syncthreads();
+    const long n = g.points();
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long base = (p / per) * per;
+    const long q0 = p - base;
+    const int z = (int)(q0 / ((long)g.ny * g.nx));
+    const long rem = q0 - (long)z * g.ny * g.nx;
+    const int y = (int)(rem / g.nx), x = (int)(rem - (long)y * g.nx);
+    float acc[kNetCh];
+#pragma unroll
+    for(int co = 0; co < kNetCh; ++co) acc[co] = 0.f;
+#pragma unroll
+    for(int t = 0; t < 27; ++t)
+    {
+        const int zz = z + t / 9 - 1, yy = y + (t / 3) % 3 - 1, xx = x + t % 3 - 1;
+        if(zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) continue;
+        const float v = in_value(in, base + ((long)zz * g.ny + yy) * g.nx + xx);
+#pragma unroll
+        for(int co = 0; co < kNetCh; ++co) acc[co] = fmaf(v, w[t * kNetCh + co], acc[co]);
+    }
+    float pos[kNetCh];
+#pragma unroll
+    for(int co = 0; co < kNetCh; ++co) pos[co] = fmaxf(acc[co], 0.f);
+    uint4* dst = reinterpret_cast<uint4*>(a1 + p * kNetCh);
+    dst[0] = pack_bf16x8(pos);
+    dst[1] = pack_bf16x8(pos + 8);
+    if(kPair)
+    {
+        float neg[kNetCh];
+#pragma unroll
+        for(int co = 0; co < kNetCh; ++co) neg[co] = fmaxf(-acc[co], 0.f);
+        uint4* d2 = reinterpret_cast<uint4*>(a1 + (p + n) * kNetCh);
+        d2[0] = pack_bf16x8(neg);
+        d2[1] = pack_bf16x8(neg + 8);
+    }
+}
+
+__device__ __forceinline__ float dot16(const __nv_bfloat16* a, const float* w)
+{
+    const uint4 u0 = *reinterpret_cast<const uint4*>(a);
+    const uint4 u1 = *reinterpret_cast<const uint4*>(a + 8);
+    const __nv_bfloat162* h0 = reinterpret_cast<const __nv_bfloat162*>(&u0);
+    const __nv_bfloat162* h1 = reinterpret_cast<const __nv_bfloat162*>(&u1);
+    float s = 0.f;
+#pragma unroll
+    for(int i = 0; i < 4; ++i)
+    {
+        const float2 f = __bfloat1622float2(h0[i]);
+        s = fmaf(f.x, w[2 * i], s);
+        s = fmaf(f.y, w[2 * i + 1], s);
+    }
+#pragma unroll
+    for(int i = 0; i < 4; ++i)
+    {
+        const float2 f = __bfloat1622float2(h1[i]);
+        s = fmaf(f.x, w[8 + 2 * i], s);
+        s = fmaf(f.y, w[8 + 2 * i + 1], s);
+    }
+    return s;
+}
+
+// Layer 3 output channel 0: y_b[p] = sum_t sum_ci w3[t][ci][0] a2_b[p + t][ci];
+// v = (y_0 - y_1) / 2 with kPair, y_0 otherwise.  kOut 0: x[row(p)] = v,
+// 1: x[row(p)] += v (a level vector through pm, one sample), 2: out[p] = v
+// (natural order, nb samples).
+template <bool kPair, int kOut>
+__global__ void __launch_bounds__(256) k_layer3_direct(ConvGrid g, PermMap pm, const __nv_bfloat16* __restrict__ a2,
+                                                       const float* __restrict__ w3, float* __restrict__ out)
+{
+    __shared__ float w[27 * kNetCh];
+    for(int i = threadIdx.x; i < 27 * kNetCh; i += blockDim.x)
+        w[i] = __bfloat162float(__float2bfloat16_rn(w3[i * kNetCh]));  // w3[t][ci][0]
+    __syncthreads();
+    const long n = g.points();
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const long per = (long)g.nz * g.ny * g.nx;
+    const long base = (p / per) * per;
+    const long q0 = p - base;
+    const int z = (int)(q0 / ((long)g.ny * g.nx));
+    const long rem = q0 - (long)z * g.ny * g.nx;
+    const int y = (int)(rem / g.nx), x = (int)(rem - (long)y * g.nx);
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for(int t = 0; t < 27; ++t)
+    {
+        const int zz = z + t / 9 - 1, yy = y + (t / 3) % 3 - 1, xx = x + t % 3 - 1;
+        if(zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) continue;
+        const long q = base + ((long)zz * g.ny + yy) * g.nx + xx;
+        y0 += dot16(a2 + q * kNetCh, w + t * kNetCh);
+        if(kPair) y1 += dot16(a2 + (q + n) * kNetCh, w + t * kNetCh);
+    }
+    const float v = kPair ? 0.5f * (y0 - y1) : y0;
+    if(kOut == 2) out[p] = v;
+    else
+    {
+        float* o = out + perm_row(pm, z, y, x);
+        if(kOut == 1) *o += v;
+        else *o = v;
+    }
+}
+
 // 1 / (e.e) (kind 0) or 1 / (e.Ae) (kind 1) per sample: one block per sample.
 __global__ void k_sample_norm(ConvGrid g, const float* __restrict__ e, int kind, float* __restrict__ out)
 {
@@ -1029,6 +1180,58 @@ int launch_odd_combine(const PermMap& pm, int nz, int ny, int nx, const float* y
     const long n = (long)nz * ny * nx;
     if(add) k_odd_combine<true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, y, x);
     else k_odd_combine<false><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, y, x);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
+                              const float* diag32, void* s1, cudaStream_t s)
+{
+    const long n = (long)nz * ny * nx;
+    k_embed_scalar_level<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, x, diag32,
+                                                                     (__nv_bfloat16*)s1);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair,
+                         cudaStream_t s)
+{
+    const unsigned grid = (unsigned)((g.points() + 255) / 256);
+    auto* out = (__nv_bfloat16*)a1;
+    if(in_f32)
+    {
+        if(pair) k_layer1_direct<true, float><<<grid, 256, 0, s>>>(g, (const float*)in, w1, out);
+        else k_layer1_direct<false, float><<<grid, 256, 0, s>>>(g, (const float*)in, w1, out);
+    }
+    else
+    {
+        if(pair) k_layer1_direct<true, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
+        else k_layer1_direct<false, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
+    }
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_layer3_direct(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
+                         float* out, cudaStream_t s)
+{
+    if(mode != 2 && (!pm || g.nb != 1)) return record_error(HPCGB200_ERR_ARG, "layer 3: level output needs one sample");
+    const unsigned grid = (unsigned)((g.points() + 255) / 256);
+    const PermMap m = pm ? *pm : PermMap{};
+    const auto* a = (const __nv_bfloat16*)a2;
+    if(pair)
+    {
+        if(mode == 0) k_layer3_direct<true, 0><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+        else if(mode == 1) k_layer3_direct<true, 1><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+        else k_layer3_direct<true, 2><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+    }
+    else
+    {
+        if(mode == 0) k_layer3_direct<false, 0><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+        else if(mode == 1) k_layer3_direct<false, 1><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+        else k_layer3_direct<false, 2><<<grid, 256, 0, s>>>(g, m, a, w3, out);
+    }
     HB_LAUNCHED();
     return 0;
 }

@@ -37,7 +37,7 @@ PermMap make_perm_map(const StencilLevel& L);
 struct ConvGrid
 {
     int nb, nz, ny, nx;
-    long points() const { return (long)nb * nz * ny * nx; }
+    __host__ __device__ long points() const { return (long)nb * nz * ny * nx; }
 };
 
 // FP32 weights -> BF16 tensor-core operand tiles (flip != 0: the mirrored-tap,
@@ -48,6 +48,20 @@ int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s);
 // tensor of kOutMaskBf16, `pm` the row map of the permuted modes (nb == 1).
 int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mode, void* out, const void* act,
                   const PermMap* pm, int* status, cudaStream_t s);
+
+// Evaluation-only layers 1 and 3 on the CUDA cores (FP32 with BF16-rounded
+// weights; layer 1 has one input channel, layer 3 one output channel).
+// s1 = bf16 scalar field of a level (r, or r - A x when x is not null).
+int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
+                              const float* diag32, void* s1, cudaStream_t s);
+// a1 = bf16(relu(conv(in, W1))) from a scalar field in (FP32 when in_f32, else
+// BF16), 16 channels; pair: also the branch of -in at a1 + 16 * points.
+int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair,
+                         cudaStream_t s);
+// Channel 0 of conv(a2, W3), odd-combined when pair ((y(a2) - y(a2 + 16 n)) / 2);
+// mode 0: set, 1: add into a level vector through pm (g.nb == 1); 2: natural out.
+int launch_layer3_direct(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
+                         float* out, cudaStream_t s);
 
 // dw[tap][ci][co] = sum_p x[p + tap][ci] * gr[p][co] (partial: one block of
 // conv16_wgrad_parts(points) x 27*256 floats).
