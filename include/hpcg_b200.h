@@ -210,8 +210,9 @@ typedef struct hpcgb200_problem hpcgb200_problem;
 #define HPCGB200_MODE_FP64 0    /* plain FP64 drop-in (the reference's optimized path) */
 #define HPCGB200_MODE_MIXED 1   /* FP64 outer CG, FP32 V-cycle on the implicit stencil */
 #define HPCGB200_MODE_LEARNED 2 /* as MIXED, with the attached learned smoother on the coarse levels
-                                   (flexible CG; falls back to MIXED once an iteration does not
-                                   reduce the FP64 residual) */
+                                   (flexible CG; falls back to MIXED for good when the FP64
+                                   residual norm jumps, stalls or shrinks too slowly:
+                                   hpcgb200_problem_set_fallback) */
 #define HPCGB200_MODE_FP64_STENCIL 3 /* FP64 as HPCGB200_MODE_FP64, V-cycle and SpMV on the implicit stencil:
                                         the same residual history bit for bit, no matrix reads (needs the
                                         27-point stencil in parity colouring, like MIXED) */
@@ -370,6 +371,12 @@ int hpcgb200_normal_rhs(long long m, unsigned long long seed, double* out, void*
  * and x += N(r - A x); the coarsest level's single SymGS becomes x = N(r)
  * followed by coarse_steps - 1 steps x += N(r - A x) (1..64). */
 int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* s, int first_level, int coarse_steps);
+/* The learned solve's failure rule: it falls back to SymGS for good after an
+ * iteration that multiplies the residual norm by more than `jump` (> 1), after
+ * `stall` iterations without a new minimum, with rate > 0 when the norm is above
+ * rate times its value `window` iterations earlier, or on a non-finite norm.
+ * Defaults: jump 2, stall 16, window 16, rate 0.8 (rate 0 turns that test off). */
+int hpcgb200_problem_set_fallback(hpcgb200_problem* p, double jump, int stall, int window, double rate);
 /* Iteration at which the last learned solve fell back to SymGS (0: never). */
 int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter);
 

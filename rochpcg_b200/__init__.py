@@ -238,6 +238,10 @@ class Problem:
             check(self.L, self.L.hpcgb200_problem_set_smoother(self.h, smoother.h, first_level, coarse_steps))
             self._smoother = smoother  # kept alive while attached
 
+    def set_fallback(self, jump: float = 2.0, stall: int = 16, window: int = 16, rate: float = 0.8):
+        """Failure rule of the learned solve (see hpcgb200_problem_set_fallback)."""
+        check(self.L, self.L.hpcgb200_problem_set_fallback(self.h, jump, stall, window, rate))
+
     def last_fallback(self) -> int:
         """Iteration at which the last MODE_LEARNED solve fell back to SymGS (0: never)."""
         it = ctypes.c_int()

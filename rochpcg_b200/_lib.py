@@ -78,6 +78,7 @@ SIGNATURES = {
     "hpcgb200_problem_solve_host": (_i, [_vp, _i, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp]),
     "hpcgb200_problem_true_residual": (_i, [_vp, _vp]),
     "hpcgb200_problem_cg_ref": (_i, [_vp, _i, _d, _i, _vp, _vp, _vp, _vp]),
+    "hpcgb200_problem_set_fallback": (_i, [_vp, _d, _i, _i, _d]),
     "hpcgb200_problem_mg_ref": (_i, [_vp, _vp, _vp]),
     "hpcgb200_ref_spmv": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_ref_symgs": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -29,6 +29,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_residual0(int n, const do
         st->normr = nr;
         st->normr0 = nr;
         st->hist[0] = nr;
+        st->best_normr = nr;
+        st->since_best = 0;
         st->k = 1;
         st->niters = 0;
         st->rtz = 0.0;
@@ -208,8 +210,20 @@ __global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watc
     const int k = st->k;
     st->niters = k;
     st->k = k + 1;
-    // learned smoother: fall back for good once an iteration fails to reduce normr
-    if(st->net == 1 && !(st->normr < st->hist[k - 1]))
+    const double nr = st->normr;
+    if(nr < st->best_normr)
+    {
+        st->best_normr = nr;
+        st->since_best = 0;
+    }
+    else
+    {
+        st->since_best += 1;
+    }
+    // learned smoother: fall back for good on a jump, a stall or a non-finite residual
+    const bool slow = st->fb_rate > 0.0 && k >= st->fb_window && !(nr <= st->fb_rate * st->hist[k - st->fb_window]);
+    const bool bad = !(nr <= st->fb_jump * st->hist[k - 1]) || st->since_best >= st->fb_stall || slow;
+    if(st->net == 1 && bad)
     {
         st->net = 2;
         st->fallback_iter = k;

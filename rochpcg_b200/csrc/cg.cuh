@@ -19,11 +19,27 @@ struct CGState
     int niters;
     int flexible;         // 1: Polak-Ribiere beta (flexible CG); 0: Fletcher-Reeves as the reference
     int status;           // nonzero: a device-side check failed
-    int net;              // learned smoother: 0 not used, 1 active, 2 failed to reduce normr (fell back)
+    int net;              // learned smoother: 0 not used, 1 active, 2 failed (fell back)
     int fallback_iter;    // iteration at which it failed (0: never); the next iteration restarts p = z
-    int pad;
+    int since_best;       // iterations since normr last reached a new minimum
+    double best_normr;    // smallest normr so far
+    // learned-smoother failure rule (set by the host): an iteration that
+    // multiplies normr by more than fb_jump; fb_stall iterations without a new
+    // minimum; with fb_rate > 0, normr above fb_rate times its value fb_window
+    // iterations earlier; or a non-finite normr.  PCG residual norms are not
+    // monotone, so a single small increase is no failure.
+    double fb_jump, fb_rate;
+    int fb_stall, fb_window;
     double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
 };
+
+// Defaults, chosen on the trained smoother (no false fallback at 64^3..256^3
+// with N(0,1) right-hand sides) and a planted diverging one (caught at
+// iteration 36 of a 64^3 solve): normr must shrink by 20 % every 16 iterations.
+constexpr double kFallbackJump = 2.0;
+constexpr int kFallbackStall = 16;
+constexpr int kFallbackWindow = 16;
+constexpr double kFallbackRate = 0.8;
 
 inline size_t cg_state_bytes(int max_iter) { return sizeof(CGState) + sizeof(double) * (size_t)(max_iter + 1); }
 

@@ -228,6 +228,10 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         h.max_iter = max_iter;
         h.flexible = flexible ? 1 : 0;
         h.net = prec == MGPrecision::LEARNED ? 1 : 0;
+        h.fb_jump = o->fb_jump;
+        h.fb_rate = o->fb_rate;
+        h.fb_stall = o->fb_stall;
+        h.fb_window = o->fb_window;
         if(prec == MGPrecision::LEARNED && !o->smoother)
             return hb::record_error(HPCGB200_ERR_ARG, "learned CG: no smoother attached to the problem");
         if(prec == MGPrecision::LEARNED) check(smoother_ready(A, s));
@@ -260,7 +264,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaStreamSynchronize(s));
 
         // Iterations: the learned mode runs until converged or until its
-        // smoother fails to reduce normr; the plain FP32 V-cycle then takes
+        // smoother fails (a jump or a stall of normr); the plain FP32 V-cycle then takes
         // over from the same state (flexible CG tolerates the switch).
         MGPrecision cur = prec;
         for(int phase = 0; phase < 2; ++phase)

@@ -102,6 +102,10 @@ struct LevelOpt
     int smoother_first_level = 2;
     int smoother_coarse_steps = 1;     // learned Richardson steps x += N(r - A x) on the coarsest level
     int last_fallback_iter = 0;        // learned CG: iteration at which the last solve fell back (0: none)
+    double fb_jump = hb::kFallbackJump;  // learned CG failure rule (CGState)
+    double fb_rate = hb::kFallbackRate;
+    int fb_stall = hb::kFallbackStall;
+    int fb_window = hb::kFallbackWindow;
     hb::PermMap pm{};                  // natural point -> permuted row (stencil levels)
 };
 

@@ -631,6 +631,20 @@ extern "C" int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoot
     });
 }
 
+extern "C" int hpcgb200_problem_set_fallback(hpcgb200_problem* p, double jump, int stall, int window, double rate)
+{
+    if(!p || !opt(p->A)) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
+    if(!(jump > 1.0) || stall < 1 || window < 1 || window > 1000 || !(rate >= 0.0))
+        return hb::record_error(HPCGB200_ERR_ARG, "fallback rule: need jump > 1, stall >= 1, 1 <= window <= 1000, "
+                                                  "rate >= 0");
+    LevelOpt* o = opt(p->A);
+    o->fb_jump = jump;
+    o->fb_stall = stall;
+    o->fb_window = window;
+    o->fb_rate = rate;
+    return 0;
+}
+
 extern "C" int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter)
 {
     if(!p || !fallback_iter) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");

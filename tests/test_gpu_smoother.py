@@ -157,11 +157,25 @@ def test_learned_cg_converges_and_falls_back():
     assert r2["normr"] / r2["normr0"] <= 1e-9
     assert Pr.true_residual() <= 2e-9
     h = r2["hist"]
-    assert all(h[k] < h[k - 1] for k in range(1, fb))
-    assert h[fb] >= h[fb - 1]
+    # the default failure rule held first at iteration fb: normr doubled, or no
+    # new minimum in 16 iterations, or it did not shrink by 20 % in 16 iterations
+    def failed(k):
+        jump = not h[k] <= 2.0 * h[k - 1]
+        stall = k >= 16 and min(h[k - 15:k + 1]) >= min(h[:k - 15])
+        slow = k >= 16 and not h[k] <= 0.8 * h[k - 16]
+        return jump or stall or slow
+    assert failed(fb)
+    assert not any(failed(k) for k in range(1, fb))
     mixed = Pr.cg(500, 1e-9, mode=R.MODE_MIXED)
     assert Pr.last_fallback() == 0
     assert r2["niters"] <= 2 * mixed["niters"]
+    # the rule is the caller's: with every test off the planted smoother runs on
+    Pr.set_fallback(jump=1e300, stall=10 ** 6, window=8, rate=0.0)
+    Pr.cg(40, 1e-9, mode=R.MODE_LEARNED)
+    assert Pr.last_fallback() == 0
+    with pytest.raises(R.HpcgError):
+        Pr.set_fallback(jump=0.5)
+    Pr.set_fallback()
     Pr.set_smoother(None)
 
 
