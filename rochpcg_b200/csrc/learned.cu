@@ -176,14 +176,24 @@ __device__ __forceinline__ uint4 pack_bf16x8(const float* v)
 // 16-column (K = 16) operands with SBO = 256 B, LBO = 128 B.
 __host__ __device__ constexpr uint32_t kmajor_off(int r, int c) { return (uint32_t)((r >> 3) * 256 + c * 128 + (r & 7) * 16); }
 
+// Weight tile slot of tap t = (dz+1)*9 + (dy+1)*3 + (dx+1): the three dz taps
+// of one (dy, dx) are adjacent, ordered dz = +1, 0, -1, so one 48-row K-major
+// B operand (SBO 256 B, tile stride 512 B) holds all three.
+__host__ __device__ constexpr int weight_slot(int t) { return (t % 9) * 3 + 2 - t / 9; }
+
 // ------------------------------------------------------------ forward conv
 //
 // Warp-specialised persistent kernel, one CTA per SM:
 //   warp 0      TMA producer: for each brick, six tiled loads (three dx
 //               shifts x two 8-channel halves) of the halo'd brick into one of
 //               kStages shared-memory stages (zero fill outside the grid);
-//   warp 1      allocates TMEM and issues the brick's 27 x kTZ tcgen05.mma
-//               into one of two TMEM accumulators;
+//   warp 1      allocates TMEM and issues the brick's tcgen05.mma into one of
+//               two TMEM accumulators: for each staged input plane q and
+//               in-plane tap (dy, dx), ONE MMA with N = 16 x (number of output
+//               planes q feeds) multiplies the plane by the stacked weights of
+//               its dz taps (output plane q - 1 - dz lives in columns 16 x that
+//               plane), so a brick of kTZ planes takes 9 (kTZ + 2) + kTZ - 1
+//               MMAs instead of 27 kTZ (57 vs 108 for kTZ = 4);
 //   warps 2-5   epilogue: tcgen05.ld of the finished accumulator, ReLU /
 //               mask / permuted scatter, global stores.
 // Stage and accumulator hand-offs are mbarriers (TMA complete_tx, MMA commit,
@@ -366,7 +376,9 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
     else if(warp == 1 && lane == 0)
     {
         // ---- MMA issuer
-        constexpr uint32_t idesc = umma_idesc_bf16(128, 16, false, false);
+        constexpr uint32_t idesc16 = umma_idesc_bf16(128, 16, false, false);
+        constexpr uint32_t idesc32 = umma_idesc_bf16(128, 32, false, false);
+        constexpr uint32_t idesc48 = umma_idesc_bf16(128, 48, false, false);
         const uint64_t bd0 = umma_desc(smem_u32(sW), 128, 256);
         long i = 0;
         for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
@@ -382,16 +394,35 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             // holds address / 16 and stays below 2^14 for any smem address)
             const uint64_t ad0 = umma_desc(smem_u32(sA + st * kStageBytes), kRegion, 128);
             const uint32_t d0 = tmem + (uint32_t)(acc * kAccCols);
+            // staged plane q (z = z0 - 1 + q) feeds output planes mt = q - 1 - dz
+            // in [lo, hi]; group mt takes B tile j = mt - q + 2 of the (dy, dx)
+            // triple.  Group q is first written at (q, dy = dx = -1), with the
+            // accumulate flag off, by an MMA of its own.
 #pragma unroll
-            for(int t = 0; t < 27; ++t)
+            for(int q = 0; q < kTZ + 2; ++q)
             {
-                const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                const int lo = q - 2 < 0 ? 0 : q - 2;
+                const int hi = q < kTZ - 1 ? q : kTZ - 1;
 #pragma unroll
-                for(int mt = 0; mt < kTZ; ++mt)
+                for(int sxy = 0; sxy < 9; ++sxy)
                 {
-                    const int row0 = ((mt + dz + 1) * kHY + (dy + 1)) * kTX;
+                    const int dy = sxy / 3 - 1, dx = sxy % 3 - 1;
+                    const int row0 = (q * kHY + (dy + 1)) * kTX;
                     const uint64_t ad = ad0 + (uint64_t)(((dx + 1) * kCopyBytes + row0 * 16) >> 4);
-                    mma_bf16(d0 + mt * 16, ad, bd0 + (uint64_t)(t * 512 >> 4), idesc, t > 0 ? 1u : 0u);
+                    const uint64_t bs = bd0 + (uint64_t)((sxy * 3 * 512) >> 4);
+                    if(q <= kTZ - 1 && sxy == 0)
+                    {
+                        if(hi > lo)
+                            mma_bf16(d0 + lo * 16, ad, bs + (uint64_t)(((lo - q + 2) * 512) >> 4),
+                                     hi - lo == 1 ? idesc16 : idesc32, 1u);
+                        mma_bf16(d0 + hi * 16, ad, bs + (uint64_t)(((hi - q + 2) * 512) >> 4), idesc16, 0u);
+                    }
+                    else
+                    {
+                        const int n = hi - lo + 1;
+                        mma_bf16(d0 + lo * 16, ad, bs + (uint64_t)(((lo - q + 2) * 512) >> 4),
+                                 n == 1 ? idesc16 : (n == 2 ? idesc32 : idesc48), 1u);
+                    }
                 }
             }
             mma_commit(&empty[st]);   // stage free once these MMAs have read it
@@ -635,7 +666,7 @@ __global__ void k_prepare_weights(const float* __restrict__ w, __nv_bfloat16* __
     if(i >= kNetLayerWeights) return;
     const int t = i / 256, nn = (i / 16) % 16, kk = i % 16;
     const float v = flip ? w[((26 - t) * 16 + nn) * 16 + kk] : w[(t * 16 + kk) * 16 + nn];
-    unsigned char* base = reinterpret_cast<unsigned char*>(wB) + t * 512;
+    unsigned char* base = reinterpret_cast<unsigned char*>(wB) + weight_slot(t) * 512;
     *reinterpret_cast<__nv_bfloat16*>(base + kmajor_off(nn, kk >> 3) + (kk & 7) * 2) = __float2bfloat16_rn(v);
 }
 
