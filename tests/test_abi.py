@@ -65,6 +65,14 @@ def test_argument_validation_without_device():
     assert L.hpcgb200_f2c_operator(3, 4, 4, None, None, None) == 1  # odd fine dimension
     ws = L.hpcgb200_reduction_workspace_bytes()
     assert ws >= 1184 * 16
+    # reference routines, protocol and learned-solve entry points reject bad input before any device work
+    assert L.hpcgb200_ref_spmv(0, 4, 4, None, None, None, None, None, None) == 1
+    assert L.hpcgb200_ref_symgs(4, 4, 4, None, None, None, None, None, None, None) == 1
+    assert L.hpcgb200_problem_cg_ref(None, 50, 0.0, 1, None, None, None, None) == 1
+    assert L.hpcgb200_problem_mg_ref(None, None, None) == 1
+    assert L.hpcgb200_benchmark_run(None, None) == 1
+    assert L.hpcgb200_benchmark_report(None, None, 0, None) == 1
+    assert L.hpcgb200_problem_set_fallback(None, 2.0, 16, 16, 0.8) == 1
 
 
 def test_no_cpu_fallback_without_device():
