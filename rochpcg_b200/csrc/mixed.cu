@@ -763,192 +763,12 @@ __global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_tile(const StencilLev
 }
 
 
-// ---- specialisation for the colouring the reference's JPL rounds produce
-// (parity class -> colour 7,2,3,6,5,4,1,0 on every grid it was run on): the
-// slot order of each class is a compile-time list, so the 27 neighbour reads
-// use immediate offsets and the staging needs no per-element divisions.
-// Levels with any other colour map take k64_spmv_tile.
+// ---- the colouring the reference's JPL rounds produce (parity class ->
+// colour 7,2,3,6,5,4,1,0 on every grid it was run on): the plane march below
+// compiles the slot order of each class in; levels with any other colour map
+// take k64_spmv_tile.
 constexpr int kCanonColor[8] = {7, 2, 3, 6, 5, 4, 1, 0};
 static_assert(((0x01456327u >> 0) & 15u) == 7 && ((0x01456327u >> 28) & 15u) == 0, "packed canonical colours");
-
-struct CanonSlots
-{
-    int delta[27];  // sub-brick slot offset of ELL slot j for a point of the class
-    int dp;         // slot of the diagonal
-};
-
-__host__ __device__ constexpr CanonSlots canon_slots(int cls)
-{
-    CanonSlots r{};
-    int key[27] = {}, dxs[27] = {}, dys[27] = {}, dzs[27] = {};
-    int k = 0;
-    for(int dz = -1; dz <= 1; ++dz)
-        for(int dy = -1; dy <= 1; ++dy)
-            for(int dx = -1; dx <= 1; ++dx)
-            {
-                const int col = kCanonColor[cls ^ (((dx & 1) << 2) | ((dy & 1) << 1) | (dz & 1))];
-                key[k] = ((col * 3 + (dz + 1)) * 3 + (dy + 1)) * 3 + (dx + 1);  // (colour, dz, dy, dx) order
-                dxs[k] = dx;
-                dys[k] = dy;
-                dzs[k] = dz;
-                ++k;
-            }
-    for(int a = 1; a < 27; ++a)
-        for(int b = a; b > 0 && key[b - 1] > key[b]; --b)
-        {
-            int t = key[b]; key[b] = key[b - 1]; key[b - 1] = t;
-            t = dxs[b]; dxs[b] = dxs[b - 1]; dxs[b - 1] = t;
-            t = dys[b]; dys[b] = dys[b - 1]; dys[b - 1] = t;
-            t = dzs[b]; dzs[b] = dzs[b - 1]; dzs[b - 1] = t;
-        }
-    const int hx = ((cls >> 2) & 1) + 1, hy = ((cls >> 1) & 1) + 1, hz = (cls & 1) + 1;
-    for(int j = 0; j < 27; ++j)
-    {
-        r.delta[j] = sub_index(hx + dxs[j], hy + dys[j], hz + dzs[j]) - sub_index(hx, hy, hz);
-        if(dxs[j] == 0 && dys[j] == 0 && dzs[j] == 0) r.dp = j;
-    }
-    return r;
-}
-
-template <int kCls>
-struct Canon
-{
-    static constexpr CanonSlots s = canon_slots(kCls);
-};
-
-template <int kCls, int J>
-__device__ __forceinline__ void canon_step(double& sum, const double* sp, int c, double d, double xr)
-{
-    constexpr int delta = Canon<kCls>::s.delta[J];
-    if constexpr(J == Canon<kCls>::s.dp) sum = fma(d, xr, sum);
-    else sum = sum - sp[c + delta];
-}
-
-template <int kCls, int... J>
-__device__ __forceinline__ double canon_row(const double* sp, int c, double d, double xr,
-                                            std::integer_sequence<int, J...>)
-{
-    double sum = 0.0;
-    (canon_step<kCls, J>(sum, sp, c, d, xr), ...);  // slots in ELL order, left to right
-    return sum;
-}
-
-constexpr int kHaloLines = kH64Y * kH64Z;  // 60 lines of 34 points
-
-template <bool kPap>
-__global__ void __launch_bounds__(kT64Threads, 2) k64_spmv_canon(const StencilLevel L, const double* __restrict__ diag,
-                                                                 const double* __restrict__ p,
-                                                                 double* __restrict__ Ap, CGState* st,
-                                                                 double* partial, unsigned int* ticket)
-{
-    __shared__ double s_p[kH64Points];
-    __shared__ double red[32];
-    __shared__ bool last;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tx = (L.nx + kT64X - 1) / kT64X, ty = (L.ny + kT64Y - 1) / kT64Y;
-    const int ntiles = tx * ty * ((L.nz + kT64Z - 1) / kT64Z);
-    const int cls = tid >> 7, i = tid & 127;
-    const int lx = 2 * (i & 15) + ((cls >> 2) & 1);
-    const int ly = 2 * ((i >> 4) & 3) + ((cls >> 1) & 1);
-    const int lz = 2 * (i >> 6) + (cls & 1);
-    const int c = sub_index(lx + 1, ly + 1, lz + 1);
-    const int vown = L.color_of_par[cls];
-
-    // halo line q of this warp = warp + 32 q; lane covers hx = lane and lane + 32
-    double hv[2][2], dv = 0.0;
-    auto load = [&](int tile) {
-        const int bz = tile / (tx * ty), rem = tile - bz * tx * ty, by = rem / tx, bx = rem - by * tx;
-        const int x0 = bx * kT64X, y0 = by * kT64Y, z0 = bz * kT64Z;
-#pragma unroll
-        for(int q = 0; q < 2; ++q)
-        {
-            const int line = warp + 32 * q;
-            hv[q][0] = hv[q][1] = 0.0;
-            if(line >= kHaloLines) continue;
-            const int hy = line % kH64Y, hz = line / kH64Y;
-            const int y = y0 + hy - 1, z = z0 + hz - 1;
-            if(y < 0 || y >= L.ny || z < 0 || z >= L.nz) continue;
-            const int pe = ((y & 1) << 1) | (z & 1);
-            const int ve = L.color_of_par[pe], vo = L.color_of_par[4 | pe];
-            const int be = L.offsets[ve] + ((z >> 1) * L.by[ve] + (y >> 1)) * L.bx[ve];
-            const int bo = L.offsets[vo] + ((z >> 1) * L.by[vo] + (y >> 1)) * L.bx[vo];
-#pragma unroll
-            for(int a = 0; a < 2; ++a)
-            {
-                const int hx = lane + 32 * a;
-                const int x = x0 + hx - 1;
-                if(hx < kH64X && x >= 0 && x < L.nx) hv[q][a] = p[((x & 1) ? bo : be) + (x >> 1)];
-            }
-        }
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        dv = (x < L.nx && y < L.ny && z < L.nz)
-                 ? diag[L.offsets[vown] + ((z >> 1) * L.by[vown] + (y >> 1)) * L.bx[vown] + (x >> 1)]
-                 : 0.0;
-    };
-
-    int tile = blockIdx.x;
-    if(tile < ntiles) load(tile);
-    double s = 0.0;
-    for(; tile < ntiles; tile += gridDim.x)
-    {
-        const int bz = tile / (tx * ty), rem = tile - bz * tx * ty, by = rem / tx, bx = rem - by * tx;
-        const int x = bx * kT64X + lx, y = by * kT64Y + ly, z = bz * kT64Z + lz;
-        __syncthreads();  // previous tile's reads of s_p are done
-#pragma unroll
-        for(int q = 0; q < 2; ++q)
-        {
-            const int line = warp + 32 * q;
-            if(line >= kHaloLines) continue;
-            const int hy = line % kH64Y, hz = line / kH64Y;
-#pragma unroll
-            for(int a = 0; a < 2; ++a)
-                if(lane + 32 * a < kH64X) s_p[sub_index(lane + 32 * a, hy, hz)] = hv[q][a];
-        }
-        const double d = dv;
-        __syncthreads();
-        if(tile + (int)gridDim.x < ntiles) load(tile + gridDim.x);
-        if(x < L.nx && y < L.ny && z < L.nz)
-        {
-            const double xr = s_p[c];
-            double sum;
-            using Seq = std::make_integer_sequence<int, 27>;
-            switch(cls)
-            {
-                case 0: sum = canon_row<0>(s_p, c, d, xr, Seq{}); break;
-                case 1: sum = canon_row<1>(s_p, c, d, xr, Seq{}); break;
-                case 2: sum = canon_row<2>(s_p, c, d, xr, Seq{}); break;
-                case 3: sum = canon_row<3>(s_p, c, d, xr, Seq{}); break;
-                case 4: sum = canon_row<4>(s_p, c, d, xr, Seq{}); break;
-                case 5: sum = canon_row<5>(s_p, c, d, xr, Seq{}); break;
-                case 6: sum = canon_row<6>(s_p, c, d, xr, Seq{}); break;
-                default: sum = canon_row<7>(s_p, c, d, xr, Seq{}); break;
-            }
-            Ap[L.offsets[vown] + ((z >> 1) * L.by[vown] + (y >> 1)) * L.bx[vown] + (x >> 1)] = sum;
-            if(kPap) s = fma(sum, xr, s);
-        }
-    }
-    if(!kPap) return;
-    s = block_sum(s, red);
-    if(tid == 0)
-    {
-        partial[blockIdx.x] = s;
-        __threadfence();
-        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if(!last) return;
-    __threadfence();
-    double acc = 0.0;
-    for(int k = tid; k < (int)gridDim.x; k += kT64Threads) acc += __ldcg(&partial[k]);
-    acc = block_sum(acc, red);
-    if(tid == 0)
-    {
-        *ticket = 0;
-        st->pAp = acc;
-        st->alpha = st->rtz / acc;
-    }
-}
-
 
 // ---- plane march (canonical colouring): a block owns a 64 x 4 column of the
 // grid and walks a chunk of z planes with a ring of four staged planes
