@@ -372,7 +372,8 @@ int hpcgb200_normal_rhs(long long m, unsigned long long seed, double* out, void*
  * followed by coarse_steps - 1 steps x += N(r - A x) (1..64). */
 int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoother* s, int first_level, int coarse_steps);
 /* The learned solve's failure rule: it falls back to SymGS for good after an
- * iteration that multiplies the residual norm by more than `jump` (> 1), after
+ * iteration that multiplies the residual norm by more than `jump` (>= 1; 1 with
+ * the other tests off is "the first iteration that does not reduce it"), after
  * `stall` iterations without a new minimum, with rate > 0 when the norm is above
  * rate times its value `window` iterations earlier, or on a non-finite norm.
  * Defaults: jump 2, stall 16, window 16, rate 0.8 (rate 0 turns that test off). */

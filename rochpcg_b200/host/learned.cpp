@@ -634,8 +634,8 @@ extern "C" int hpcgb200_problem_set_smoother(hpcgb200_problem* p, hpcgb200_smoot
 extern "C" int hpcgb200_problem_set_fallback(hpcgb200_problem* p, double jump, int stall, int window, double rate)
 {
     if(!p || !opt(p->A)) return hb::record_error(HPCGB200_ERR_ARG, "null problem");
-    if(!(jump > 1.0) || stall < 1 || window < 1 || window > 1000 || !(rate >= 0.0))
-        return hb::record_error(HPCGB200_ERR_ARG, "fallback rule: need jump > 1, stall >= 1, 1 <= window <= 1000, "
+    if(!(jump >= 1.0) || stall < 1 || window < 1 || window > 1000 || !(rate >= 0.0))
+        return hb::record_error(HPCGB200_ERR_ARG, "fallback rule: need jump >= 1, stall >= 1, 1 <= window <= 1000, "
                                                   "rate >= 0");
     LevelOpt* o = opt(p->A);
     o->fb_jump = jump;
