@@ -233,6 +233,14 @@ __global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watc
     if(cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, go);
 }
 
+__global__ void k_cg_timer(CGState* st, int phase)
+{
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    if(phase >= 0) st->phase_ns[phase] += (double)(now - st->t_last);
+    st->t_last = now;
+}
+
 __global__ void k_cast_d2f(int n, const double* __restrict__ in, float* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -290,6 +298,13 @@ int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, dou
     k_cg_update_xr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
     HB_LAUNCHED();
     k_cg_loop_control<<<1, 1, 0, s>>>(st, cond, watch_net);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_timer(CGState* st, int phase, cudaStream_t s)
+{
+    k_cg_timer<<<1, 1, 0, s>>>(st, phase);
     HB_LAUNCHED();
     return 0;
 }

@@ -30,7 +30,21 @@ struct CGState
     // monotone, so a single small increase is no failure.
     double fb_jump, fb_rate;
     int fb_stall, fb_window;
+    // phase timers of an instrumented solve (k_cg_timer): nanoseconds spent in
+    // dot products, vector updates, SpMV and MG, and the last time stamp
+    double phase_ns[4];
+    unsigned long long t_last;
     double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
+};
+
+// Phases of an instrumented CG iteration (the reference's times[] slots 1, 2, 3, 5).
+enum CGPhase
+{
+    kPhaseDot = 0,
+    kPhaseWaxpby = 1,
+    kPhaseSpmv = 2,
+    kPhaseMG = 3,
+    kPhaseStart = -1
 };
 
 // Defaults, chosen on the trained smoother (no false fallback at 64^3..256^3
@@ -67,6 +81,11 @@ int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const do
 // normr marks it failed (net = 2); with watch_net the loop then also ends.
 int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
                         CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+
+// One thread: adds the time since the previous stamp to phase_ns[phase]
+// (phase kPhaseStart only stamps).  Kernels on one stream run in order, so
+// the stamps bracket the kernels launched between them.
+int launch_cg_timer(CGState* st, int phase, cudaStream_t s);
 
 // Mixed precision glue: r32 = (float) r and z = (double) z32.
 int launch_cast_d2f(int n, const double* in, float* out, cudaStream_t s);

@@ -345,8 +345,8 @@ extern "C" int hpcgb200_benchmark_report(hpcgb200_benchmark_result* R, char* jso
     J.num("Raw Total B/W", R->gbs_raw);
     J.num("Total with convergence and optimization phase overhead", R->gbs_final);
     J.close();
-    // Per-operator rates need per-operator times; the timed sets run as one
-    // device-resident graph per solve, so only the totals are measured (null).
+    // Per-operator times come from device timers between the operators of the
+    // graph-resident solve (CG_B200 with times); a rate is null when its time is 0.
     J.open("GFLOP/s Summary");
     J.num("Raw DDOT", rate(fnops_ddot, times[1]) / 1e9);
     J.num("Raw WAXPBY", rate(fnops_waxpby, times[2]) / 1e9);

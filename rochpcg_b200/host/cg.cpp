@@ -38,10 +38,15 @@ static void ensure_state(LevelOpt* o, int max_iter)
     o->graphs.clear();
 }
 
+// timed: phase timers around the operators (reference times[] slots: MG,
+// r.z -> dot, p update -> WAXPBY, SpMV with p.Ap -> SpMV, r/x update with
+// ||r|| -> WAXPBY).
 static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool precond, MGPrecision prec,
-                        hb::CGState* st, unsigned long long cond, cudaStream_t s)
+                        hb::CGState* st, unsigned long long cond, cudaStream_t s, bool timed = false)
 {
     const int n = A.localNumberOfRows;
+    auto stamp = [&](int phase) { return timed ? hb::launch_cg_timer(st, phase, s) : 0; };
+    HB_RETURN_IF(stamp(hb::kPhaseStart));
     if(precond)
     {
         if(prec == MGPrecision::FP64) HB_RETURN_IF(ComputeMG(A, data.r, data.z));
@@ -55,8 +60,11 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
             cudaMemcpyAsync(data.z.d_values, data.r.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
         if(e != cudaSuccess) return hb::cuda_error(e, "copy r to z", __FILE__, __LINE__);
     }
+    HB_RETURN_IF(stamp(hb::kPhaseMG));
     HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
+    HB_RETURN_IF(stamp(hb::kPhaseDot));
     HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
+    HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
     if(prec == MGPrecision::FP64_STENCIL)
     {
         // the implicit-stencil product, then p.Ap with the ELL kernel's partition: the FP64 path's scalars
@@ -78,9 +86,13 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
         HB_RETURN_IF(hb::launch_cg_spmv_pap(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, st,
                                             o->spmv_partial, o->spmv_ticket, s));
     }
+    HB_RETURN_IF(stamp(hb::kPhaseSpmv));
     HB_RETURN_IF(hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
                                          data.z.d_values, st, rt().ws, cond, prec == MGPrecision::LEARNED ? 1 : 0,
                                          s));
+    // (the r/x update kernel launches the loop control after itself; its
+    // stamp below also covers that one-thread kernel)
+    HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
     return 0;
 }
 
@@ -100,7 +112,7 @@ static int count_kernel_nodes(cudaGraph_t g)
 }
 
 static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, bool precond,
-                          MGPrecision prec, bool flexible)
+                          MGPrecision prec, bool flexible, bool timed = false)
 {
     LevelOpt* o = opt(A);
     const double* key[6] = {data.r.d_values, data.z.d_values, data.p.d_values, data.Ap.d_values, b.d_values,
@@ -111,7 +123,7 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
     {
         CGGraph* g = it->get();
         if(std::memcmp(g->key, key, sizeof(key)) || g->mode != (int)prec || g->precond != precond ||
-           g->flexible != flexible)
+           g->flexible != flexible || g->timed != timed)
             continue;
         if(g->smoother == sm && g->smoother_epoch == sm_epoch) return g;
         if(g->exec) cudaGraphExecDestroy(g->exec);  // captured other smoother buffers
@@ -125,6 +137,7 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
     G->mode = (int)prec;
     G->precond = precond;
     G->flexible = flexible;
+    G->timed = timed;
     G->smoother = sm;
     G->smoother_epoch = sm_epoch;
     cudaStream_t s = rt().stream;
@@ -149,7 +162,8 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
                 if(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
                    cudaSuccess)
                 {
-                    const int rc = capture_body(A, data, x, precond, prec, o->cg_state, (unsigned long long)h, s);
+                    const int rc =
+                        capture_body(A, data, x, precond, prec, o->cg_state, (unsigned long long)h, s, timed);
                     cudaGraph_t out = nullptr;
                     const cudaError_t e = cudaStreamEndCapture(s, &out);
                     if(rc == 0 && e == cudaSuccess && cudaGraphInstantiate(&G->exec, g, 0) == cudaSuccess)
@@ -173,7 +187,7 @@ static CGGraph* get_graph(const SparseMatrix& A, CGData& data, const Vector& b, 
         // Fallback: one iteration per launch, host checks the condition.
         cudaGraph_t g = nullptr;
         HB_HOST_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        const int rc = capture_body(A, data, x, precond, prec, o->cg_state, 0ULL, s);
+        const int rc = capture_body(A, data, x, precond, prec, o->cg_state, 0ULL, s, timed);
         const cudaError_t e = cudaStreamEndCapture(s, &g);
         if(rc) throw_last(rc);
         HB_HOST_CUDA(e);
@@ -210,8 +224,9 @@ static bool graphs_enabled()
 
 int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,
            double& normr, double& normr0, bool precond, MGPrecision prec, bool flexible, double* hist,
-           double* seconds)
+           double* seconds, double* phase_seconds)
 {
+    const bool timed = phase_seconds != nullptr;
     try
     {
         ensure_runtime();
@@ -275,7 +290,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             {
                 for(int k = h.k; k <= max_iter; ++k)
                 {
-                    check(capture_body(A, data, x, precond, cur, st, 0ULL, s));
+                    check(capture_body(A, data, x, precond, cur, st, 0ULL, s, timed));
                     HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
                     HB_HOST_CUDA(cudaStreamSynchronize(s));
                     if(!(h.normr / h.normr0 > tol) || (cur == MGPrecision::LEARNED && h.net == 2)) break;
@@ -283,7 +298,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             }
             else
             {
-                CGGraph* G = get_graph(A, data, b, x, precond, cur, flexible);
+                CGGraph* G = get_graph(A, data, b, x, precond, cur, flexible, timed);
                 if(G->conditional)
                 {
                     HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
@@ -322,6 +337,8 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         normr = h.normr;
         normr0 = h.normr0;
         if(seconds) *seconds = ms * 1e-3;
+        if(phase_seconds)
+            for(int q = 0; q < 4; ++q) phase_seconds[q] = h.phase_ns[q] * 1e-9;
         return 0;
     }
     catch(const Error& e)
@@ -337,9 +354,18 @@ int CG_B200(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int
             bool flexible, double* normr_hist)
 {
     const auto t0 = std::chrono::steady_clock::now();
+    double phase[4] = {0.0, 0.0, 0.0, 0.0};
     const int rc = run_cg(A, data, b, x, max_iter, tolerance, niters, normr, normr0, doPreconditioning, prec, flexible,
-                          normr_hist, nullptr);
-    if(times) times[0] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                          normr_hist, nullptr, times ? phase : nullptr);
+    if(times)
+    {
+        times[0] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        // src/CG.cpp's slots: 1 dot products, 2 WAXPBY, 3 SpMV, 5 preconditioner
+        times[1] += phase[hb::kPhaseDot];
+        times[2] += phase[hb::kPhaseWaxpby];
+        times[3] += phase[hb::kPhaseSpmv];
+        times[5] += phase[hb::kPhaseMG];
+    }
     return rc;
 }
 

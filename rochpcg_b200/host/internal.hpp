@@ -65,6 +65,7 @@ struct CGGraph
     int mode = -1;
     bool precond = true;
     bool flexible = false;
+    bool timed = false;                // phase timers between the operators
     int kernels_per_iteration = 0;     // kernel nodes of one iteration body
     const void* smoother = nullptr;    // learned mode: smoother and buffer epoch the body captured
     long long smoother_epoch = -1;
@@ -130,8 +131,10 @@ int iteration_kernels(const SparseMatrix& A, CGData& data, const Vector& b, Vect
                       MGPrecision prec, bool flexible);
 
 // Graph-cached solve, defined in cg.cpp.
+// phase_seconds (optional, 4 entries: dot, WAXPBY, SpMV, MG) selects the
+// instrumented iteration body and receives the device time of each phase.
 int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int max_iter, double tol, int& niters,
            double& normr, double& normr0, bool precond, MGPrecision prec, bool flexible, double* hist,
-           double* seconds);
+           double* seconds, double* phase_seconds = nullptr);
 
 }  // namespace hpcg_b200

@@ -52,7 +52,7 @@ def test_report_matches_reference_formulas():
     assert g["Raw Total"] == pytest.approx(ref["raw_gflops"], rel=1e-14)
     assert g["Total with convergence overhead"] == pytest.approx(ref["convergence_gflops"], rel=1e-14)
     assert g["Total with convergence and optimization phase overhead"] == pytest.approx(ref["final_gflops"], rel=1e-14)
-    # per-operator times are not measured (one device-resident graph per solve): null, not infinity
+    # a phase whose time is 0 has no rate: null, not infinity
     assert g["Raw DDOT"] is None and g["Raw MG"] is None
     bw = rep["GB/s Summary"]
     assert bw["Raw Total B/W"] == pytest.approx(ref["raw_gbs"], rel=1e-14)

@@ -130,6 +130,13 @@ def test_protocol_quickpath_valid(n, bound):
     assert rep["Final Summary"]["HPCG result is VALID with a GFLOP/s rating of"] == pytest.approx(res["gflops_final"])
     assert rep["Linear System Information"]["Number of Equations"] == n ** 3
     assert res["times"][0] > 0 and res["times"][7] > 0 and res["times"][8] > 0 and res["times"][9] > 0
+    # phase timers inside the timed sets: every slot measured, their sum within the wall time
+    t = res["times"]
+    assert t[1] > 0 and t[2] > 0 and t[3] > 0 and t[5] > 0
+    assert t[1] + t[2] + t[3] + t[5] <= t[0]
+    assert t[5] > t[3] > 0  # the V-cycle costs more than the SpMV
+    g = rep["GFLOP/s Summary"]
+    assert all(g[k] is not None and g[k] > 0 for k in ("Raw DDOT", "Raw WAXPBY", "Raw SpMV", "Raw MG"))
     if n == 64:
         g = golden("ref_64x64x64.npz")
         assert res["ref_tolerance"] == pytest.approx(float(g["cg50_normr"]) / float(g["cg50_normr0"]), rel=1e-6)
