@@ -215,7 +215,9 @@ typedef struct hpcgb200_problem hpcgb200_problem;
                                    hpcgb200_problem_set_fallback) */
 #define HPCGB200_MODE_FP64_STENCIL 3 /* FP64 as HPCGB200_MODE_FP64, V-cycle and SpMV on the implicit stencil:
                                         the same residual history bit for bit, no matrix reads (needs the
-                                        27-point stencil in parity colouring, like MIXED) */
+                                        27-point stencil in parity colouring on level 0; coarse levels
+                                        without it, or with colour bricks not 4-aligned, use the ELL
+                                        kernels) */
 
 int hpcgb200_problem_create(int nx, int ny, int nz, int nlevels, hpcgb200_problem** out);
 /* flags: HPCGB200_FLAG_KEEP_GENERATED keeps the row-major generated arrays

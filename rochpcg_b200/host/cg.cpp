@@ -264,7 +264,10 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
         if(prec != MGPrecision::FP64)
         {
-            for(const SparseMatrix* M = &A; M; M = M->Ac)
+            // the FP32 V-cycles need the stencil on every level; the FP64 stencil
+            // V-cycle takes the ELL kernels on levels without it, only the outer
+            // SpMV needs it on level 0
+            for(const SparseMatrix* M = &A; M; M = prec == MGPrecision::FP64_STENCIL ? nullptr : M->Ac)
                 if(!opt(*M) || !opt(*M)->stencil_ok)
                     return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
                                             "stencil CG needs the 27-point stencil in parity colouring on every level");
