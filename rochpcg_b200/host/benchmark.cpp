@@ -403,6 +403,25 @@ extern "C" int hpcgb200_benchmark_report(hpcgb200_benchmark_result* R, char* jso
 
 namespace {
 
+// A device vector released on every exit path.
+struct OwnedVector
+{
+    Vector v;
+    explicit OwnedVector(local_int_t n) { CudaInitializeVector(v, n); }
+    ~OwnedVector()
+    {
+        try
+        {
+            CudaDeleteVector(v);
+        }
+        catch(const Error&)
+        {
+        }
+    }
+    OwnedVector(const OwnedVector&) = delete;
+    OwnedVector& operator=(const OwnedVector&) = delete;
+};
+
 struct Hierarchy
 {
     Geometry* geom = nullptr;
@@ -499,22 +518,18 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     const int numberOfCalls = quickPath ? 1 : 10;
     if(verify)
     {
-        Vector x_overlap, b_computed;
-        CudaInitializeVector(x_overlap, H.A.localNumberOfColumns);
-        CudaInitializeVector(b_computed, H.A.localNumberOfRows);
-        CudaFillRandomVector(x_overlap);
+        OwnedVector x_overlap(H.A.localNumberOfColumns), b_computed(H.A.localNumberOfRows);
+        CudaFillRandomVector(x_overlap.v);
         int rc = 0;
         sync();
         t = wall();
         for(int i = 0; i < numberOfCalls && !rc; ++i)
         {
-            rc = ComputeSPMV_ref(H.A, x_overlap, b_computed);
-            if(!rc) rc = ComputeMG_ref(H.A, b_computed, x_overlap);
+            rc = ComputeSPMV_ref(H.A, x_overlap.v, b_computed.v);
+            if(!rc) rc = ComputeMG_ref(H.A, b_computed.v, x_overlap.v);
         }
         sync();
         times[8] = (wall() - t) / numberOfCalls;
-        CudaDeleteVector(x_overlap);
-        CudaDeleteVector(b_computed);
         if(rc) return rc;
     }
 
