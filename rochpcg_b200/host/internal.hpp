@@ -3,6 +3,7 @@
 
 #include <cstdio>
 #include <memory>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -44,6 +45,26 @@ struct Runtime
 };
 Runtime& rt();
 void ensure_runtime();
+
+// Runs f() (which returns a status code) for a C ABI / operator entry point:
+// initialises the runtime and turns a host-layer exception into its code.
+template <typename F>
+int guarded(F&& f)
+{
+    try
+    {
+        ensure_runtime();
+        return f();
+    }
+    catch(const Error& e)
+    {
+        return report(e);
+    }
+    catch(const std::bad_alloc&)
+    {
+        return hb::record_error(HPCGB200_ERR_CUDA, "host allocation failed");
+    }
+}
 
 template <typename T>
 T* dalloc(size_t n)

@@ -302,24 +302,6 @@ struct hpcgb200_smoother
 
 namespace {
 
-template <typename F>
-int guarded(F&& f)
-{
-    try
-    {
-        ensure_runtime();
-        return f();
-    }
-    catch(const Error& e)
-    {
-        return report(e);
-    }
-    catch(const std::bad_alloc&)
-    {
-        return hb::record_error(HPCGB200_ERR_CUDA, "host allocation failed");
-    }
-}
-
 cudaStream_t stream_of(void* s) { return s ? reinterpret_cast<cudaStream_t>(s) : rt().stream; }
 
 // SplitMix64 stream for the initial weights and the batch order.

@@ -9,20 +9,6 @@ using namespace hpcg_b200;
 
 namespace {
 
-template <typename F>
-int guarded(F&& f)
-{
-    try
-    {
-        ensure_runtime();
-        return f();
-    }
-    catch(const Error& e)
-    {
-        return report(e);
-    }
-}
-
 double read_scalar(int slot)
 {
     Runtime& R = rt();

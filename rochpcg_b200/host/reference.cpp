@@ -22,20 +22,6 @@ using namespace hpcg_b200;
 
 namespace {
 
-template <typename F>
-int guarded(F&& f)
-{
-    try
-    {
-        ensure_runtime();
-        return f();
-    }
-    catch(const Error& e)
-    {
-        return report(e);
-    }
-}
-
 hb::NaturalLevel natural(const SparseMatrix& A)
 {
     if(!A.d_mtxIndL || !A.d_matrixValues || !A.d_nonzerosInRow || !A.d_matrixDiagonal)

@@ -44,24 +44,6 @@ bool flexible_of(int mode) { return needs_flexible(prec_of(mode)); }
 // modes TestCG / TestSymmetry run with (the learned V-cycle is not symmetric)
 bool test_mode_ok(int mode) { return mode_ok(mode) && mode != HPCGB200_MODE_LEARNED; }
 
-template <typename F>
-int guarded(F&& f)
-{
-    try
-    {
-        ensure_runtime();
-        return f();
-    }
-    catch(const Error& e)
-    {
-        return report(e);
-    }
-    catch(const std::bad_alloc&)
-    {
-        return hb::record_error(HPCGB200_ERR_CUDA, "host allocation failed");
-    }
-}
-
 SparseMatrix* level_of(const hpcgb200_problem* p, int level)
 {
     if(!p || level < 0 || level >= (int)p->levels.size()) return nullptr;
