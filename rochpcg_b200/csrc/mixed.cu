@@ -13,6 +13,89 @@ namespace hb {
 
 constexpr int kBS32 = 256;
 
+// Slot tables of the colouring the reference's JPL rounds produce (parity
+// class p -> colour 7,2,3,6,5,4,1,0, packed in nibbles, class 0 lowest) as
+// compile-time constants: per ELL slot j of a row of class `cls`, its
+// neighbour offset, the low two bits of its column delta (every other term of
+// the delta is a multiple of 4 when the colour bricks are 4-aligned), the
+// faces that remove it, and the diagonal slot.
+struct KvSlots
+{
+    int dx[27], dy[27], dz[27];
+    int s[27];        // delta & 3
+    unsigned bm[27];  // faces that remove the slot (bit order of StencilTab::bmask)
+    int dp;
+};
+
+__host__ __device__ constexpr int canon_colour(int par) { return (int)((0x01456327u >> (4 * par)) & 15u); }
+
+__host__ __device__ constexpr KvSlots kv_slots(int cls)
+{
+    KvSlots r{};
+    int key[27] = {}, dxs[27] = {}, dys[27] = {}, dzs[27] = {};
+    int k = 0;
+    for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy)
+            for(int dx = -1; dx <= 1; ++dx)
+            {
+                const int col = canon_colour(cls ^ (((dx & 1) << 2) | ((dy & 1) << 1) | (dz & 1)));
+                key[k] = ((col * 3 + (dz + 1)) * 3 + (dy + 1)) * 3 + (dx + 1);
+                dxs[k] = dx;
+                dys[k] = dy;
+                dzs[k] = dz;
+                ++k;
+            }
+    for(int a = 1; a < 27; ++a)
+        for(int b = a; b > 0 && key[b - 1] > key[b]; --b)
+        {
+            int t = key[b]; key[b] = key[b - 1]; key[b - 1] = t;
+            t = dxs[b]; dxs[b] = dxs[b - 1]; dxs[b - 1] = t;
+            t = dys[b]; dys[b] = dys[b - 1]; dys[b - 1] = t;
+            t = dzs[b]; dzs[b] = dzs[b - 1]; dzs[b - 1] = t;
+        }
+    const int px = (cls >> 2) & 1;
+    for(int j = 0; j < 27; ++j)
+    {
+        r.dx[j] = dxs[j];
+        r.dy[j] = dys[j];
+        r.dz[j] = dzs[j];
+        r.s[j] = ((px + dxs[j] + 2) / 2 - 1) & 3;
+        r.bm[j] = (dxs[j] < 0 ? 1u : 0u) | (dxs[j] > 0 ? 2u : 0u) | (dys[j] < 0 ? 4u : 0u) | (dys[j] > 0 ? 8u : 0u) |
+                  (dzs[j] < 0 ? 16u : 0u) | (dzs[j] > 0 ? 32u : 0u);
+        if(dxs[j] == 0 && dys[j] == 0 && dzs[j] == 0) r.dp = j;
+    }
+    return r;
+}
+
+template <int kCls>
+struct KvTab
+{
+    static constexpr KvSlots s = kv_slots(kCls);
+};
+
+// The level's runtime tables agree with the compile-time ones (canonical
+// colouring, 4-aligned bricks): the kernels may use the latter.
+static bool kv_tables_match(const StencilLevel& L)
+{
+    if(!L.even || L.ncolors != 8) return false;
+    for(int v = 0; v < 8; ++v)
+    {
+        if(L.bx[v] % 4 || L.offsets[v] % 4) return false;
+        const int p = L.par[v];
+        if(canon_colour(p) != v) return false;
+        const KvSlots k = kv_slots(p);
+        const StencilTab& T = L.tab[v];
+        if(T.dp != k.dp) return false;
+        for(int j = 0; j < 27; ++j)
+        {
+            const int dx = (int)(T.nb[j] & 3) - 1, dy = (int)((T.nb[j] >> 2) & 3) - 1, dz = (int)((T.nb[j] >> 4) & 3) - 1;
+            if(dx != k.dx[j] || dy != k.dy[j] || dz != k.dz[j]) return false;
+            if((T.delta[j] & 3) != k.s[j] || T.bmask[j] != k.bm[j]) return false;
+        }
+    }
+    return true;
+}
+
 bool make_stencil_level(int nx, int ny, int nz, const int* offsets, const int color_of_par[8], StencilLevel* out)
 {
     StencilLevel L{};
@@ -70,6 +153,7 @@ bool make_stencil_level(int nx, int ny, int nz, const int* offsets, const int co
                                          (dz < 0 ? 16 : 0) | (dz > 0 ? 32 : 0));
         }
     }
+    L.canon = kv_tables_match(L) ? 1 : 0;
     *out = L;
     return true;
 }
@@ -470,9 +554,93 @@ __device__ __forceinline__ void add_slots4(const ColorLaunch& c, const Rows4& b,
     }
 }
 
+// The same slot walk with the canonical colouring's compile-time tables (kCls
+// = the colour's parity class): slot selection, the alignment of each
+// neighbour quad and the face bits are constants, so no slot costs a runtime
+// branch or select; the deltas still come from the launch's table.
+template <int kS, typename T>
+__device__ __forceinline__ void load4s(const T* x, int base, int m, T (&v)[4])
+{
+    if constexpr(kS == 0)
+    {
+        ld4(x, base, m, v);
+    }
+    else
+    {
+        T a[4], b[4];
+        ld4(x, base - kS, m, a);
+        ld4(x, base - kS + 4, m, b);
+#pragma unroll
+        for(int r = 0; r < 4; ++r) v[r] = (kS + r < 4) ? a[kS + r] : b[kS + r - 4];
+    }
+}
+
+template <int kSel, int kCls>
+__host__ __device__ constexpr bool kv_selected(int j)
+{
+    return kSel == kBefore ? j < KvTab<kCls>::s.dp : (kSel == kAfter ? j > KvTab<kCls>::s.dp : j != KvTab<kCls>::s.dp);
+}
+
+template <int kSel, int kCls, int J, typename T>
+__device__ __forceinline__ void kv_load(const ColorLaunch& c, const Rows4& b, const T* x, int m, T (&v)[27][4])
+{
+    if constexpr(J < 27)
+    {
+        if constexpr(kv_selected<kSel, kCls>(J)) load4s<KvTab<kCls>::s.s[J]>(x, b.row0 + c.tb.delta[J], m, v[J]);
+    }
+}
+
+template <int kSel, int kCls, int J, typename T>
+__device__ __forceinline__ void kv_add(const Rows4& b, const T (&v)[27][4], T (&sum)[4])
+{
+    if constexpr(J < 27)
+    {
+        if constexpr(kv_selected<kSel, kCls>(J))
+        {
+            constexpr unsigned bj = KvTab<kCls>::s.bm[J];
+            if(b.fast)
+            {
+#pragma unroll
+                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + v[J][r];
+            }
+            else
+            {
+#pragma unroll
+                for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & bj) ? T(-0.0) : v[J][r]);
+            }
+        }
+    }
+}
+
+template <int kSel, int kCls, int G0, typename T, int... K>
+__device__ __forceinline__ void kv_group(const ColorLaunch& c, const Rows4& b, const T* x, int m, T (&v)[27][4],
+                                         T (&sum)[4], std::integer_sequence<int, K...>)
+{
+    (kv_load<kSel, kCls, G0 + K>(c, b, x, m, v), ...);
+    (kv_add<kSel, kCls, G0 + K>(b, v, sum), ...);
+}
+
+template <int kSel, int kGroup, int kCls, typename T, int... Gs>
+__device__ __forceinline__ void kv_groups(const ColorLaunch& c, const Rows4& b, const T* x, int m, T (&sum)[4],
+                                          std::integer_sequence<int, Gs...>)
+{
+    T v[27][4];
+    (kv_group<kSel, kCls, Gs * kGroup>(c, b, x, m, v, sum, std::make_integer_sequence<int, kGroup>{}), ...);
+}
+
+// add_slots4 for kCls < 0, its compile-time form otherwise.
+template <int kSel, int kGroup, int kCls, typename T>
+__device__ __forceinline__ void add_slots(const ColorLaunch& c, const Rows4& b, const T* x, int m, T (&sum)[4])
+{
+    if constexpr(kCls < 0)
+        add_slots4<kSel, kGroup>(c, b, x, m, sum);
+    else
+        kv_groups<kSel, kGroup, kCls>(c, b, x, m, sum, std::make_integer_sequence<int, (27 + kGroup - 1) / kGroup>{});
+}
+
 // Zero-guess forward sweep of one colour.  FP32 with kFromDouble: r comes in
 // FP64 (the CG residual) and its float copy is stored for the later sweeps.
-template <typename T, bool kFromDouble, int kG>
+template <typename T, bool kFromDouble, int kG, int kCls = -1>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_fwd0(const ColorLaunch c, const StencilLevel L,
                                                        const T* __restrict__ inv_diag, const double* __restrict__ r64,
                                                        T* __restrict__ r, T* x)
@@ -492,7 +660,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_fwd0(const ColorLaunch c, cons
     {
         Quad<T>::load(r + b.row0, sum);
     }
-    if(c.tb.dp > 0) add_slots4<kBefore, kG>(c, b, x, L.m, sum);
+    if(c.tb.dp > 0) add_slots<kBefore, kG, kCls>(c, b, x, L.m, sum);
     T inv[4], out[4];
     Quad<T>::load(inv_diag + b.row0, inv);
 #pragma unroll
@@ -500,7 +668,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_fwd0(const ColorLaunch c, cons
     Quad<T>::store(x + b.row0, out);
 }
 
-template <typename T, int kG>
+template <typename T, int kG, int kCls = -1>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_bwd0(const ColorLaunch c, const StencilLevel L,
                                                        const T* __restrict__ diag, const T* __restrict__ inv_diag, T* x)
 {
@@ -511,7 +679,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_bwd0(const ColorLaunch c, cons
     Quad<T>::load(diag + b.row0, dv);
 #pragma unroll
     for(int q = 0; q < 4; ++q) sum[q] = mul_rn(xv[q], dv[q]);
-    add_slots4<kAfter, kG>(c, b, x, L.m, sum);
+    add_slots<kAfter, kG, kCls>(c, b, x, L.m, sum);
     T inv[4], out[4];
     Quad<T>::load(inv_diag + b.row0, inv);
 #pragma unroll
@@ -520,7 +688,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_bwd0(const ColorLaunch c, cons
 }
 
 // Full sweep of one colour; FP32 with z64: also the FP64 copy of the new x.
-template <typename T, int kG>
+template <typename T, int kG, int kCls = -1>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, const StencilLevel L,
                                                         const T* __restrict__ inv_diag, const T* __restrict__ r, T* x,
                                                         double* __restrict__ z64)
@@ -529,7 +697,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, con
     if(!b.in) return;
     T sum[4];
     Quad<T>::load(r + b.row0, sum);
-    add_slots4<kOff, kG>(c, b, x, L.m, sum);
+    add_slots<kOff, kG, kCls>(c, b, x, L.m, sum);
     T inv[4], out[4];
     Quad<T>::load(inv_diag + b.row0, inv);
 #pragma unroll
@@ -549,7 +717,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, con
 // colour's brick, whose brick-local index is the coarse natural index, so
 // rc[inj_c[row - off]] = (rf - A xf)[row] with the same per-row arithmetic as
 // the ELL restriction (slot order, fma(-a_ii, x_i, .) at the diagonal slot).
-template <typename T, int kG>
+template <typename T, int kG, int kCls = -1>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_restrict(const ColorLaunch c, const StencilLevel L,
                                                            const int* __restrict__ inj_c, const T* __restrict__ diag,
                                                            const T* __restrict__ rf, const T* __restrict__ xf,
@@ -560,13 +728,13 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_restrict(const ColorLaunch c, 
     T sum[4];
     Quad<T>::load(rf + b.row0, sum);
     // slots before the diagonal, fma(-a_ii, x_i, .) at it, slots after it
-    add_slots4<kBefore, kG>(c, b, xf, L.m, sum);
+    add_slots<kBefore, kG, kCls>(c, b, xf, L.m, sum);
     T xv[4], dv[4];
     Quad<T>::load(xf + b.row0, xv);
     Quad<T>::load(diag + b.row0, dv);
 #pragma unroll
     for(int q = 0; q < 4; ++q) sum[q] = fma_rn(-dv[q], xv[q], sum[q]);
-    add_slots4<kAfter, kG>(c, b, xf, L.m, sum);
+    add_slots<kAfter, kG, kCls>(c, b, xf, L.m, sum);
     const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
     rc[ic.x] = sum[0];
     rc[ic.y] = sum[1];
@@ -1058,6 +1226,21 @@ int launch_diag32(int m, const double* diag, float* diag32, float* inv_diag32, c
     return 0;
 }
 
+// Runs the statement with kC = the colour's parity class as a compile-time
+// constant (the canonical-colouring kernels).
+#define HB_CLASS_DISPATCH(par, ...)                  \
+    switch(par)                                      \
+    {                                                \
+        case 0: { constexpr int kC = 0; __VA_ARGS__; } break; \
+        case 1: { constexpr int kC = 1; __VA_ARGS__; } break; \
+        case 2: { constexpr int kC = 2; __VA_ARGS__; } break; \
+        case 3: { constexpr int kC = 3; __VA_ARGS__; } break; \
+        case 4: { constexpr int kC = 4; __VA_ARGS__; } break; \
+        case 5: { constexpr int kC = 5; __VA_ARGS__; } break; \
+        case 6: { constexpr int kC = 6; __VA_ARGS__; } break; \
+        default: { constexpr int kC = 7; __VA_ARGS__; } break; \
+    }
+
 int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float* inv_diag32, const double* r64,
                         float* r32, float* x, cudaStream_t s)
 {
@@ -1074,6 +1257,15 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         {
             if(r64) kv_fwd0<float, true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
             else kv_fwd0<float, false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+        }
+        else if(vec && L.canon)
+        {
+            if(r64)
+                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, true, kV4GroupLarge, kC>
+                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x))
+            else
+                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, false, kV4GroupLarge, kC>
+                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x))
         }
         else if(vec)
         {
@@ -1097,6 +1289,9 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         if(vec && small) kv_bwd0<float, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        else if(vec && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_bwd0<float, kV4GroupLarge, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x))
         else if(vec) kv_bwd0<float, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
         else if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
@@ -1116,6 +1311,9 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
         const ColorLaunch c = color_launch(L, v);
         if(vec && small)
             kv_sweep<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+        else if(vec && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_sweep<float, kV4GroupLarge, kC>
+                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z))
         else if(vec)
             kv_sweep<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
         else if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
@@ -1136,6 +1334,9 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
     const bool vec = vec4_ok(Lf) && nc == c.bx * c.by * c.bz;
     if(vec && Lf.m / 8 < kV4SmallRows)
         kv_restrict<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+    else if(vec && Lf.canon)
+        kv_restrict<float, kV4GroupLarge, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf,
+                                                                                        rc);
     else if(vec)
         kv_restrict<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
     else if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
@@ -1178,6 +1379,9 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
         if(small)
             kv_fwd0<double, false, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
                                                                                 const_cast<double*>(r), x);
+        else if(L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_fwd0<double, false, kV4GroupLarge, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr, const_cast<double*>(r), x))
         else
             kv_fwd0<double, false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
                                                                               const_cast<double*>(r), x);
@@ -1188,6 +1392,9 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         if(small) kv_bwd0<double, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
+        else if(L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_bwd0<double, kV4GroupLarge, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x))
         else kv_bwd0<double, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
         HB_LAUNCHED();
     }
@@ -1204,6 +1411,9 @@ int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double*
         if(small)
             kv_sweep<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
                                                                                         nullptr);
+        else if(L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_sweep<double, kV4GroupLarge, kC>
+                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x, nullptr))
         else
             kv_sweep<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
                                                                                       nullptr);
@@ -1224,6 +1434,9 @@ int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const d
     if(Lf.m / 8 < kV4SmallRows)
         kv_restrict<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
                                                                                        rc);
+    else if(Lf.canon)
+        kv_restrict<double, kV4GroupLarge, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
+                                                                                         rc);
     else
         kv_restrict<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf, rc);
     HB_LAUNCHED();

@@ -43,6 +43,7 @@ struct StencilLevel
     int bx[kMaxStencilColors], by[kMaxStencilColors];
     int par[kMaxStencilColors];           // parity bits (ix&1)<<2 | (iy&1)<<1 | (iz&1) of colour v
     int color_of_par[8];
+    int canon;                 // slot tables equal the compile-time ones of the canonical colouring
     StencilTab tab[kMaxStencilColors];
 };
 
