@@ -1253,7 +1253,16 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const dim3 g = brick_grid(c);
-        if(vec && small)
+        if(vec && small && L.canon)
+        {
+            if(r64)
+                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, true, kV4GroupSmall, kC>
+                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x))
+            else
+                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, false, kV4GroupSmall, kC>
+                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x))
+        }
+        else if(vec && small)
         {
             if(r64) kv_fwd0<float, true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
             else kv_fwd0<float, false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
@@ -1288,7 +1297,10 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(vec && small) kv_bwd0<float, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        if(vec && small && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_bwd0<float, kV4GroupSmall, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x))
+        else if(vec && small) kv_bwd0<float, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
         else if(vec && L.canon)
             HB_CLASS_DISPATCH(c.par, kv_bwd0<float, kV4GroupLarge, kC>
                               <<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x))
@@ -1309,7 +1321,10 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
     auto sweep = [&](int v, double* z) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(vec && small)
+        if(vec && small && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_sweep<float, kV4GroupSmall, kC>
+                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z))
+        else if(vec && small)
             kv_sweep<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
         else if(vec && L.canon)
             HB_CLASS_DISPATCH(c.par, kv_sweep<float, kV4GroupLarge, kC>
@@ -1332,7 +1347,10 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     const bool vec = vec4_ok(Lf) && nc == c.bx * c.by * c.bz;
-    if(vec && Lf.m / 8 < kV4SmallRows)
+    if(vec && Lf.m / 8 < kV4SmallRows && Lf.canon)
+        kv_restrict<float, kV4GroupSmall, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf,
+                                                                                        rc);
+    else if(vec && Lf.m / 8 < kV4SmallRows)
         kv_restrict<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
     else if(vec && Lf.canon)
         kv_restrict<float, kV4GroupLarge, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf,
@@ -1376,7 +1394,10 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(small)
+        if(small && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_fwd0<double, false, kV4GroupSmall64, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr, const_cast<double*>(r), x))
+        else if(small)
             kv_fwd0<double, false, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
                                                                                 const_cast<double*>(r), x);
         else if(L.canon)
@@ -1391,7 +1412,10 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(small) kv_bwd0<double, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
+        if(small && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_bwd0<double, kV4GroupSmall64, kC>
+                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x))
+        else if(small) kv_bwd0<double, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
         else if(L.canon)
             HB_CLASS_DISPATCH(c.par, kv_bwd0<double, kV4GroupLarge, kC>
                               <<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x))
@@ -1408,7 +1432,10 @@ int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double*
     auto sweep = [&](int v) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(small)
+        if(small && L.canon)
+            HB_CLASS_DISPATCH(c.par, kv_sweep<double, kV4GroupSmall64, kC>
+                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x, nullptr))
+        else if(small)
             kv_sweep<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
                                                                                         nullptr);
         else if(L.canon)
@@ -1431,7 +1458,10 @@ int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const d
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
         return record_error(HPCGB200_ERR_ARG, "FP64 stencil restriction: colour bricks not 4-aligned");
-    if(Lf.m / 8 < kV4SmallRows)
+    if(Lf.m / 8 < kV4SmallRows && Lf.canon)
+        kv_restrict<double, kV4GroupSmall64, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
+                                                                                           rc);
+    else if(Lf.m / 8 < kV4SmallRows)
         kv_restrict<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
                                                                                        rc);
     else if(Lf.canon)
