@@ -1022,12 +1022,31 @@ __device__ __forceinline__ double march_row(const double* pm, const double* p0, 
     return sum;
 }
 
-// Colour-permuted row of natural (x, y, z) for the canonical colouring.
-__device__ __forceinline__ int canon_row_of(const StencilLevel& L, int x, int y, int z)
+// Colour-permuted row of natural (x, y, z) for the canonical colouring, as
+// base + (z >> 1) * stride with base and stride fixed per (x, y, z parity).
+struct CanonColumn
 {
-    // kCanonColor packed in nibbles (parity class 0 in the lowest)
-    const int v = (int)((0x01456327u >> (4 * (((x & 1) << 2) | ((y & 1) << 1) | (z & 1)))) & 15u);
-    return L.offsets[v] + ((z >> 1) * L.by[v] + (y >> 1)) * L.bx[v] + (x >> 1);
+    int base[2], stride[2];  // indexed by z parity
+};
+
+__device__ __forceinline__ CanonColumn canon_column(const StencilLevel& L, int x, int y)
+{
+    CanonColumn c;
+#pragma unroll
+    for(int q = 0; q < 2; ++q)
+    {
+        // kCanonColor packed in nibbles (parity class 0 in the lowest)
+        const int v = (int)((0x01456327u >> (4 * (((x & 1) << 2) | ((y & 1) << 1) | q))) & 15u);
+        c.base[q] = L.offsets[v] + (y >> 1) * L.bx[v] + (x >> 1);
+        c.stride[q] = L.by[v] * L.bx[v];
+    }
+    return c;
+}
+
+template <int kQ>
+__device__ __forceinline__ int canon_row(const CanonColumn& c, int z)
+{
+    return c.base[kQ] + (z >> 1) * c.stride[kQ];
 }
 
 template <bool kPap>
@@ -1039,35 +1058,41 @@ __global__ void __launch_bounds__(kMThreads) k64_spmv_march(const StencilLevel L
     __shared__ double red[32];
     __shared__ bool last;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, zb = blockIdx.z * kMZ;
+    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, zb = blockIdx.z * kMZ;  // zb even
     const int ze = zb + kMZ < L.nz ? zb + kMZ : L.nz;
 
-    // this thread's staged positions (fixed for every plane) and whether they exist
-    int hxs[kMLoads], hys[kMLoads];
+    // this thread's staged positions (fixed for every plane), whether they
+    // exist, and their rows as functions of z
+    int slot[kMLoads];
     bool inxy[kMLoads];
+    CanonColumn col[kMLoads];
 #pragma unroll
     for(int k = 0; k < kMLoads; ++k)
     {
         const int e = tid + k * kMThreads;
-        hxs[k] = e % kPX;
-        hys[k] = e / kPX;
-        const int x = x0 + hxs[k] - 1, y = y0 + hys[k] - 1;
+        const int hx = e % kPX, hy = e / kPX;
+        const int x = x0 + hx - 1, y = y0 + hy - 1;
+        slot[k] = e < kPlane ? plane_slot(hx, hy) : -1;
         inxy[k] = e < kPlane && x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+        col[k] = canon_column(L, inxy[k] ? x : 0, inxy[k] ? y : 0);
     }
-    auto load_plane = [&](int z, double (&v)[kMLoads]) {
+    auto load_plane = [&](int z, auto zq, double (&v)[kMLoads]) {
+        constexpr int q = decltype(zq)::value;  // z & 1
 #pragma unroll
         for(int k = 0; k < kMLoads; ++k)
         {
             v[k] = 0.0;
-            if(inxy[k] && z >= 0 && z < L.nz) v[k] = p[canon_row_of(L, x0 + hxs[k] - 1, y0 + hys[k] - 1, z)];
+            if(inxy[k] && z >= 0 && z < L.nz) v[k] = p[canon_row<q>(col[k], z)];
         }
     };
     auto store_plane = [&](int z, const double (&v)[kMLoads]) {
         double* dst = ring[(z + 4) & 3];
 #pragma unroll
         for(int k = 0; k < kMLoads; ++k)
-            if(tid + k * kMThreads < kPlane) dst[plane_slot(hxs[k], hys[k])] = v[k];
+            if(slot[k] >= 0) dst[slot[k]] = v[k];
     };
+    using Q0 = std::integral_constant<int, 0>;
+    using Q1 = std::integral_constant<int, 1>;
 
     // own column: warp -> (x parity, row); lane -> x
     const int px = warp & 1, ly = warp >> 1;
@@ -1075,50 +1100,54 @@ __global__ void __launch_bounds__(kMThreads) k64_spmv_march(const StencilLevel L
     const int x = x0 + lx, y = y0 + ly;
     const bool mine = x < L.nx && y < L.ny;
     const int c = plane_slot(lx + 1, ly + 1);
+    const CanonColumn own = canon_column(L, mine ? x : 0, mine ? y : 0);
 
     double hv[kMLoads];
-    load_plane(zb - 1, hv);
+    load_plane(zb - 1, Q1{}, hv);
     store_plane(zb - 1, hv);
-    load_plane(zb, hv);
+    load_plane(zb, Q0{}, hv);
     store_plane(zb, hv);
-    load_plane(zb + 1, hv);
+    load_plane(zb + 1, Q1{}, hv);
     store_plane(zb + 1, hv);
-    load_plane(zb + 2, hv);
-    double dv = (mine && zb < ze) ? diag[canon_row_of(L, x, y, zb)] : 0.0;
+    load_plane(zb + 2, Q0{}, hv);
+    double dv = (mine && zb < ze) ? diag[canon_row<0>(own, zb)] : 0.0;
     __syncthreads();
     double s = 0.0;
-    for(int z = zb; z < ze; ++z)
-    {
+    // one plane: z & 1 == q
+    auto step = [&](int z, auto zq) {
+        constexpr int q = decltype(zq)::value;
+        using QN = std::integral_constant<int, q ^ 1>;
         store_plane(z + 2, hv);  // ring slot of plane z-2: free since the last step
         const double d = dv;
         if(z + 1 < ze)
         {
-            load_plane(z + 3, hv);
-            dv = mine ? diag[canon_row_of(L, x, y, z + 1)] : 0.0;
+            load_plane(z + 3, QN{}, hv);
+            dv = mine ? diag[canon_row<q ^ 1>(own, z + 1)] : 0.0;
         }
         if(mine)
         {
-            const double* pm = ring[(z + 3) & 3];
-            const double* p0 = ring[(z + 4) & 3];
-            const double* pp = ring[(z + 5) & 3];
-            const double xr = p0[c];
+            const double* pm = ring[(z + 3) & 3] + c;
+            const double* p0 = ring[(z + 4) & 3] + c;
+            const double* pp = ring[(z + 5) & 3] + c;
+            const double xr = *p0;
             double sum;
             using Seq = std::make_integer_sequence<int, 27>;
-            switch((px << 2) | ((ly & 1) << 1) | (z & 1))
+            switch((px << 1) | (ly & 1))
             {
-                case 0: sum = march_row<0>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 1: sum = march_row<1>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 2: sum = march_row<2>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 3: sum = march_row<3>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 4: sum = march_row<4>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 5: sum = march_row<5>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                case 6: sum = march_row<6>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
-                default: sum = march_row<7>(pm + c, p0 + c, pp + c, d, xr, Seq{}); break;
+                case 0: sum = march_row<0 | q>(pm, p0, pp, d, xr, Seq{}); break;
+                case 1: sum = march_row<2 | q>(pm, p0, pp, d, xr, Seq{}); break;
+                case 2: sum = march_row<4 | q>(pm, p0, pp, d, xr, Seq{}); break;
+                default: sum = march_row<6 | q>(pm, p0, pp, d, xr, Seq{}); break;
             }
-            Ap[canon_row_of(L, x, y, z)] = sum;
+            Ap[canon_row<q>(own, z)] = sum;
             if(kPap) s = fma(sum, xr, s);
         }
         __syncthreads();  // plane z+2 stored, plane z-1 no longer read
+    };
+    for(int z = zb; z < ze; z += 2)
+    {
+        step(z, Q0{});
+        if(z + 1 < ze) step(z + 1, Q1{});
     }
     if(!kPap) return;
     s = block_sum(s, red);
