@@ -389,7 +389,8 @@ int hpcgb200_problem_last_fallback(const hpcgb200_problem* p, int* fallback_iter
  * "symgs","symgs_zero","mg","mg_mixed", "symgs32_sweep" (one FP32 implicit
  * colour sweep, averaged over a SymGS step), "spmv_stencil", "mg_learned"
  * (the V-cycle with the attached learned smoother), "mg_stencil" (the FP64
- * V-cycle on the implicit stencil). */
+ * V-cycle on the implicit stencil).  "graph:<op>" captures one call of <op>
+ * into a CUDA graph and times launches of the graph instead. */
 int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int n, double* ms_per_launch);
 
 /* ---------------------------------------------- reference routines (natural order)

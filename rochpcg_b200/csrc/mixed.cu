@@ -5,6 +5,7 @@
 // rounding sequence is exactly the ELL sweep's).
 #include <algorithm>
 #include <array>
+#include <type_traits>
 #include <utility>
 
 #include "mixed.cuh"
@@ -645,6 +646,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_fwd0(const ColorLaunch c, cons
                                                        const T* __restrict__ inv_diag, const double* __restrict__ r64,
                                                        T* __restrict__ r, T* x)
 {
+    pdl_begin();
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
     T sum[4];
@@ -672,6 +674,7 @@ template <typename T, int kG, int kCls = -1>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_bwd0(const ColorLaunch c, const StencilLevel L,
                                                        const T* __restrict__ diag, const T* __restrict__ inv_diag, T* x)
 {
+    pdl_begin();
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
     T xv[4], dv[4], sum[4];
@@ -693,6 +696,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, con
                                                         const T* __restrict__ inv_diag, const T* __restrict__ r, T* x,
                                                         double* __restrict__ z64)
 {
+    pdl_begin();
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
     T sum[4];
@@ -723,6 +727,7 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_restrict(const ColorLaunch c, 
                                                            const T* __restrict__ rf, const T* __restrict__ xf,
                                                            T* __restrict__ rc)
 {
+    pdl_begin();
     const Rows4 b = rows4(c, blockIdx.z);
     if(!b.in) return;
     T sum[4];
@@ -747,6 +752,7 @@ template <typename T>
 __global__ void __launch_bounds__(kV4X * kV4Y) kv_prolong(const ColorLaunch c, const int* __restrict__ inj_c,
                                                           const T* __restrict__ xc, T* __restrict__ xf)
 {
+    pdl_begin();
     const int kx0 = (blockIdx.x * kV4X + threadIdx.x) * 4;
     const int ky = blockIdx.y * kV4Y + threadIdx.y;
     const int kz = blockIdx.z;
@@ -1255,20 +1261,48 @@ int launch_diag32(int m, const double* diag, float* diag32, float* inv_diag32, c
     return 0;
 }
 
-// Runs the statement with kC = the colour's parity class as a compile-time
-// constant (the canonical-colouring kernels).
-#define HB_CLASS_DISPATCH(par, ...)                  \
-    switch(par)                                      \
-    {                                                \
-        case 0: { constexpr int kC = 0; __VA_ARGS__; } break; \
-        case 1: { constexpr int kC = 1; __VA_ARGS__; } break; \
-        case 2: { constexpr int kC = 2; __VA_ARGS__; } break; \
-        case 3: { constexpr int kC = 3; __VA_ARGS__; } break; \
-        case 4: { constexpr int kC = 4; __VA_ARGS__; } break; \
-        case 5: { constexpr int kC = 5; __VA_ARGS__; } break; \
-        case 6: { constexpr int kC = 6; __VA_ARGS__; } break; \
-        default: { constexpr int kC = 7; __VA_ARGS__; } break; \
+// Compile-time parameters of the 4-row kernels: the slot-group size (all
+// slots at once on small levels) and the colour's parity class when the level
+// has the canonical colouring (compile-time slot tables; -1: the launch's
+// runtime tables).
+template <int K>
+using IntC = std::integral_constant<int, K>;
+
+template <typename F>
+cudaError_t by_class(const StencilLevel& L, int par, F&& f)
+{
+    if(!L.canon) return f(IntC<-1>{});
+    switch(par)
+    {
+        case 0: return f(IntC<0>{});
+        case 1: return f(IntC<1>{});
+        case 2: return f(IntC<2>{});
+        case 3: return f(IntC<3>{});
+        case 4: return f(IntC<4>{});
+        case 5: return f(IntC<5>{});
+        case 6: return f(IntC<6>{});
+        default: return f(IntC<7>{});
     }
+}
+
+template <typename T>
+constexpr int kV4GroupSmallOf = std::is_same<T, float>::value ? kV4GroupSmall : kV4GroupSmall64;
+
+// f(group, class) for colour c of level L.
+template <typename T, typename F>
+cudaError_t by_shape(const StencilLevel& L, const ColorLaunch& c, F&& f)
+{
+    if(L.m / 8 < kV4SmallRows) return by_class(L, c.par, [&](auto k) { return f(IntC<kV4GroupSmallOf<T>>{}, k); });
+    return by_class(L, c.par, [&](auto k) { return f(IntC<kV4GroupLarge>{}, k); });
+}
+
+// f(group, class) for the restriction, which runs on the parity-0 colour.
+template <typename T, typename F>
+cudaError_t by_shape_restrict(const StencilLevel& Lf, F&& f)
+{
+    auto cls = [&](auto g) { return Lf.canon ? f(g, IntC<0>{}) : f(g, IntC<-1>{}); };
+    return Lf.m / 8 < kV4SmallRows ? cls(IntC<kV4GroupSmallOf<T>>{}) : cls(IntC<kV4GroupLarge>{});
+}
 
 int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float* inv_diag32, const double* r64,
                         float* r32, float* x, cudaStream_t s)
@@ -1276,39 +1310,20 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     const int n = L.ncolors;
     const dim3 t(32, 8), t4(kV4X, kV4Y);
     const bool vec = vec4_ok(L);
-    const bool small = L.m / 8 < kV4SmallRows;
     for(int v = 0; v < n; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const dim3 g = brick_grid(c);
-        if(vec && small && L.canon)
+        if(vec)
         {
-            if(r64)
-                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, true, kV4GroupSmall, kC>
-                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x))
-            else
-                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, false, kV4GroupSmall, kC>
-                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x))
-        }
-        else if(vec && small)
-        {
-            if(r64) kv_fwd0<float, true, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
-            else kv_fwd0<float, false, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
-        }
-        else if(vec && L.canon)
-        {
-            if(r64)
-                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, true, kV4GroupLarge, kC>
-                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x))
-            else
-                HB_CLASS_DISPATCH(c.par, kv_fwd0<float, false, kV4GroupLarge, kC>
-                                  <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x))
-        }
-        else if(vec)
-        {
-            if(r64) kv_fwd0<float, true, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, r64, r32, x);
-            else kv_fwd0<float, false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag32, nullptr, r32, x);
+            HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
+                constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+                return r64 ? launch_pdl(kv_fwd0<float, true, G, C>, brick_grid4(c), t4, s, c, L, inv_diag32, r64,
+                                        r32, x)
+                           : launch_pdl(kv_fwd0<float, false, G, C>, brick_grid4(c), t4, s, c, L, inv_diag32, nullptr,
+                                        r32, x);
+            }));
         }
         else if(L.even)
         {
@@ -1326,14 +1341,13 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(vec && small && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_bwd0<float, kV4GroupSmall, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x))
-        else if(vec && small) kv_bwd0<float, kV4GroupSmall><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
-        else if(vec && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_bwd0<float, kV4GroupLarge, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x))
-        else if(vec) kv_bwd0<float, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag32, inv_diag32, x);
+        if(vec)
+        {
+            HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
+                constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+                return launch_pdl(kv_bwd0<float, G, C>, brick_grid4(c), t4, s, c, L, diag32, inv_diag32, x);
+            }));
+        }
         else if(L.even) k32_bwd0<true><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         else k32_bwd0<false><<<brick_grid(c), t, 0, s>>>(c, L, diag32, inv_diag32, x);
         HB_LAUNCHED();
@@ -1346,20 +1360,17 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
 {
     const int n = L.ncolors;
     const bool vec = vec4_ok(L);
-    const bool small = L.m / 8 < kV4SmallRows;
     auto sweep = [&](int v, double* z) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(vec && small && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_sweep<float, kV4GroupSmall, kC>
-                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z))
-        else if(vec && small)
-            kv_sweep<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
-        else if(vec && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_sweep<float, kV4GroupLarge, kC>
-                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z))
-        else if(vec)
-            kv_sweep<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag32, r, x, z);
+        if(vec)
+        {
+            HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
+                constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+                return launch_pdl(kv_sweep<float, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, L, inv_diag32, r, x,
+                                  z);
+            }));
+        }
         else if(L.even) k32_sweep<true><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         else k32_sweep<false><<<brick_grid(c), dim3(32, 8), 0, s>>>(c, L, inv_diag32, r, x, z);
         HB_LAUNCHED();
@@ -1375,17 +1386,14 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
                       const float* rf, const float* xf, float* rc, cudaStream_t s)
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
-    const bool vec = vec4_ok(Lf) && nc == c.bx * c.by * c.bz;
-    if(vec && Lf.m / 8 < kV4SmallRows && Lf.canon)
-        kv_restrict<float, kV4GroupSmall, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf,
-                                                                                        rc);
-    else if(vec && Lf.m / 8 < kV4SmallRows)
-        kv_restrict<float, kV4GroupSmall><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
-    else if(vec && Lf.canon)
-        kv_restrict<float, kV4GroupLarge, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf,
-                                                                                        rc);
-    else if(vec)
-        kv_restrict<float, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag32, rf, xf, rc);
+    if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
+    {
+        HB_CUDA(by_shape_restrict<float>(Lf, [&](auto kg, auto kc) {
+            constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+            return launch_pdl(kv_restrict<float, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, Lf, inj_c, diag32, rf,
+                              xf, rc);
+        }));
+    }
     else if(Lf.even) k32_restrict<true><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     else k32_restrict<false><<<nblk(nc), kBS32, 0, s>>>(c, Lf, nc, inj_f, inj_c, diag32, rf, xf, rc);
     HB_LAUNCHED();
@@ -1397,7 +1405,7 @@ int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
-        kv_prolong<float><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
+        HB_CUDA(launch_pdl(kv_prolong<float>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, inj_c, xc, xf));
     else
         k32_prolong<<<nblk(nc), kBS32, 0, s>>>(nc, inj_f, inj_c, xc, xf);
     HB_LAUNCHED();
@@ -1418,38 +1426,24 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
     const dim3 t4(kV4X, kV4Y);
-    const bool small = L.m / 8 < kV4SmallRows;
     for(int v = 0; v < L.ncolors; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(small && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_fwd0<double, false, kV4GroupSmall64, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr, const_cast<double*>(r), x))
-        else if(small)
-            kv_fwd0<double, false, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
-                                                                                const_cast<double*>(r), x);
-        else if(L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_fwd0<double, false, kV4GroupLarge, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr, const_cast<double*>(r), x))
-        else
-            kv_fwd0<double, false, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, inv_diag, nullptr,
-                                                                              const_cast<double*>(r), x);
-        HB_LAUNCHED();
+        HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
+            constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+            return launch_pdl(kv_fwd0<double, false, G, C>, brick_grid4(c), t4, s, c, L, inv_diag, nullptr,
+                              const_cast<double*>(r), x);
+        }));
     }
     for(int v = L.ncolors - 2; v >= 0; --v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(small && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_bwd0<double, kV4GroupSmall64, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x))
-        else if(small) kv_bwd0<double, kV4GroupSmall64><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
-        else if(L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_bwd0<double, kV4GroupLarge, kC>
-                              <<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x))
-        else kv_bwd0<double, kV4GroupLarge><<<brick_grid4(c), t4, 0, s>>>(c, L, diag, inv_diag, x);
-        HB_LAUNCHED();
+        HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
+            constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+            return launch_pdl(kv_bwd0<double, G, C>, brick_grid4(c), t4, s, c, L, diag, inv_diag, x);
+        }));
     }
     return 0;
 }
@@ -1457,23 +1451,14 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
 int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double* r, double* x, cudaStream_t s)
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
-    const bool small = L.m / 8 < kV4SmallRows;
     auto sweep = [&](int v) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(small && L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_sweep<double, kV4GroupSmall64, kC>
-                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x, nullptr))
-        else if(small)
-            kv_sweep<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
-                                                                                        nullptr);
-        else if(L.canon)
-            HB_CLASS_DISPATCH(c.par, kv_sweep<double, kV4GroupLarge, kC>
-                              <<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x, nullptr))
-        else
-            kv_sweep<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, L, inv_diag, r, x,
-                                                                                      nullptr);
-        HB_LAUNCHED();
+        HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
+            constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+            return launch_pdl(kv_sweep<double, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, L, inv_diag, r, x,
+                              nullptr);
+        }));
         return 0;
     };
     for(int v = 0; v < L.ncolors; ++v) HB_RETURN_IF(sweep(v));
@@ -1487,18 +1472,11 @@ int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const d
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
         return record_error(HPCGB200_ERR_ARG, "FP64 stencil restriction: colour bricks not 4-aligned");
-    if(Lf.m / 8 < kV4SmallRows && Lf.canon)
-        kv_restrict<double, kV4GroupSmall64, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
-                                                                                           rc);
-    else if(Lf.m / 8 < kV4SmallRows)
-        kv_restrict<double, kV4GroupSmall64><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
-                                                                                       rc);
-    else if(Lf.canon)
-        kv_restrict<double, kV4GroupLarge, 0><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf,
-                                                                                         rc);
-    else
-        kv_restrict<double, kV4GroupLarge><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, Lf, inj_c, diag, rf, xf, rc);
-    HB_LAUNCHED();
+    HB_CUDA(by_shape_restrict<double>(Lf, [&](auto kg, auto kc) {
+        constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
+        return launch_pdl(kv_restrict<double, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, Lf, inj_c, diag, rf, xf,
+                          rc);
+    }));
     return 0;
 }
 
@@ -1507,8 +1485,7 @@ int launch64v_prolong(const StencilLevel& Lf, int nc, const int* inj_c, const do
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
         return record_error(HPCGB200_ERR_ARG, "FP64 stencil prolongation: colour bricks not 4-aligned");
-    kv_prolong<double><<<brick_grid4(c), dim3(kV4X, kV4Y), 0, s>>>(c, inj_c, xc, xf);
-    HB_LAUNCHED();
+    HB_CUDA(launch_pdl(kv_prolong<double>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, inj_c, xc, xf));
     return 0;
 }
 

@@ -523,7 +523,11 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
 {
     if(!p || !op || n < 1 || !ms_per_launch) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
     return guarded([&] {
-        const std::string o(op);
+        // "graph:<op>" captures one call of <op> into a CUDA graph and times
+        // launches of that graph (the way the solver runs it)
+        std::string o(op);
+        const bool as_graph = o.rfind("graph:", 0) == 0;
+        if(as_graph) o = o.substr(6);
         SparseMatrix& A = p->A;
         cudaStream_t s = rt().stream;
         Vector& r = p->data.r;
@@ -559,6 +563,29 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
             }
         }
         else return hb::record_error(HPCGB200_ERR_ARG, "unknown op '%s'", op);
+        struct GraphGuard
+        {
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            ~GraphGuard()
+            {
+                if(exec) cudaGraphExecDestroy(exec);
+                if(g) cudaGraphDestroy(g);
+            }
+        } gg;
+        if(as_graph)
+        {
+            HB_HOST_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            const int rc = f();
+            const cudaError_t e = cudaStreamEndCapture(s, &gg.g);
+            HB_RETURN_IF(rc);
+            HB_HOST_CUDA(e);
+            HB_HOST_CUDA(cudaGraphInstantiate(&gg.exec, gg.g, 0));
+            f = [&] {
+                HB_CUDA(cudaGraphLaunch(gg.exec, s));
+                return 0;
+            };
+        }
         HB_RETURN_IF(f());  // warm-up
         cudaEvent_t e0, e1;
         HB_HOST_CUDA(cudaEventCreate(&e0));

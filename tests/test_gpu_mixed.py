@@ -74,3 +74,26 @@ def test_stencil_spmv_equals_ell_spmv_bitwise(dims):
         sync(P)
         assert torch.equal(y1, y2)
         assert np.array_equal(host(y2), O.levels[l].spmv(x))
+
+
+@pytest.mark.parametrize("mode_name", ["MODE_MIXED", "MODE_FP64_STENCIL"])
+def test_direct_launches_equal_graph(mode_name, monkeypatch):
+    """The solve as one graph (kernels back to back, no programmatic launch)
+    and as direct launches (the 4-row kernels with programmatic dependent
+    launch, a host check per iteration) give the same residual history bit
+    for bit; the graph form of the V-cycle times like the direct one."""
+    import rochpcg_b200 as R
+
+    mode = getattr(R, mode_name)
+    P = R.Problem(48, 40, 56)
+    g = P.cg(40, 0.0, mode=mode)
+    monkeypatch.setenv("HPCGB200_GRAPH", "0")
+    d = P.cg(40, 0.0, mode=mode)
+    monkeypatch.delenv("HPCGB200_GRAPH")
+    assert g["niters"] == d["niters"] == 40
+    assert np.array_equal(g["hist"], d["hist"])
+    op = "mg_mixed" if mode == R.MODE_MIXED else "mg_stencil"
+    assert P.time_op("graph:" + op, 2) > 0 and P.time_op(op, 2) > 0
+    with pytest.raises(R.HpcgError):
+        P.time_op("graph:no_such_op", 1)
+    P.close()
