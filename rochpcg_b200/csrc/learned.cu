@@ -57,6 +57,15 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
+// Descriptor of a K-major operand with 32-byte rows (K = 16 BF16) in the
+// 32-byte swizzle (layout type 6): 8-row groups 256 B apart (SBO), the two
+// 16-byte halves of a row 16 B apart (LBO).  Start addresses must keep the
+// 256-byte atom phase (base offset 0).
+__device__ __forceinline__ uint64_t umma_desc_sw32(uint32_t saddr)
+{
+    return umma_desc(saddr, 16, 256) | ((uint64_t)6 << 61);
+}
+
 // Instruction descriptor of kind::f16: BF16 x BF16 -> FP32, M x N.
 __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N, bool a_mn_major, bool b_mn_major)
 {
@@ -184,9 +193,10 @@ __host__ __device__ constexpr int weight_slot(int t) { return (t % 9) * 3 + 2 - 
 // ------------------------------------------------------------ forward conv
 //
 // Warp-specialised persistent kernel, one CTA per SM:
-//   warp 0      TMA producer: for each brick, six tiled loads (three dx
-//               shifts x two 8-channel halves) of the halo'd brick into one of
-//               kStages shared-memory stages (zero fill outside the grid);
+//   warp 0      TMA producer: for each brick, three tiled loads (one per dx
+//               shift, 32-byte rows of 16 channels in the 32-byte swizzle) of
+//               the halo'd brick into one of kStages shared-memory stages
+//               (zero fill outside the grid);
 //   warp 1      allocates TMEM and issues the brick's tcgen05.mma into one of
 //               two TMEM accumulators: for each staged input plane q and
 //               in-plane tap (dy, dx), ONE MMA with N = 16 x (number of output
@@ -211,8 +221,8 @@ __host__ __device__ constexpr int weight_slot(int t) { return (t % 9) * 3 + 2 - 
 constexpr int kTX = 16, kTY = 8, kTZ = HB_CONV_TZ;
 constexpr int kHY = kTY + 2, kHZ = kTZ + 2;
 constexpr int kCopyRows = kTX * kHY * kHZ;            // 960 rows per shifted copy
-constexpr int kRegion = kCopyRows * 16;               // one 8-channel half: 15360 B = one TMA box (the K-major LBO)
-constexpr int kCopyBytes = 2 * kRegion;
+constexpr int kRowBytes = kNetCh * 2;                 // the 16 BF16 channels of a point: one 32-byte swizzle row
+constexpr int kCopyBytes = kCopyRows * kRowBytes;     // 30720 B = one TMA box
 constexpr int kStageBytes = 3 * kCopyBytes;           // 92160 B
 constexpr int kStages = HB_CONV_STAGES;
 constexpr int kAccCols = kTZ * 16;                    // FP32 columns of one brick's accumulator
@@ -221,9 +231,9 @@ constexpr int kConvThreads = 192;
 constexpr int kEpiThreads = 128;
 constexpr int kConvSmem = kStages * kStageBytes + kNetWeightTileBytes + 256 + 1024;
 
-static_assert((kRegion >> 4) < (1 << 14), "LBO field");
+static_assert(kRowBytes == 32, "one point per 32-byte swizzle row (K = 16 per MMA)");
 static_assert(kTX * kTY == 128, "one z plane of the brick is one 128-row M tile");
-static_assert(kStageBytes % 1024 == 0 && kRegion % 128 == 0, "stage alignment");
+static_assert(kStageBytes % 1024 == 0 && kCopyBytes % 1024 == 0, "stages and copies start on swizzle-atom boundaries");
 static_assert(kConvSmem <= 227 * 1024, "shared memory per CTA");
 
 struct Brick
@@ -347,14 +357,11 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             const uint32_t ph = (uint32_t)((issued / kStages) & 1);
             if(!role_wait(&empty[st], ph ^ 1u, abort_flag, status, 3)) break;
             const Brick bk = brick_of(g, tile, tx, ty, per_sample);
-            mbar_expect_tx(&full[st], 6u * kRegion);
+            mbar_expect_tx(&full[st], 3u * kCopyBytes);
             unsigned char* dst = sA + st * kStageBytes;
 #pragma unroll
             for(int dxi = 0; dxi < 3; ++dxi)
-#pragma unroll
-                for(int c8 = 0; c8 < 2; ++c8)
-                    tma_load_5d(dst + dxi * kCopyBytes + c8 * kRegion, &in_map, c8 * 8, bk.x0 + dxi - 1, bk.y0 - 1,
-                                bk.z0 - 1, bk.b, &full[st]);
+                tma_load_5d(dst + dxi * kCopyBytes, &in_map, 0, bk.x0 + dxi - 1, bk.y0 - 1, bk.z0 - 1, bk.b, &full[st]);
         }
         if(*abort_flag)
         {
@@ -392,7 +399,7 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             tc_fence_after();
             // descriptors = base + compile-time offset (the 14-bit start field
             // holds address / 16 and stays below 2^14 for any smem address)
-            const uint64_t ad0 = umma_desc(smem_u32(sA + st * kStageBytes), kRegion, 128);
+            const uint64_t ad0 = umma_desc_sw32(smem_u32(sA + st * kStageBytes));
             const uint32_t d0 = tmem + (uint32_t)(acc * kAccCols);
             // staged plane q (z = z0 - 1 + q) feeds output planes mt = q - 1 - dz
             // in [lo, hi]; group mt takes B tile j = mt - q + 2 of the (dy, dx)
@@ -408,7 +415,7 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
                 {
                     const int dy = sxy / 3 - 1, dx = sxy % 3 - 1;
                     const int row0 = (q * kHY + (dy + 1)) * kTX;
-                    const uint64_t ad = ad0 + (uint64_t)(((dx + 1) * kCopyBytes + row0 * 16) >> 4);
+                    const uint64_t ad = ad0 + (uint64_t)(((dx + 1) * kCopyBytes + row0 * kRowBytes) >> 4);
                     const uint64_t bs = bd0 + (uint64_t)((sxy * 3 * 512) >> 4);
                     if(q <= kTZ - 1 && sxy == 0)
                     {
@@ -1099,8 +1106,9 @@ static int sm_count()
 }
 
 // Tensor map of a channel-last BF16 tensor [nb][nz][ny][nx][16] with the
-// brick box (8 channels, 16 x 10 x 6 points, 1 sample); the driver entry
-// point is looked up once through the runtime.
+// brick box (16 channels, 16 x 10 x 6 points, 1 sample) written in the 32-byte
+// swizzle that the A descriptors declare; the driver entry point is looked up
+// once through the runtime.
 static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -1117,10 +1125,10 @@ static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
                                 (cuuint64_t)g.nb};
     const cuuint64_t row = (cuuint64_t)kNetCh * 2;
     const cuuint64_t strides[4] = {row, row * g.nx, row * g.nx * g.ny, row * g.nx * g.ny * g.nz};
-    const cuuint32_t box[5] = {8, (cuuint32_t)kTX, (cuuint32_t)kHY, (cuuint32_t)kHZ, 1};
+    const cuuint32_t box[5] = {(cuuint32_t)kNetCh, (cuuint32_t)kTX, (cuuint32_t)kHY, (cuuint32_t)kHZ, 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(in), dims, strides, box,
-                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if(r != CUDA_SUCCESS) return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return 0;
