@@ -520,6 +520,253 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
     if(warp == 1) tmem_free(tmem, kTmemCols);
 }
 
+// ------------------------------------------------------------ layer 3 (16 -> 1)
+//
+// One output channel: the 27 taps are stacked in N instead of the input being
+// shifted.  For each staged input point p, ONE MMA row computes
+// D[p][t] = sum_c a2[p][c] w3[t][c] for all taps t (M = 128 points, N = 32,
+// K = 16), and the output is y[o] = sum_t D[o + off_t][t], gathered by the
+// epilogue from shared memory in tap order (deterministic, no atomics).  In
+// the odd evaluation the pair is folded into K: the branch of -r is a second
+// MMA into the same accumulator with the weights negated, both halved, so D
+// already holds (y(r) - y(-r)) / 2.
+//   warp 0      TMA producer: per brick one (two with the pair) box of the
+//               halo'd input, 18 x 10 x 4 points of 16 channels, 32-byte
+//               swizzled rows, zero fill outside the grid;
+//   warp 1      TMEM owner and MMA issuer: 6 MMAs (12 with the pair) per brick
+//               into one of two accumulators of 6 x 32 columns;
+//   warps 2-5   epilogue: TMEM -> shared memory (27 floats per staged point),
+//               then the 27-tap gather for the brick's 16 x 8 x 2 outputs.
+constexpr int k3X = 16, k3Y = 8, k3Z = 2;                       // output brick
+constexpr int k3HX = k3X + 2, k3HY = k3Y + 2, k3HZ = k3Z + 2;  // staged box 18 x 10 x 4
+constexpr int k3Rows = k3HX * k3HY * k3HZ;                      // 720 staged points
+constexpr int k3Chunks = (k3Rows + 127) / 128;                  // 6 M tiles per box
+constexpr int k3BoxBytes = k3Chunks * 128 * kRowBytes;          // 24 KB (the TMA fills the first 720 rows)
+constexpr int k3StageBytes = 2 * k3BoxBytes;                    // the two branches of the pair
+constexpr int k3Stages = 2;
+constexpr int k3N = 32;                                         // 27 taps + 5 zero columns
+constexpr int k3AccCols = k3Chunks * k3N;                       // 192 TMEM columns per brick
+constexpr int k3TmemCols = 512;                                 // two accumulators, power of two
+constexpr int k3DStride = 27;                                   // floats per staged point (odd: no bank conflicts)
+constexpr int k3WTileBytes = k3N * kRowBytes;                   // 32 tap rows x 16 channels, K-major
+constexpr int k3Outputs = k3X * k3Y * k3Z;                      // 256 per brick
+constexpr int k3Smem = k3Stages * k3StageBytes + 2 * k3WTileBytes + k3Rows * k3DStride * 4 + 256 + 1024;
+
+static_assert(k3BoxBytes % 1024 == 0 && k3Rows * kRowBytes <= k3BoxBytes, "layer-3 box");
+static_assert(k3Outputs % kEpiThreads == 0, "whole outputs per epilogue thread");
+static_assert(k3Smem <= 227 * 1024, "shared memory per CTA");
+
+// Named barrier 1 of the four epilogue warps (the non-aligned forms: lanes
+// may arrive apart); the OR reduction makes a give-up decision of any one
+// thread the decision of all, so they take the same barriers.
+__device__ __forceinline__ bool epi_any(bool pred)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "barrier.red.or.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t"
+        "}\n"
+        : "=r"(r)
+        : "r"(pred ? 1u : 0u)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void epi_sync() { asm volatile("barrier.sync 1, 128;" ::: "memory"); }
+
+template <int kOut, bool kPair>
+__global__ void __launch_bounds__(kConvThreads, 1)
+    k_layer3_tc(const __grid_constant__ CUtensorMap in_map, ConvGrid g, const float* __restrict__ w3, float* out,
+                PermMap pm, int* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sA = smem;                                       // k3Stages x k3StageBytes
+    unsigned char* sW = smem + k3Stages * k3StageBytes;             // + and - weight tiles
+    float* sD = (float*)(sW + 2 * k3WTileBytes);                    // k3Rows x k3DStride
+    uint64_t* full = (uint64_t*)(sD + k3Rows * k3DStride);
+    uint64_t* empty = full + k3Stages;
+    uint64_t* tfull = empty + k3Stages;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tholder = (uint32_t*)(tempty + 2);
+    volatile int* abort_flag = (volatile int*)(tholder + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int tx = (g.nx + k3X - 1) / k3X, ty = (g.ny + k3Y - 1) / k3Y, tz = (g.nz + k3Z - 1) / k3Z;
+    const long per_sample = (long)tx * ty * tz;
+    const long ntiles = per_sample * g.nb;
+
+    // weight tiles: row t = tap, 16 channels; the bf16 weight, halved and
+    // negated for the pair (exact in bf16)
+    for(int i = tid; i < k3N * kNetCh; i += kConvThreads)
+    {
+        const int t = i / kNetCh, c = i % kNetCh;
+        float w = t < 27 ? __bfloat162float(__float2bfloat16_rn(w3[(t * kNetCh + c) * kNetCh])) : 0.f;
+        if(kPair) w *= 0.5f;
+        const uint32_t off = kmajor_off(t, c >> 3) + (uint32_t)(c & 7) * 2;
+        *reinterpret_cast<__nv_bfloat16*>(sW + off) = __float2bfloat16_rn(w);
+        *reinterpret_cast<__nv_bfloat16*>(sW + k3WTileBytes + off) = __float2bfloat16_rn(-w);
+    }
+    if(tid == 0)
+    {
+        for(int s = 0; s < k3Stages; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for(int a = 0; a < 2; ++a)
+        {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], kEpiThreads);
+        }
+        *abort_flag = 0;
+    }
+    if(warp == 1) tmem_alloc(tholder, k3TmemCols);
+    fence_async_smem();  // the weights are read by the tensor cores
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tholder;
+    constexpr uint32_t kBoxTx = (uint32_t)(k3Rows * kRowBytes) * (kPair ? 2u : 1u);
+
+    if(warp == 0 && lane == 0)
+    {
+        // ---- TMA producer
+        long issued = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++issued)
+        {
+            const int st = (int)(issued % k3Stages);
+            const uint32_t ph = (uint32_t)((issued / k3Stages) & 1);
+            if(!role_wait(&empty[st], ph ^ 1u, abort_flag, status, 3)) break;
+            const int b = (int)(tile / per_sample);
+            long t2 = tile - (long)b * per_sample;
+            const int bz = (int)(t2 / ((long)tx * ty));
+            t2 -= (long)bz * tx * ty;
+            const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
+            mbar_expect_tx(&full[st], kBoxTx);
+            unsigned char* dst = sA + st * k3StageBytes;
+            tma_load_5d(dst, &in_map, 0, bx * k3X - 1, by * k3Y - 1, bz * k3Z - 1, b, &full[st]);
+            if(kPair)
+                tma_load_5d(dst + k3BoxBytes, &in_map, 0, bx * k3X - 1, by * k3Y - 1, bz * k3Z - 1, b + g.nb,
+                            &full[st]);
+        }
+        if(*abort_flag)
+        {
+            // let the loads already issued land before the CTA's shared memory goes away
+            for(long k = issued - k3Stages < 0 ? 0 : issued - k3Stages; k < issued; ++k)
+                mbar_wait(&full[k % k3Stages], (uint32_t)((k / k3Stages) & 1));
+        }
+    }
+    else if(warp == 1 && lane == 0)
+    {
+        // ---- MMA issuer
+        constexpr uint32_t idesc = umma_idesc_bf16(128, k3N, false, false);
+        const uint64_t bpos = umma_desc(smem_u32(sW), 128, 256);
+        const uint64_t bneg = umma_desc(smem_u32(sW + k3WTileBytes), 128, 256);
+        long i = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
+        {
+            const int st = (int)(i % k3Stages);
+            const uint32_t ph = (uint32_t)((i / k3Stages) & 1);
+            const int acc = (int)(i & 1);
+            const uint32_t aph = (uint32_t)((i >> 1) & 1);
+            if(!role_wait(&tempty[acc], aph ^ 1u, abort_flag, status, 4)) break;
+            if(!role_wait(&full[st], ph, abort_flag, status, 5)) break;
+            tc_fence_after();
+            const uint64_t a0 = umma_desc_sw32(smem_u32(sA + st * k3StageBytes));
+            const uint32_t d0 = tmem + (uint32_t)(acc * k3AccCols);
+#pragma unroll
+            for(int c = 0; c < k3Chunks; ++c)
+            {
+                const uint64_t ac = a0 + (uint64_t)((c * 128 * kRowBytes) >> 4);
+                mma_bf16(d0 + c * k3N, ac, bpos, idesc, 0u);
+                if(kPair) mma_bf16(d0 + c * k3N, ac + (uint64_t)(k3BoxBytes >> 4), bneg, idesc, 1u);
+            }
+            mma_commit(&empty[st]);   // stage free once these MMAs have read it
+            mma_commit(&tfull[acc]);  // accumulator ready for the epilogue
+        }
+        if(*abort_flag && i > 0)
+        {
+            // MMAs in flight must finish before TMEM is released
+            const long k = i - 1;
+            mbar_wait(&tfull[k & 1], (uint32_t)((k >> 1) & 1));
+        }
+    }
+    else if(warp >= 2)
+    {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        const int qd = warp & 3;
+        const int et = tid - 64;  // 0 .. 127
+        long i = 0;
+        for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
+        {
+            const int acc = (int)(i & 1);
+            const uint32_t aph = (uint32_t)((i >> 1) & 1);
+            const bool ok = role_wait(&tfull[acc], aph, abort_flag, status, 6);
+            if(epi_any(!ok)) break;
+            __syncwarp();  // tcgen05.ld is warp-collective
+            tc_fence_after();
+#pragma unroll 1
+            for(int c = 0; c < k3Chunks; ++c)
+            {
+                float v[32];
+                const uint32_t ta = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(acc * k3AccCols + c * k3N);
+                tmem_ld16(ta, *reinterpret_cast<float(*)[16]>(v));
+                tmem_ld16(ta + 16, *reinterpret_cast<float(*)[16]>(v + 16));
+                const int row = c * 128 + qd * 32 + lane;
+                if(row < k3Rows)
+                {
+#pragma unroll
+                    for(int t = 0; t < 27; ++t) sD[row * k3DStride + t] = v[t];
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);  // the accumulator may take the next brick
+            epi_sync();                 // every staged point's taps are in shared memory
+            const int b = (int)(tile / per_sample);
+            long t2 = tile - (long)b * per_sample;
+            const int bz = (int)(t2 / ((long)tx * ty));
+            t2 -= (long)bz * tx * ty;
+            const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
+#pragma unroll
+            for(int k = 0; k < k3Outputs / kEpiThreads; ++k)
+            {
+                const int o = et + k * kEpiThreads;
+                const int ox = o % k3X, oy = (o / k3X) % k3Y, oz = o / (k3X * k3Y);
+                const int x = bx * k3X + ox, y = by * k3Y + oy, z = bz * k3Z + oz;
+                if(x >= g.nx || y >= g.ny || z >= g.nz) continue;
+                float sum = 0.f;
+#pragma unroll
+                for(int t = 0; t < 27; ++t)
+                {
+                    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                    const int r = ((oz + 1 + dz) * k3HY + (oy + 1 + dy)) * k3HX + (ox + 1 + dx);
+                    sum += sD[r * k3DStride + t];
+                }
+                if constexpr(kOut == 2)
+                {
+                    out[(((long)b * g.nz + z) * g.ny + y) * g.nx + x] = sum;
+                }
+                else
+                {
+                    float* xo = out + perm_row(pm, z, y, x);
+                    if constexpr(kOut == 1) *xo += sum;
+                    else *xo = sum;
+                }
+            }
+            epi_sync();  // shared memory free for the next brick
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if(warp == 1) tmem_free(tmem, k3TmemCols);
+}
+
 // ------------------------------------------------------------ weight gradient
 
 constexpr int kWgK = 64;                  // points per K block
@@ -914,71 +1161,6 @@ __global__ void __launch_bounds__(256) k_layer1_direct(ConvGrid g, const Tin* __
     }
 }
 
-__device__ __forceinline__ float dot16(const __nv_bfloat16* a, const float* w)
-{
-    const uint4 u0 = *reinterpret_cast<const uint4*>(a);
-    const uint4 u1 = *reinterpret_cast<const uint4*>(a + 8);
-    const __nv_bfloat162* h0 = reinterpret_cast<const __nv_bfloat162*>(&u0);
-    const __nv_bfloat162* h1 = reinterpret_cast<const __nv_bfloat162*>(&u1);
-    float s = 0.f;
-#pragma unroll
-    for(int i = 0; i < 4; ++i)
-    {
-        const float2 f = __bfloat1622float2(h0[i]);
-        s = fmaf(f.x, w[2 * i], s);
-        s = fmaf(f.y, w[2 * i + 1], s);
-    }
-#pragma unroll
-    for(int i = 0; i < 4; ++i)
-    {
-        const float2 f = __bfloat1622float2(h1[i]);
-        s = fmaf(f.x, w[8 + 2 * i], s);
-        s = fmaf(f.y, w[8 + 2 * i + 1], s);
-    }
-    return s;
-}
-
-// Layer 3 output channel 0: y_b[p] = sum_t sum_ci w3[t][ci][0] a2_b[p + t][ci];
-// v = (y_0 - y_1) / 2 with kPair, y_0 otherwise.  kOut 0: x[row(p)] = v,
-// 1: x[row(p)] += v (a level vector through pm, one sample), 2: out[p] = v
-// (natural order, nb samples).
-template <bool kPair, int kOut>
-__global__ void __launch_bounds__(256) k_layer3_direct(ConvGrid g, PermMap pm, const __nv_bfloat16* __restrict__ a2,
-                                                       const float* __restrict__ w3, float* __restrict__ out)
-{
-    __shared__ float w[27 * kNetCh];
-    for(int i = threadIdx.x; i < 27 * kNetCh; i += blockDim.x)
-        w[i] = __bfloat162float(__float2bfloat16_rn(w3[i * kNetCh]));  // w3[t][ci][0]
-    __syncthreads();
-    const long n = g.points();
-    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if(p >= n) return;
-    const long per = (long)g.nz * g.ny * g.nx;
-    const long base = (p / per) * per;
-    const long q0 = p - base;
-    const int z = (int)(q0 / ((long)g.ny * g.nx));
-    const long rem = q0 - (long)z * g.ny * g.nx;
-    const int y = (int)(rem / g.nx), x = (int)(rem - (long)y * g.nx);
-    float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-    for(int t = 0; t < 27; ++t)
-    {
-        const int zz = z + t / 9 - 1, yy = y + (t / 3) % 3 - 1, xx = x + t % 3 - 1;
-        if(zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) continue;
-        const long q = base + ((long)zz * g.ny + yy) * g.nx + xx;
-        y0 += dot16(a2 + q * kNetCh, w + t * kNetCh);
-        if(kPair) y1 += dot16(a2 + (q + n) * kNetCh, w + t * kNetCh);
-    }
-    const float v = kPair ? 0.5f * (y0 - y1) : y0;
-    if(kOut == 2) out[p] = v;
-    else
-    {
-        float* o = out + perm_row(pm, z, y, x);
-        if(kOut == 1) *o += v;
-        else *o = v;
-    }
-}
-
 // 1 / (e.e) (kind 0) or 1 / (e.Ae) (kind 1) per sample: one block per sample.
 __global__ void k_sample_norm(ConvGrid g, const float* __restrict__ e, int kind, float* __restrict__ out)
 {
@@ -1105,11 +1287,11 @@ static int sm_count()
     return sms;
 }
 
-// Tensor map of a channel-last BF16 tensor [nb][nz][ny][nx][16] with the
-// brick box (16 channels, 16 x 10 x 6 points, 1 sample) written in the 32-byte
+// Tensor map of a channel-last BF16 tensor [nb][nz][ny][nx][16] with a box
+// of 16 channels x bx x by x bz points x 1 sample, written in the 32-byte
 // swizzle that the A descriptors declare; the driver entry point is looked up
 // once through the runtime.
-static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
+static int bf16_box_map(const ConvGrid& g, const void* in, int bx, int by, int bz, CUtensorMap* map)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if(!encode)
@@ -1125,13 +1307,19 @@ static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
                                 (cuuint64_t)g.nb};
     const cuuint64_t row = (cuuint64_t)kNetCh * 2;
     const cuuint64_t strides[4] = {row, row * g.nx, row * g.nx * g.ny, row * g.nx * g.ny * g.nz};
-    const cuuint32_t box[5] = {(cuuint32_t)kNetCh, (cuuint32_t)kTX, (cuuint32_t)kHY, (cuuint32_t)kHZ, 1};
+    const cuuint32_t box[5] = {(cuuint32_t)kNetCh, (cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(in), dims, strides, box,
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if(r != CUDA_SUCCESS) return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return 0;
+}
+
+// The conv brick box: 16 x 10 x 6 points (x without halo: three shifted loads).
+static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
+{
+    return bf16_box_map(g, in, kTX, kHY, kHZ, map);
 }
 
 template <int kOut>
@@ -1170,6 +1358,44 @@ int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mod
         case kOutPermAdd: return conv_launch<kOutPermAdd>(g, in, wB, out, act, m, status, s);
         default: return record_error(HPCGB200_ERR_ARG, "conv16: unknown output mode %d", out_mode);
     }
+}
+
+template <int kOut, bool kPair>
+static int layer3_launch(const ConvGrid& g, const void* a2, const float* w3, float* out, const PermMap& pm,
+                         int* status, cudaStream_t s)
+{
+    static bool attr = false;
+    if(!attr)
+    {
+        HB_CUDA(cudaFuncSetAttribute(k_layer3_tc<kOut, kPair>, cudaFuncAttributeMaxDynamicSharedMemorySize, k3Smem));
+        attr = true;
+    }
+    CUtensorMap map;
+    const ConvGrid gin{kPair ? 2 * g.nb : g.nb, g.nz, g.ny, g.nx};
+    HB_RETURN_IF(bf16_box_map(gin, a2, k3HX, k3HY, k3HZ, &map));
+    const long tiles = (long)g.nb * ((g.nx + k3X - 1) / k3X) * ((g.ny + k3Y - 1) / k3Y) * ((g.nz + k3Z - 1) / k3Z);
+    const long cap = sm_count();
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    k_layer3_tc<kOut, kPair><<<grid, kConvThreads, k3Smem, s>>>(map, g, w3, out, pm, status);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_layer3_tc(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
+                     float* out, int* status, cudaStream_t s)
+{
+    if(mode < 0 || mode > 2) return record_error(HPCGB200_ERR_ARG, "layer 3: unknown output mode %d", mode);
+    if(mode != 2 && (!pm || g.nb != 1)) return record_error(HPCGB200_ERR_ARG, "layer 3: level output needs one sample");
+    const PermMap m = pm ? *pm : PermMap{};
+    if(pair)
+    {
+        if(mode == 0) return layer3_launch<0, true>(g, a2, w3, out, m, status, s);
+        if(mode == 1) return layer3_launch<1, true>(g, a2, w3, out, m, status, s);
+        return layer3_launch<2, true>(g, a2, w3, out, m, status, s);
+    }
+    if(mode == 0) return layer3_launch<0, false>(g, a2, w3, out, m, status, s);
+    if(mode == 1) return layer3_launch<1, false>(g, a2, w3, out, m, status, s);
+    return layer3_launch<2, false>(g, a2, w3, out, m, status, s);
 }
 
 int conv16_wgrad_parts(long points)
@@ -1247,29 +1473,6 @@ int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const fl
     {
         if(pair) k_layer1_direct<true, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
         else k_layer1_direct<false, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
-    }
-    HB_LAUNCHED();
-    return 0;
-}
-
-int launch_layer3_direct(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
-                         float* out, cudaStream_t s)
-{
-    if(mode != 2 && (!pm || g.nb != 1)) return record_error(HPCGB200_ERR_ARG, "layer 3: level output needs one sample");
-    const unsigned grid = (unsigned)((g.points() + 255) / 256);
-    const PermMap m = pm ? *pm : PermMap{};
-    const auto* a = (const __nv_bfloat16*)a2;
-    if(pair)
-    {
-        if(mode == 0) k_layer3_direct<true, 0><<<grid, 256, 0, s>>>(g, m, a, w3, out);
-        else if(mode == 1) k_layer3_direct<true, 1><<<grid, 256, 0, s>>>(g, m, a, w3, out);
-        else k_layer3_direct<true, 2><<<grid, 256, 0, s>>>(g, m, a, w3, out);
-    }
-    else
-    {
-        if(mode == 0) k_layer3_direct<false, 0><<<grid, 256, 0, s>>>(g, m, a, w3, out);
-        else if(mode == 1) k_layer3_direct<false, 1><<<grid, 256, 0, s>>>(g, m, a, w3, out);
-        else k_layer3_direct<false, 2><<<grid, 256, 0, s>>>(g, m, a, w3, out);
     }
     HB_LAUNCHED();
     return 0;

@@ -49,8 +49,9 @@ int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s);
 int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mode, void* out, const void* act,
                   const PermMap* pm, int* status, cudaStream_t s);
 
-// Evaluation-only layers 1 and 3 on the CUDA cores (FP32 with BF16-rounded
-// weights; layer 1 has one input channel, layer 3 one output channel).
+// Evaluation-only kernels of the layers with one channel on one side: layer 1
+// on the CUDA cores (FP32 with BF16-rounded weights, one input channel),
+// layer 3 on the tensor cores (one output channel).
 // s1 = bf16 scalar field of a level (r, or r - A x when x is not null).
 int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
                               const float* diag32, void* s1, cudaStream_t s);
@@ -60,8 +61,11 @@ int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const fl
                          cudaStream_t s);
 // Channel 0 of conv(a2, W3), odd-combined when pair ((y(a2) - y(a2 + 16 n)) / 2);
 // mode 0: set, 1: add into a level vector through pm (g.nb == 1); 2: natural out.
-int launch_layer3_direct(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
-                         float* out, cudaStream_t s);
+// The 27 taps are stacked in N (one MMA row per staged input point gives its
+// contribution to each neighbour), the pair is folded into K, and the 27-tap
+// gather runs in the epilogue; `status` receives the code of a wait that gave up.
+int launch_layer3_tc(const ConvGrid& g, const PermMap* pm, const void* a2, const float* w3, int pair, int mode,
+                     float* out, int* status, cudaStream_t s);
 
 // dw[tap][ci][co] = sum_p x[p + tap][ci] * gr[p][co] (partial: one block of
 // conv16_wgrad_parts(points) x 27*256 floats).

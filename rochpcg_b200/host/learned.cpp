@@ -143,15 +143,15 @@ int smoother_level_apply(Smoother& S, const LevelOpt& o, const float* r, float* 
     if((long)L.nz * L.ny * L.nx > S.cap)
         return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: buffers not reserved");
     if(S.tiles_stale) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: weights not prepared");
-    // layer 1 (one input channel) and layer 3 (one output channel) on the CUDA
-    // cores, layer 2 (16 -> 16) on the tensor cores; the scalar input field
-    // lives in a0
+    // layer 1 (one input channel) on the CUDA cores, layer 2 (16 -> 16) and
+    // layer 3 (taps stacked in N, the odd pair folded into K) on the tensor
+    // cores; the scalar input field lives in a0
     const hb::ConvGrid g1{1, L.nz, L.ny, L.nx};
     HB_RETURN_IF(hb::launch_embed_scalar_level(o.pm, L.nz, L.ny, L.nx, r, residual ? x : nullptr, o.diag32, S.a0, s));
     HB_RETURN_IF(hb::launch_layer1_direct(g1, S.a0, 0, S.w, S.a1, S.odd ? 1 : 0, s));
     HB_RETURN_IF(hb::launch_conv16(g, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
-    return hb::launch_layer3_direct(g1, &o.pm, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, residual ? 1 : 0,
-                                    x, s);
+    return hb::launch_layer3_tc(g1, &o.pm, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, residual ? 1 : 0, x,
+                                S.status, s);
 }
 
 // Raw network output of a batch into y (both branches, 2 g.nb samples, when odd).
@@ -165,7 +165,8 @@ static int forward_batch(Smoother& S, const hb::ConvGrid& g, const float* r, flo
     return hb::launch_conv16(gg, S.a2, tiles(S, 2), hb::kOutF32C0, y, nullptr, nullptr, S.status, s);
 }
 
-// Evaluation as in the V-cycle: layers 1 and 3 on the CUDA cores.
+// Evaluation as in the V-cycle: layer 1 on the CUDA cores, layers 2 and 3 on
+// the tensor cores.
 int smoother_forward(Smoother& S, const hb::ConvGrid& g, const float* r, float* y, cudaStream_t s)
 {
     smoother_reserve(S, g.points(), false);
@@ -173,7 +174,7 @@ int smoother_forward(Smoother& S, const hb::ConvGrid& g, const float* r, float* 
     const hb::ConvGrid gg{S.odd ? 2 * g.nb : g.nb, g.nz, g.ny, g.nx};
     HB_RETURN_IF(hb::launch_layer1_direct(g, r, 1, S.w, S.a1, S.odd ? 1 : 0, s));
     HB_RETURN_IF(hb::launch_conv16(gg, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
-    return hb::launch_layer3_direct(g, nullptr, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, 2, y, s);
+    return hb::launch_layer3_tc(g, nullptr, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, 2, y, S.status, s);
 }
 
 int smoother_loss_grad(Smoother& S, const hb::ConvGrid& g0, const float* r, const float* e, const float* wnorm,
