@@ -1113,53 +1113,167 @@ __global__ void k_embed_scalar_level(PermMap pm, int nz, int ny, int nx, const f
 __device__ __forceinline__ float in_value(const __nv_bfloat16* v, long q) { return __bfloat162float(v[q]); }
 __device__ __forceinline__ float in_value(const float* v, long q) { return __bfloat162float(__float2bfloat16_rn(v[q])); }
 
-// a1[p] = bf16(relu(z)), z[co] = sum_t w1[t][0][co] in[p + t]; with kPair also
-// a1[p + n] = bf16(relu(-z)) (the branch of -in).  nb samples back to back.
-template <bool kPair, typename Tin>
-__global__ void __launch_bounds__(256) k_layer1_direct(ConvGrid g, const Tin* __restrict__ in,
-                                                       const float* __restrict__ w1, __nv_bfloat16* __restrict__ a1)
+
+// ------------------------------------------------------------ layer 1 (1 -> 16)
+//
+// One input channel: the 27 taps are the K dimension.  Per brick of
+// 16 x 8 x 4 points the CTA stages the halo'd scalar field (18 x 10 x 6,
+// BF16-rounded, zero outside the grid), each thread writes the im2col row of
+// its point in every z plane (27 neighbours, 5 zeros: K = 32), and two MMAs
+// per plane (M = 128 points, N = 16 channels, K = 16 each) give the 16
+// pre-activations in TMEM; the epilogue writes relu(z) and, for the odd pair,
+// relu(-z) as BF16.  Several CTAs per SM overlap one CTA's MMA round trip with
+// the others' staging.
+constexpr int k1X = 16, k1Y = 8, k1Z = 4;
+constexpr int k1HX = k1X + 2, k1HY = k1Y + 2, k1HZ = k1Z + 2;
+constexpr int k1Halo = k1HX * k1HY * k1HZ;  // 1080 staged scalars
+constexpr int k1Threads = 128;              // one thread per point of a plane
+constexpr int k1K = 32;                     // 27 taps + 5 zeros
+constexpr int k1PlaneBytes = 128 * k1K * 2; // 8 KB of im2col rows per plane
+constexpr int k1Cols = k1Z * kNetCh;        // TMEM columns per brick
+constexpr int k1WBytes = kNetCh * k1K * 2;  // B: 16 channel rows x 32 taps
+constexpr int k1Smem = k1Z * k1PlaneBytes + k1WBytes + k1Halo * 4 + 64 + 1024;
+constexpr int k1CtasPerSm = 4;
+
+static_assert(k1X * k1Y == k1Threads, "one plane of the brick is one 128-row M tile");
+static_assert(k1Cols * k1CtasPerSm <= 512, "TMEM columns of the co-resident CTAs");
+
+// K-major no-swizzle offset of row r, 8-element K chunk c8 of a 32-wide K
+// operand: chunks 128 B apart (LBO), 8-row groups 512 B apart (SBO).
+__host__ __device__ constexpr uint32_t k1_off(int r, int c8)
 {
-    __shared__ float w[27 * kNetCh];
-    for(int i = threadIdx.x; i < 27 * kNetCh; i += blockDim.x)
-        w[i] = __bfloat162float(__float2bfloat16_rn(w1[(i / kNetCh) * kNetCh * kNetCh + (i % kNetCh)]));
-    __syncthreads();
-    const long n = g.points();
-    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if(p >= n) return;
-    const long per = (long)g.nz * g.ny * g.nx;
-    const long base = (p / per) * per;
-    const long q0 = p - base;
-    const int z = (int)(q0 / ((long)g.ny * g.nx));
-    const long rem = q0 - (long)z * g.ny * g.nx;
-    const int y = (int)(rem / g.nx), x = (int)(rem - (long)y * g.nx);
-    float acc[kNetCh];
-#pragma unroll
-    for(int co = 0; co < kNetCh; ++co) acc[co] = 0.f;
-#pragma unroll
-    for(int t = 0; t < 27; ++t)
-    {
-        const int zz = z + t / 9 - 1, yy = y + (t / 3) % 3 - 1, xx = x + t % 3 - 1;
-        if(zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) continue;
-        const float v = in_value(in, base + ((long)zz * g.ny + yy) * g.nx + xx);
-#pragma unroll
-        for(int co = 0; co < kNetCh; ++co) acc[co] = fmaf(v, w[t * kNetCh + co], acc[co]);
-    }
-    float pos[kNetCh];
-#pragma unroll
-    for(int co = 0; co < kNetCh; ++co) pos[co] = fmaxf(acc[co], 0.f);
-    uint4* dst = reinterpret_cast<uint4*>(a1 + p * kNetCh);
-    dst[0] = pack_bf16x8(pos);
-    dst[1] = pack_bf16x8(pos + 8);
-    if(kPair)
-    {
-        float neg[kNetCh];
-#pragma unroll
-        for(int co = 0; co < kNetCh; ++co) neg[co] = fmaxf(-acc[co], 0.f);
-        uint4* d2 = reinterpret_cast<uint4*>(a1 + (p + n) * kNetCh);
-        d2[0] = pack_bf16x8(neg);
-        d2[1] = pack_bf16x8(neg + 8);
-    }
+    return (uint32_t)((r >> 3) * 512 + c8 * 128 + (r & 7) * 16);
 }
+
+template <typename Tin, bool kPair>
+__global__ void __launch_bounds__(k1Threads) k_layer1_tc(ConvGrid g, const Tin* __restrict__ in,
+                                                         const float* __restrict__ w1,
+                                                         __nv_bfloat16* __restrict__ a1, int* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sA = smem;                           // k1Z im2col planes
+    unsigned char* sW = sA + k1Z * k1PlaneBytes;        // weights
+    float* sS = (float*)(sW + k1WBytes);                // staged scalars
+    uint64_t* mbar = (uint64_t*)(sS + k1Halo);
+    uint32_t* tholder = (uint32_t*)(mbar + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for(int i = tid; i < kNetCh * k1K; i += k1Threads)
+    {
+        const int co = i / k1K, t = i % k1K;
+        const float w = t < 27 ? w1[t * kNetCh * kNetCh + co] : 0.f;  // w1[t][0][co]
+        *reinterpret_cast<__nv_bfloat16*>(sW + k1_off(co, t >> 3) + (t & 7) * 2) = __float2bfloat16_rn(w);
+    }
+    if(tid == 0) mbar_init(mbar, 1);
+    if(warp == 0) tmem_alloc(tholder, k1Cols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tholder;
+
+    const long n = g.points();
+    const int tx = (g.nx + k1X - 1) / k1X, ty = (g.ny + k1Y - 1) / k1Y, tz = (g.nz + k1Z - 1) / k1Z;
+    const long per_sample = (long)tx * ty * tz;
+    const long ntiles = per_sample * g.nb;
+    constexpr uint32_t idesc = umma_idesc_bf16(128, kNetCh, false, false);
+    const uint64_t bd = umma_desc(smem_u32(sW), 128, 512);
+    const int mx = tid % k1X, my = tid / k1X;
+    uint32_t phase = 0;
+    bool failed = false;
+    for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    {
+        const int b = (int)(tile / per_sample);
+        long t2 = tile - (long)b * per_sample;
+        const int bz = (int)(t2 / ((long)tx * ty));
+        t2 -= (long)bz * tx * ty;
+        const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
+        const int x0 = bx * k1X, y0 = by * k1Y, z0 = bz * k1Z;
+        const long base = (long)b * g.nz * g.ny * g.nx;
+        for(int e = tid; e < k1Halo; e += k1Threads)
+        {
+            const int hx = e % k1HX, hy = (e / k1HX) % k1HY, hz = e / (k1HX * k1HY);
+            const int x = x0 + hx - 1, y = y0 + hy - 1, z = z0 + hz - 1;
+            float v = 0.f;
+            if(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)
+                v = in_value(in, base + ((long)z * g.ny + y) * g.nx + x);
+            sS[e] = v;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for(int q = 0; q < k1Z; ++q)
+        {
+            __align__(16) __nv_bfloat16 h[k1K];
+#pragma unroll
+            for(int t = 0; t < 27; ++t)
+            {
+                const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                h[t] = __float2bfloat16_rn(sS[((q + 1 + dz) * k1HY + (my + 1 + dy)) * k1HX + (mx + 1 + dx)]);
+            }
+#pragma unroll
+            for(int t = 27; t < k1K; ++t) h[t] = __float2bfloat16_rn(0.f);
+            unsigned char* row = sA + q * k1PlaneBytes;
+#pragma unroll
+            for(int c8 = 0; c8 < k1K / 8; ++c8)
+                *reinterpret_cast<uint4*>(row + k1_off(tid, c8)) = *reinterpret_cast<const uint4*>(h + 8 * c8);
+        }
+        fence_async_smem();  // the im2col rows are read by the tensor cores
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if(tid == 0)
+        {
+#pragma unroll
+            for(int q = 0; q < k1Z; ++q)
+#pragma unroll
+                for(int kh = 0; kh < 2; ++kh)
+                    mma_bf16(tmem + q * kNetCh, umma_desc(smem_u32(sA + q * k1PlaneBytes + kh * 256), 128, 512),
+                             bd + (uint64_t)((kh * 256) >> 4), idesc, (uint32_t)kh);
+            mma_commit(mbar);
+        }
+        const bool ok = mbar_wait(mbar, phase);
+        phase ^= 1u;
+        if(__syncthreads_or(!ok))
+        {
+            if(tid == 0) atomicExch(status, 7);
+            failed = true;
+            break;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for(int q = 0; q < k1Z; ++q)
+        {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * kNetCh), v);
+            const int x = x0 + mx, y = y0 + my, z = z0 + q;
+            if(x >= g.nx || y >= g.ny || z >= g.nz) continue;
+            const long p = base + ((long)z * g.ny + y) * g.nx + x;
+            float pos[16];
+#pragma unroll
+            for(int c = 0; c < 16; ++c) pos[c] = fmaxf(v[c], 0.f);
+            uint4* dst = reinterpret_cast<uint4*>(a1 + p * kNetCh);
+            dst[0] = pack_bf16x8(pos);
+            dst[1] = pack_bf16x8(pos + 8);
+            if(kPair)
+            {
+#pragma unroll
+                for(int c = 0; c < 16; ++c) pos[c] = fmaxf(-v[c], 0.f);
+                uint4* d2 = reinterpret_cast<uint4*>(a1 + (p + n) * kNetCh);
+                d2[0] = pack_bf16x8(pos);
+                d2[1] = pack_bf16x8(pos + 8);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM, im2col planes and staged scalars free for the next brick
+    }
+    if(failed) mbar_wait(mbar, phase ^ 1u);  // the MMAs in flight finish before TMEM is released
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if(warp == 0) tmem_free(tmem, k1Cols);
+}
+
 
 // 1 / (e.e) (kind 0) or 1 / (e.Ae) (kind 1) per sample: one block per sample.
 __global__ void k_sample_norm(ConvGrid g, const float* __restrict__ e, int kind, float* __restrict__ out)
@@ -1459,23 +1573,34 @@ int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const f
     return 0;
 }
 
-int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair,
+
+template <typename Tin, bool kPair>
+static int layer1_launch(const ConvGrid& g, const Tin* in, const float* w1, __nv_bfloat16* a1, int* status,
                          cudaStream_t s)
 {
-    const unsigned grid = (unsigned)((g.points() + 255) / 256);
-    auto* out = (__nv_bfloat16*)a1;
-    if(in_f32)
+    static bool attr = false;
+    if(!attr)
     {
-        if(pair) k_layer1_direct<true, float><<<grid, 256, 0, s>>>(g, (const float*)in, w1, out);
-        else k_layer1_direct<false, float><<<grid, 256, 0, s>>>(g, (const float*)in, w1, out);
+        HB_CUDA(cudaFuncSetAttribute(k_layer1_tc<Tin, kPair>, cudaFuncAttributeMaxDynamicSharedMemorySize, k1Smem));
+        attr = true;
     }
-    else
-    {
-        if(pair) k_layer1_direct<true, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
-        else k_layer1_direct<false, __nv_bfloat16><<<grid, 256, 0, s>>>(g, (const __nv_bfloat16*)in, w1, out);
-    }
+    const long tiles = (long)g.nb * ((g.nx + k1X - 1) / k1X) * ((g.ny + k1Y - 1) / k1Y) * ((g.nz + k1Z - 1) / k1Z);
+    const long cap = (long)k1CtasPerSm * sm_count();
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    k_layer1_tc<Tin, kPair><<<grid, k1Threads, k1Smem, s>>>(g, in, w1, a1, status);
     HB_LAUNCHED();
     return 0;
+}
+
+int launch_layer1_tc(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair, int* status,
+                     cudaStream_t s)
+{
+    auto* out = (__nv_bfloat16*)a1;
+    if(in_f32)
+        return pair ? layer1_launch<float, true>(g, (const float*)in, w1, out, status, s)
+                    : layer1_launch<float, false>(g, (const float*)in, w1, out, status, s);
+    return pair ? layer1_launch<__nv_bfloat16, true>(g, (const __nv_bfloat16*)in, w1, out, status, s)
+                : layer1_launch<__nv_bfloat16, false>(g, (const __nv_bfloat16*)in, w1, out, status, s);
 }
 
 int launch_odd_natural(long n, const float* y, float* out, cudaStream_t s)

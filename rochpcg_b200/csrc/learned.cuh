@@ -49,16 +49,18 @@ int launch_prepare_weights(const float* w, void* wB, int flip, cudaStream_t s);
 int launch_conv16(const ConvGrid& g, const void* in, const void* wB, int out_mode, void* out, const void* act,
                   const PermMap* pm, int* status, cudaStream_t s);
 
-// Evaluation-only kernels of the layers with one channel on one side: layer 1
-// on the CUDA cores (FP32 with BF16-rounded weights, one input channel),
-// layer 3 on the tensor cores (one output channel).
+// Evaluation-only kernels: the scalar input field of a level, and the
+// tensor-core forms of the layers with one channel on one side (layer 1: one
+// input channel, layer 3: one output channel).
 // s1 = bf16 scalar field of a level (r, or r - A x when x is not null).
 int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const float* r, const float* x,
                               const float* diag32, void* s1, cudaStream_t s);
 // a1 = bf16(relu(conv(in, W1))) from a scalar field in (FP32 when in_f32, else
-// BF16), 16 channels; pair: also the branch of -in at a1 + 16 * points.
-int launch_layer1_direct(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair,
-                         cudaStream_t s);
+// BF16), 16 channels; pair: also the branch of -in at a1 + 16 * points.  The
+// 27 taps are the K dimension (im2col rows built in shared memory), the 16
+// channels N; `status` receives the code of a wait that gave up.
+int launch_layer1_tc(const ConvGrid& g, const void* in, int in_f32, const float* w1, void* a1, int pair, int* status,
+                     cudaStream_t s);
 // Channel 0 of conv(a2, W3), odd-combined when pair ((y(a2) - y(a2 + 16 n)) / 2);
 // mode 0: set, 1: add into a level vector through pm (g.nb == 1); 2: natural out.
 // The 27 taps are stacked in N (one MMA row per staged input point gives its

@@ -143,12 +143,12 @@ int smoother_level_apply(Smoother& S, const LevelOpt& o, const float* r, float* 
     if((long)L.nz * L.ny * L.nx > S.cap)
         return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: buffers not reserved");
     if(S.tiles_stale) return hb::record_error(HPCGB200_ERR_ARG, "learned smoother: weights not prepared");
-    // layer 1 (one input channel) on the CUDA cores, layer 2 (16 -> 16) and
-    // layer 3 (taps stacked in N, the odd pair folded into K) on the tensor
-    // cores; the scalar input field lives in a0
+    // all three layers on the tensor cores: layer 1 with the taps as K (one
+    // input channel), layer 2 (16 -> 16), layer 3 with the taps stacked in N
+    // and the odd pair folded into K; the scalar input field lives in a0
     const hb::ConvGrid g1{1, L.nz, L.ny, L.nx};
     HB_RETURN_IF(hb::launch_embed_scalar_level(o.pm, L.nz, L.ny, L.nx, r, residual ? x : nullptr, o.diag32, S.a0, s));
-    HB_RETURN_IF(hb::launch_layer1_direct(g1, S.a0, 0, S.w, S.a1, S.odd ? 1 : 0, s));
+    HB_RETURN_IF(hb::launch_layer1_tc(g1, S.a0, 0, S.w, S.a1, S.odd ? 1 : 0, S.status, s));
     HB_RETURN_IF(hb::launch_conv16(g, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
     return hb::launch_layer3_tc(g1, &o.pm, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, residual ? 1 : 0, x,
                                 S.status, s);
@@ -165,14 +165,13 @@ static int forward_batch(Smoother& S, const hb::ConvGrid& g, const float* r, flo
     return hb::launch_conv16(gg, S.a2, tiles(S, 2), hb::kOutF32C0, y, nullptr, nullptr, S.status, s);
 }
 
-// Evaluation as in the V-cycle: layer 1 on the CUDA cores, layers 2 and 3 on
-// the tensor cores.
+// Evaluation as in the V-cycle (the one-channel forms of layers 1 and 3).
 int smoother_forward(Smoother& S, const hb::ConvGrid& g, const float* r, float* y, cudaStream_t s)
 {
     smoother_reserve(S, g.points(), false);
     HB_RETURN_IF(smoother_prepare(S, s));
     const hb::ConvGrid gg{S.odd ? 2 * g.nb : g.nb, g.nz, g.ny, g.nx};
-    HB_RETURN_IF(hb::launch_layer1_direct(g, r, 1, S.w, S.a1, S.odd ? 1 : 0, s));
+    HB_RETURN_IF(hb::launch_layer1_tc(g, r, 1, S.w, S.a1, S.odd ? 1 : 0, S.status, s));
     HB_RETURN_IF(hb::launch_conv16(gg, S.a1, tiles(S, 1), hb::kOutReluBf16, S.a2, nullptr, nullptr, S.status, s));
     return hb::launch_layer3_tc(g, nullptr, S.a2, S.w + 2 * hb::kNetLayerWeights, S.odd ? 1 : 0, 2, y, S.status, s);
 }
