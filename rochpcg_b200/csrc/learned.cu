@@ -185,27 +185,30 @@ __device__ __forceinline__ uint4 pack_bf16x8(const float* v)
 // 16-column (K = 16) operands with SBO = 256 B, LBO = 128 B.
 __host__ __device__ constexpr uint32_t kmajor_off(int r, int c) { return (uint32_t)((r >> 3) * 256 + c * 128 + (r & 7) * 16); }
 
-// Weight tile slot of tap t = (dz+1)*9 + (dy+1)*3 + (dx+1): the three dz taps
-// of one (dy, dx) are adjacent, ordered dz = +1, 0, -1, so one 48-row K-major
-// B operand (SBO 256 B, tile stride 512 B) holds all three.
-__host__ __device__ constexpr int weight_slot(int t) { return (t % 9) * 3 + 2 - t / 9; }
+// Weight tile slot (16 output-channel rows x 16 input channels, 512 B) of tap
+// t = (dz+1)*9 + (dy+1)*3 + (dx+1): ordered [dy][dz = +1, 0, -1][dx], so the
+// 9 taps of one dy form one 144-row K-major B operand (SBO 256 B) whose rows
+// are (dz, dx, output channel) -- any run of its dz blocks is contiguous.
+__host__ __device__ constexpr int weight_slot(int t) { return ((t / 3) % 3) * 9 + (2 - t / 9) * 3 + t % 3; }
 
 // ------------------------------------------------------------ forward conv
 //
-// Warp-specialised persistent kernel, one CTA per SM:
-//   warp 0      TMA producer: for each brick, three tiled loads (one per dx
-//               shift, 32-byte rows of 16 channels in the 32-byte swizzle) of
-//               the halo'd brick into one of kStages shared-memory stages
-//               (zero fill outside the grid);
-//   warp 1      allocates TMEM and issues the brick's tcgen05.mma into one of
-//               two TMEM accumulators: for each staged input plane q and
-//               in-plane tap (dy, dx), ONE MMA with N = 16 x (number of output
-//               planes q feeds) multiplies the plane by the stacked weights of
-//               its dz taps (output plane q - 1 - dz lives in columns 16 x that
-//               plane), so a brick of kTZ planes takes 9 (kTZ + 2) + kTZ - 1
-//               MMAs instead of 27 kTZ (57 vs 108 for kTZ = 4);
-//   warps 2-5   epilogue: tcgen05.ld of the finished accumulator, ReLU /
-//               mask / permuted scatter, global stores.
+// Warp-specialised persistent kernel, one CTA per SM.  A brick is 14 x 8 x kTZ
+// output points; its input box is 16 x 10 x (kTZ + 2) points (one point of
+// halo on every side), one TMA load of 32-byte swizzled rows.  The dx and dz
+// taps are stacked in N: for each staged plane q and row shift dy, ONE MMA
+// (M = 128 staged points of the plane, K = 16 input channels) multiplies the
+// shifted plane by the weights of all (dz, dx) taps it feeds, N = 48 per
+// output plane (3 dx x 16 channels) for the 1-3 output planes q - 1 - dz;
+// the epilogue adds the dx = -1 / +1 blocks of the x-neighbouring rows (lane
+// shuffles), so the two halo columns of the box produce no output.
+//   warp 0      TMA producer into kStages shared-memory stages (zero fill
+//               outside the grid);
+//   warp 1      TMEM owner and MMA issuer: 3 (kTZ + 2) + kTZ - 1 MMAs per
+//               brick (21 for kTZ = 4) into one of two accumulators of
+//               kTZ x 48 columns;
+//   warps 2-5   epilogue: tcgen05.ld of the finished accumulator, the dx
+//               combination, ReLU / mask / permuted scatter, global stores.
 // Stage and accumulator hand-offs are mbarriers (TMA complete_tx, MMA commit,
 // epilogue arrivals), so loads, MMAs and stores of consecutive bricks overlap.
 
@@ -213,27 +216,31 @@ __host__ __device__ constexpr int weight_slot(int t) { return (t % 9) * 3 + 2 - 
 #define HB_CONV_TZ 4
 #endif
 #ifndef HB_CONV_STAGES
-#define HB_CONV_STAGES 2
+#define HB_CONV_STAGES 4
 #endif
 #ifndef HB_CONV_CTAS
 #define HB_CONV_CTAS 1
 #endif
-constexpr int kTX = 16, kTY = 8, kTZ = HB_CONV_TZ;
+constexpr int kTX = 16, kTY = 8, kTZ = HB_CONV_TZ;  // staged x width (with halo), output y, output z
+constexpr int kOX = kTX - 2;                          // output x per brick
 constexpr int kHY = kTY + 2, kHZ = kTZ + 2;
-constexpr int kCopyRows = kTX * kHY * kHZ;            // 960 rows per shifted copy
+constexpr int kCopyRows = kTX * kHY * kHZ;            // 960 staged points
 constexpr int kRowBytes = kNetCh * 2;                 // the 16 BF16 channels of a point: one 32-byte swizzle row
 constexpr int kCopyBytes = kCopyRows * kRowBytes;     // 30720 B = one TMA box
-constexpr int kStageBytes = 3 * kCopyBytes;           // 92160 B
+constexpr int kStageBytes = kCopyBytes;
 constexpr int kStages = HB_CONV_STAGES;
-constexpr int kAccCols = kTZ * 16;                    // FP32 columns of one brick's accumulator
-constexpr int kTmemCols = 2 * kAccCols;               // double-buffered: 128 columns
+constexpr int kPlaneCols = 3 * kNetCh;                // one output plane: 3 dx blocks of 16 channels
+constexpr int kAccCols = kTZ * kPlaneCols;            // FP32 columns of one brick's accumulator (192)
+constexpr int kTmemCols = 512;                        // two accumulators, rounded to a power of two
 constexpr int kConvThreads = 192;
 constexpr int kEpiThreads = 128;
 constexpr int kConvSmem = kStages * kStageBytes + kNetWeightTileBytes + 256 + 1024;
 
 static_assert(kRowBytes == 32, "one point per 32-byte swizzle row (K = 16 per MMA)");
 static_assert(kTX * kTY == 128, "one z plane of the brick is one 128-row M tile");
-static_assert(kStageBytes % 1024 == 0 && kCopyBytes % 1024 == 0, "stages and copies start on swizzle-atom boundaries");
+static_assert(kStageBytes % 1024 == 0, "stages start on swizzle-atom boundaries");
+static_assert(2 * kAccCols <= kTmemCols && kTmemCols <= 512, "TMEM accumulators");
+static_assert(3 * kPlaneCols <= 256, "MMA N");
 static_assert(kConvSmem <= 227 * 1024, "shared memory per CTA");
 
 struct Brick
@@ -249,7 +256,7 @@ __device__ __forceinline__ Brick brick_of(const ConvGrid& g, long tile, int tx, 
     const int bz = (int)(t2 / ((long)tx * ty));
     t2 -= (long)bz * tx * ty;
     const int by = (int)(t2 / tx), bx = (int)(t2 - (long)by * tx);
-    r.x0 = bx * kTX;
+    r.x0 = bx * kOX;  // first output x; the box starts one point before
     r.y0 = by * kTY;
     r.z0 = bz * kTZ;
     return r;
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY, tz = (g.nz + kTZ - 1) / kTZ;
+    const int tx = (g.nx + kOX - 1) / kOX, ty = (g.ny + kTY - 1) / kTY, tz = (g.nz + kTZ - 1) / kTZ;
     const long per_sample = (long)tx * ty * tz;
     const long ntiles = per_sample * g.nb;
 
@@ -357,11 +364,8 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             const uint32_t ph = (uint32_t)((issued / kStages) & 1);
             if(!role_wait(&empty[st], ph ^ 1u, abort_flag, status, 3)) break;
             const Brick bk = brick_of(g, tile, tx, ty, per_sample);
-            mbar_expect_tx(&full[st], 3u * kCopyBytes);
-            unsigned char* dst = sA + st * kStageBytes;
-#pragma unroll
-            for(int dxi = 0; dxi < 3; ++dxi)
-                tma_load_5d(dst + dxi * kCopyBytes, &in_map, 0, bk.x0 + dxi - 1, bk.y0 - 1, bk.z0 - 1, bk.b, &full[st]);
+            mbar_expect_tx(&full[st], (uint32_t)kCopyBytes);
+            tma_load_5d(sA + st * kStageBytes, &in_map, 0, bk.x0 - 1, bk.y0 - 1, bk.z0 - 1, bk.b, &full[st]);
         }
         if(*abort_flag)
         {
@@ -383,9 +387,6 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
     else if(warp == 1 && lane == 0)
     {
         // ---- MMA issuer
-        constexpr uint32_t idesc16 = umma_idesc_bf16(128, 16, false, false);
-        constexpr uint32_t idesc32 = umma_idesc_bf16(128, 32, false, false);
-        constexpr uint32_t idesc48 = umma_idesc_bf16(128, 48, false, false);
         const uint64_t bd0 = umma_desc(smem_u32(sW), 128, 256);
         long i = 0;
         for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i)
@@ -402,33 +403,33 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             const uint64_t ad0 = umma_desc_sw32(smem_u32(sA + st * kStageBytes));
             const uint32_t d0 = tmem + (uint32_t)(acc * kAccCols);
             // staged plane q (z = z0 - 1 + q) feeds output planes mt = q - 1 - dz
-            // in [lo, hi]; group mt takes B tile j = mt - q + 2 of the (dy, dx)
-            // triple.  Group q is first written at (q, dy = dx = -1), with the
-            // accumulate flag off, by an MMA of its own.
+            // in [lo, hi]; output plane mt takes dz block j = mt - q + 2 of the
+            // row shift's 144-row operand.  Output plane q is first written at
+            // (q, dy = -1), with the accumulate flag off, by an MMA of its own.
 #pragma unroll
             for(int q = 0; q < kTZ + 2; ++q)
             {
                 const int lo = q - 2 < 0 ? 0 : q - 2;
                 const int hi = q < kTZ - 1 ? q : kTZ - 1;
 #pragma unroll
-                for(int sxy = 0; sxy < 9; ++sxy)
+                for(int dyi = 0; dyi < 3; ++dyi)
                 {
-                    const int dy = sxy / 3 - 1, dx = sxy % 3 - 1;
-                    const int row0 = (q * kHY + (dy + 1)) * kTX;
-                    const uint64_t ad = ad0 + (uint64_t)(((dx + 1) * kCopyBytes + row0 * kRowBytes) >> 4);
-                    const uint64_t bs = bd0 + (uint64_t)((sxy * 3 * 512) >> 4);
-                    if(q <= kTZ - 1 && sxy == 0)
+                    const int row0 = (q * kHY + dyi) * kTX;
+                    const uint64_t ad = ad0 + (uint64_t)((row0 * kRowBytes) >> 4);
+                    const uint64_t bs = bd0 + (uint64_t)((dyi * 9 * 512) >> 4);
+                    auto mma = [&](int m0, int m1, uint32_t accumulate) {
+                        const uint32_t idesc = umma_idesc_bf16(128, (m1 - m0 + 1) * kPlaneCols, false, false);
+                        mma_bf16(d0 + m0 * kPlaneCols, ad, bs + (uint64_t)(((m0 - q + 2) * 3 * 512) >> 4), idesc,
+                                 accumulate);
+                    };
+                    if(q <= kTZ - 1 && dyi == 0)
                     {
-                        if(hi > lo)
-                            mma_bf16(d0 + lo * 16, ad, bs + (uint64_t)(((lo - q + 2) * 512) >> 4),
-                                     hi - lo == 1 ? idesc16 : idesc32, 1u);
-                        mma_bf16(d0 + hi * 16, ad, bs + (uint64_t)(((hi - q + 2) * 512) >> 4), idesc16, 0u);
+                        if(hi > lo) mma(lo, hi - 1, 1u);
+                        mma(hi, hi, 0u);
                     }
                     else
                     {
-                        const int n = hi - lo + 1;
-                        mma_bf16(d0 + lo * 16, ad, bs + (uint64_t)(((lo - q + 2) * 512) >> 4),
-                                 n == 1 ? idesc16 : (n == 2 ? idesc32 : idesc48), 1u);
+                        mma(lo, hi, 1u);
                     }
                 }
             }
@@ -463,14 +464,31 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
             if(!role_wait(&tfull[acc], aph, abort_flag, status, 6)) break;
             tc_fence_after();
             const Brick bk = brick_of(g, tile, tx, ty, per_sample);
-            const int x = bk.x0 + (m & 15), y = bk.y0 + (m >> 4);
+            // row m is staged point (xi, yi) of the plane; xi = 0 and kTX - 1
+            // are the halo columns
+            const int xi = m % kTX;
+            const int x = bk.x0 - 1 + xi, y = bk.y0 + m / kTX;
+            const bool halo = xi == 0 || xi == kTX - 1;
 #pragma unroll 1
             for(int mt = 0; mt < kTZ; ++mt)
             {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(acc * kAccCols + mt * 16), v);
+                // out(x) = D_{dx=-1}[x - 1] + D_{dx=0}[x] + D_{dx=+1}[x + 1]: rows
+                // x +- 1 are the neighbouring lanes of the same 16-lane line
+                float dm[16], dc[16], dp[16], v[16];
+                const uint32_t ta =
+                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(acc * kAccCols + mt * kPlaneCols);
+                tmem_ld16(ta, dm);
+                tmem_ld16(ta + kNetCh, dc);
+                tmem_ld16(ta + 2 * kNetCh, dp);
+#pragma unroll
+                for(int c = 0; c < 16; ++c)
+                {
+                    const float left = __shfl_up_sync(0xffffffffu, dm[c], 1);
+                    const float right = __shfl_down_sync(0xffffffffu, dp[c], 1);
+                    v[c] = (left + dc[c]) + right;
+                }
                 const int z = bk.z0 + mt;
-                if(x >= g.nx || y >= g.ny || z >= g.nz) continue;
+                if(halo || x >= g.nx || y >= g.ny || z >= g.nz) continue;
                 const long p = (((long)bk.b * g.nz + z) * g.ny + y) * g.nx + x;
                 if constexpr(kOut == kOutReluBf16 || kOut == kOutMaskBf16)
                 {
@@ -1430,7 +1448,7 @@ static int bf16_box_map(const ConvGrid& g, const void* in, int bx, int by, int b
     return 0;
 }
 
-// The conv brick box: 16 x 10 x 6 points (x without halo: three shifted loads).
+// The conv brick box: 16 x 10 x 6 points (14 x 8 x 4 outputs and their halo).
 static int conv_tensor_map(const ConvGrid& g, const void* in, CUtensorMap* map)
 {
     return bf16_box_map(g, in, kTX, kHY, kHZ, map);
@@ -1448,7 +1466,7 @@ static int conv_launch(const ConvGrid& g, const void* in, const void* wB, void* 
     }
     CUtensorMap map;
     HB_RETURN_IF(conv_tensor_map(g, in, &map));
-    const long tiles = (long)g.nb * ((g.nx + kTX - 1) / kTX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ);
+    const long tiles = (long)g.nb * ((g.nx + kOX - 1) / kOX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ);
     const long cap = (long)HB_CONV_CTAS * sm_count();
     const int grid = (int)(tiles < cap ? tiles : cap);
     k_conv16<kOut><<<grid, kConvThreads, kConvSmem, s>>>(map, g, (const __nv_bfloat16*)wB, out,
