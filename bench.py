@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
-    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256", "mixed320"],
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256", "mixed320", "net64"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--largest", action="store_true",
                     help="also run configs[4]: 560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs")
@@ -674,6 +674,18 @@ def run_profile_case(case: str) -> int:
     elif case == "sweep128":
         P = R.Problem(128)
         print(json.dumps({"symgs_sweep_ms": P.time_op("symgs_sweep", 2)}))
+    elif case == "net64":
+        # the learned smoother's evaluation on one 64^3 sample, both odd branches
+        # (layer 1 and layer 3 in their one-channel tensor-core forms)
+        from rochpcg_b200 import learned as LS
+
+        S = LS.Smoother.load()
+        g = torch.Generator(device="cuda").manual_seed(3)
+        r = torch.randn(64 ** 3, device="cuda", generator=g)
+        for _ in range(3):
+            y = S.forward(r, (64, 64, 64), 1)
+        torch.cuda.synchronize()
+        print(json.dumps({"net64_norm": float(y.norm())}))
     elif case == "mixed320":
         # one mixed V-cycle + one stencil SpMV at 320^3 (eager launches)
         P = R.Problem(320)
