@@ -587,8 +587,9 @@ def learned_comparison(args, R, barrier, steps=2):
     meta = S.meta
     conv = conv_kernel_timing(2, n >> 2)  # level 2, both branches of the odd evaluation
     peak = measured_bf16_peak()
-    res["conv_kernel"] = dict(conv, kernel="k_conv16 (layer 2, 16->16, tcgen05 M128 K16, dz taps stacked in N<=48, TMA-pipelined)",
-                              bound="tensor", peak_tflops=peak, frac=conv["tflops"] / peak if peak else None)
+    label = "k_conv16 (layer 2, 16->16, tcgen05 M128 K16, dz and dx taps stacked in N<=144, one TMA box per brick)"
+    res["conv_kernel"] = dict(conv, kernel=label, bound="tensor", peak_tflops=peak,
+                              frac=conv["tflops"] / peak if peak else None)
     res["weights"] = {"file": "rochpcg_b200/weights/smoother_l23.npz", "sha256": meta.get("sha256"),
                       "symmetry": meta.get("symmetry"), "heldout": meta.get("heldout"),
                       "training": {k: meta.get("training", {}).get(k) for k in ("epochs", "loss", "lr0", "lr1")}}
