@@ -517,10 +517,11 @@ __device__ __forceinline__ void load4(const T* x, int base, int m, int s, T (&v)
     else { v[0] = a[3]; v[1] = b[0]; v[2] = b[1]; v[3] = b[2]; }
 }
 
-// Slots whose loads are issued together before their in-order adds: 3 on
-// large levels (keeps registers low, occupancy high), all 27 (FP32) or 9
-// (FP64) on small levels (few threads: fewer round trips).
-constexpr int kV4GroupLarge = 3, kV4GroupSmall = 27, kV4GroupSmall64 = 9;
+// Slots whose loads are issued together before their in-order adds: 5 on
+// large levels (keeps registers low, occupancy high; 320^3 mixed V-cycle 1.43
+// ms with 3, 1.39 ms with 5, 1.42 ms with 9), all 27 (FP32) or 9 (FP64) on
+// small levels (few threads: fewer round trips).
+constexpr int kV4GroupLarge = 5, kV4GroupSmall = 27, kV4GroupSmall64 = 9;
 constexpr int kV4SmallRows = 1 << 17;  // rows per colour below which a level counts as small
 
 template <int kSel, int kGroup, typename T>
