@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256", "mixed320", "net64"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--largest", action="store_true",
-                    help="also run configs[4]: 560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs")
+                    help="also run the largest workload: 560x560x280, FP64 vs mixed vs learned, "
+                         "seed-7 and all-ones rhs")
     ap.add_argument("--learned-nx", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
@@ -445,9 +446,9 @@ def run_ours(args):
 
 
 def mixed_comparison(args, R, barrier, steps=2, warmup=1):
-    """FP64-outer / FP32 V-cycle vs plain FP64 on the same n^3
-    system with b ~ N(0,1) (seed 0), both to args.tol, both verified with an
-    FP64 true residual."""
+    """Mixed precision (320^3 by default): FP64-outer / FP32 V-cycle vs plain
+    FP64 on the same n^3 system with b ~ N(0,1) (seed 0), both to args.tol,
+    both verified with an FP64 true residual."""
     from rochpcg_b200.rhs import normal_rhs
 
     n3 = args.mixed_nx
@@ -542,7 +543,7 @@ def R_load():
 
 
 def learned_comparison(args, R, barrier, steps=2):
-    """levels 2-3 SymGS replaced by the trained conv net (committed
+    """Learned smoother (256^3 by default): levels 2-3 SymGS replaced by the trained conv net (committed
     weights), flexible CG with fallback, vs the plain FP32 V-cycle and FP64, on
     an n^3 system with b ~ N(0,1) (seed 9999), all to args.tol."""
     from rochpcg_b200 import learned as LS
@@ -599,7 +600,7 @@ def learned_comparison(args, R, barrier, steps=2):
 
 
 def largest_comparison(args, R, barrier):
-    """560 x 560 x 280 (87.8M rows), FP64 outer CG with the FP32
+    """Largest workload: 560 x 560 x 280 (87.8M rows), FP64 outer CG with the FP32
     V-cycle and the learned level-2/3 smoother, against plain mixed and FP64,
     for b ~ N(0,1) seed 7 and for the generated b (exact solution ones), all to
     args.tol verified in FP64; fine-level bandwidth from the HPCG byte model

@@ -141,7 +141,7 @@ int TestSymmetry_B200(SparseMatrix& A, Vector& b, Vector& xexact, TestSymmetryDa
     ierr |= ComputeDotProduct(nrow, y_ncol, z_ncol, ytMinvx, t4, opt_flag);
     d.depsym_mg = std::fabs((long double)(xtMinvy - ytMinvx)) / ((xNorm2 * ANorm * yNorm2 + yNorm2 * ANorm * xNorm2) * (DBL_EPSILON));
     // an FP32 V-cycle is symmetric to single-precision rounding: the same
-    // departure (still reported in DBL_EPSILON units) is judged at FLT_EPSILON
+    // departure (still reported in DBL_EPSILON units) is held to FLT_EPSILON
     const double mg_limit = needs_flexible(prec) ? (double)FLT_EPSILON / DBL_EPSILON : 1.0;
     if(d.depsym_mg > mg_limit) ++d.count_fail;
 

@@ -149,7 +149,7 @@ def test_solve_host_recovers_exact_solution():
 
 
 def test_cg_256_full_size_properties():
-    """configs[1] size: converges to 1e-9 in FP64 (verified with the true
+    """256^3, the FP64 benchmark workload: converges to 1e-9 in FP64 (verified with the true
     residual), recovers x* = 1, and beats the 50-iteration CG_ref residual
     of the reference within its check_niter bound when that golden exists."""
     import rochpcg_b200 as R

@@ -1,5 +1,5 @@
 """Device problem generation and optimization vs the CPU restatement:
-every index array bit-exact (north_star (d)), values exact."""
+every index array bit-exact, values exact."""
 import numpy as np
 import pytest
 
