@@ -73,7 +73,10 @@ def abs_bound(dims, nb, x, w):
     return oracle_conv(dims, nb, np.abs(x), np.abs(w))
 
 
-GRIDS = [((2, 8, 16), 1), ((5, 12, 20), 3), ((3, 3, 3), 2), ((1, 1, 40), 1), ((16, 16, 16), 2), ((9, 17, 33), 1)]
+# (z, y, x) extents: partial bricks in every dimension, x across the 14-point
+# brick stride (16, 20, 33, 40) and on it (14, 28)
+GRIDS = [((2, 8, 16), 1), ((5, 12, 20), 3), ((3, 3, 3), 2), ((1, 1, 40), 1), ((16, 16, 16), 2), ((9, 17, 33), 1),
+         ((4, 8, 28), 2), ((6, 10, 14), 1)]
 
 
 @pytest.mark.parametrize("dims,nb", GRIDS)

@@ -45,7 +45,7 @@ def test_normal_rhs_device_matches_python():
 
 
 @pytest.mark.parametrize("dims,nb,odd", [((6, 9, 20), 2, False), ((16, 16, 16), 1, False), ((8, 8, 8), 4, False),
-                                         ((6, 9, 20), 2, True), ((16, 16, 16), 1, True)])
+                                         ((6, 9, 20), 2, True), ((16, 16, 16), 1, True), ((5, 17, 28), 1, True)])
 def test_forward_matches_oracle(dims, nb, odd):
     rng = np.random.default_rng(1)
     per = int(np.prod(dims))
