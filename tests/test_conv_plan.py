@@ -1,10 +1,11 @@
-"""CPU restatement of the tcgen05 convolution's issue plan and data layout
-(rochpcg_b200/csrc/learned.cu, k_conv16): the weight slot order, the MMAs per
-(staged plane, row shift) with the dz and dx taps stacked in N, their
+"""CPU restatement of the tcgen05 network kernels' issue plans and data
+layouts (rochpcg_b200/csrc/learned.cu).  k_conv16: the weight slot order, the
+MMAs per (staged plane, row shift) with the dz and dx taps stacked in N, their
 accumulate flags, the shared-memory and TMEM ranges they touch, and the
 epilogue's combination of the dx blocks of neighbouring rows -- checked
 exhaustively for brick depths 1-5 and numerically against a direct 3x3x3
-convolution of one brick."""
+convolution of one brick.  k_layer3_tc: taps stacked in N, the odd pair folded
+into K, the 27-term gather.  k_layer1_tc: the im2col layout and product."""
 import numpy as np
 import pytest
 
@@ -93,4 +94,86 @@ def test_plan_and_epilogue_equal_a_direct_convolution(ktz):
             dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
             src = box[mt + 1 + dz, 1 + dy:1 + dy + KTY, 1 + dx:1 + dx + 14, :]
             want += src @ w[t]
+        assert np.allclose(got, want, rtol=1e-12, atol=1e-12)
+
+
+# ---- the one-channel layers (k_layer3_tc, k_layer1_tc)
+
+K3X, K3Y, K3Z = 16, 8, 2                     # layer-3 output brick
+K3HX, K3HY, K3HZ = K3X + 2, K3Y + 2, K3Z + 2  # its staged box, 720 points
+K3N = 32                                      # 27 taps + 5 zero columns
+
+
+def test_layer3_tap_stacking_and_pair_folding_equal_the_odd_conv():
+    """D[p][t] = sum_c a[p][c] w[t][c] over the staged points (pair folded into
+    K with the weights halved and negated), then y[o] = sum_t D[o + off_t][t]
+    in tap order, equals (conv(a+) - conv(a-)) / 2 on the brick's outputs."""
+    rng = np.random.default_rng(3)
+    rows = K3HX * K3HY * K3HZ
+    chunks = (rows + 127) // 128
+    assert chunks * 128 >= rows and chunks * K3N * 2 <= 512          # two accumulators fit TMEM
+    pos = rng.standard_normal((K3HZ, K3HY, K3HX, CH))
+    neg = rng.standard_normal((K3HZ, K3HY, K3HX, CH))
+    w = rng.standard_normal((27, CH))                               # w3[t][ci][0]
+    B = np.zeros((K3N, CH))
+    B[:27] = 0.5 * w
+    D = pos.reshape(rows, CH) @ B.T + neg.reshape(rows, CH) @ (-B).T
+    got = np.zeros((K3Z, K3Y, K3X))
+    for oz in range(K3Z):
+        for oy in range(K3Y):
+            for ox in range(K3X):
+                s = 0.0
+                for t in range(27):
+                    dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+                    r = ((oz + 1 + dz) * K3HY + (oy + 1 + dy)) * K3HX + (ox + 1 + dx)
+                    assert 0 <= r < rows
+                    s += D[r, t]
+                got[oz, oy, ox] = s
+    want = np.zeros((K3Z, K3Y, K3X))
+    for t in range(27):
+        dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+        sl = (slice(1 + dz, 1 + dz + K3Z), slice(1 + dy, 1 + dy + K3Y), slice(1 + dx, 1 + dx + K3X))
+        want += 0.5 * (pos[sl] @ w[t] - neg[sl] @ w[t])
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-12)
+
+
+def k1_off(r, c8):
+    """Byte offset of im2col row r, 8-element K chunk c8 (k_layer1_tc)."""
+    return (r >> 3) * 512 + c8 * 128 + (r & 7) * 16
+
+
+def test_layer1_im2col_layout_tiles_its_plane():
+    """128 rows x 4 K chunks of 16 bytes fill one 8 KB plane exactly once; the
+    MMA's K halves start 256 B apart with LBO 128 and SBO 512; the 16 x 32
+    weight operand ends at 1 KB."""
+    offs = sorted(k1_off(r, c) for r in range(128) for c in range(4))
+    assert offs == list(range(0, 8192, 16))
+    for r in range(128):
+        for c in range(4):
+            kh, cc = divmod(c, 2)
+            assert k1_off(r, c) == kh * 256 + (r >> 3) * 512 + cc * 128 + (r & 7) * 16
+    assert max(k1_off(co, t >> 3) + (t & 7) * 2 for co in range(16) for t in range(32)) == 1022
+
+
+def test_layer1_im2col_product_equals_the_conv():
+    """Each row = the 27 neighbours of its point (5 zero taps); the K = 32
+    product with w1[t][0][co] gives layer 1's 16 pre-activations."""
+    rng = np.random.default_rng(4)
+    hz, hy, hx = 6, 10, 18
+    field = rng.standard_normal((hz, hy, hx))
+    w = rng.standard_normal((27, CH))
+    Bw = np.zeros((32, CH))
+    Bw[:27] = w
+    for q in range(4):
+        A = np.zeros((128, 32))
+        for m in range(128):
+            mx, my = m % 16, m // 16
+            for t in range(27):
+                dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+                A[m, t] = field[q + 1 + dz, my + 1 + dy, mx + 1 + dx]
+        got = (A @ Bw).reshape(8, 16, CH)
+        want = np.zeros((8, 16, CH))
+        for t in range(27):
+            dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+            want += field[q + 1 + dz, 1 + dy:9 + dy, 1 + dx:17 + dx][..., None] * w[t]
         assert np.allclose(got, want, rtol=1e-12, atol=1e-12)
