@@ -22,6 +22,13 @@ device time).  The same line carries:
   learned      the learned coarse-level smoother vs SymGS at 256^3
                (b ~ N(0,1), seed 9999), with the tcgen05 conv kernel's
                tensor roofline
+  largest      560 x 560 x 280 (87.8M rows), FP64 vs mixed vs learned, for
+               b ~ N(0,1) seed 7 and the generated b, with the fine-level
+               sweep bandwidths
+  every solve's final x is also checked on the host with the reference's
+  own ComputeSPMV_ref (oracle/_ref, natural order) in a worker process that
+  runs beside the GPU work: `rel_residual_ref_spmv` next to each
+  `rel_residual_fp64_true`
 
 `--impl reference` times the reference's CPU CG_ref on this machine instead.
 Under torchrun (N>1) every rank solves its own local problem (HPCG weak
@@ -64,11 +71,13 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
-    ap.add_argument("--profile-case", choices=["conv", "sweep128", "vcycle256", "mixed320", "net64"],
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "vcycle256", "mixed320",
+                                               "net64"],
                     help="run one small case for a profiler and exit (no JSON line)")
-    ap.add_argument("--largest", action="store_true",
-                    help="also run the largest workload: 560x560x280, FP64 vs mixed vs learned, "
-                         "seed-7 and all-ones rhs")
+    ap.add_argument("--no-largest", action="store_true",
+                    help="skip the largest workload (560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs)")
+    ap.add_argument("--no-refcheck", action="store_true",
+                    help="skip the host check of each solve's x with the reference's ComputeSPMV_ref")
     ap.add_argument("--learned-nx", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
@@ -186,19 +195,95 @@ def profile_traffic(key: str):
     return None
 
 
-def cpu_baseline_sample(n: int, iters: int):
-    """The reference's CPU CG_ref (OpenMP, all host threads) on an n^3 sample."""
+def fp64_algorithmic_bytes_per_iter(rows_per_level):
+    """Bytes one FP64 MG-PCG iteration of this implementation must move (the
+    per-kernel algorithmic bytes, not the reference's traffic model), per
+    level of m rows in 8 colours of m/8 rows, ELL width 27 (12 B per slot):
+
+      zero-guess SymGS (8 forward + 7 backward colour launches): every slot
+        but the diagonal read once (26 * 12); forward r, 1/a_ii, diag index,
+        x written (28); backward (7 of 8 colours) diag index, x, a_ii,
+        1/a_ii, x written (36 * 7/8); neighbour x of earlier / later colours,
+        read once per launch (28 + 28)                        = 427.5 B/row
+      fused SpMV + restriction (m/8 rows): 27 * 12 + rf + rc + two transfer
+        indices (348 / 8), x of the whole fine grid once (8)     = 51.5 B/row
+      prolongation (m/8 rows): indices, xc, xf read + written (32 / 8) = 4
+      full SymGS (15 colour launches): per launch m/8 rows of
+        27 * 12 + r + 1/a_ii + x written (348 / 8) + the other colours' x (7)
+                                                                 = 757.5 B/row
+      coarsest level: the zero-guess SymGS only                  = 427.5 B/row
+      level 0 also: SpMV + p.Ap (27 * 12 + p + Ap = 340), r.z (16), p update
+        (24), r and x update (48)                                 = 428 B/row
+    """
+    total = 0.0
+    last = len(rows_per_level) - 1
+    for l, m in enumerate(rows_per_level):
+        per_row = 427.5 if l == last else 427.5 + 51.5 + 4.0 + 757.5
+        if l == 0:
+            per_row += 340.0 + 16.0 + 24.0 + 48.0
+        total += per_row * m
+    return total
+
+
+def cpu_facts():
+    """Model name and core counts of the host the CPU figures ran on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        import psutil
+
+        physical = psutil.cpu_count(logical=False)
+    except Exception:
+        physical = None
+    return {"cpu_model": model, "physical_cores": physical, "logical_cpus": os.cpu_count()}
+
+
+def cpu_baseline_sample(n: int, iters: int, min_seconds: float = 0.0):
+    """The reference's CPU CG_ref (OpenMP, all host threads) on an n^3 sample:
+    `iters` iterations from x0 = 0 on the generated b, repeated until at least
+    min_seconds of solve time have been measured.  Returns (GFLOP/s, seconds
+    per solve, iterations, solves)."""
     from oracle.oracle import RefProblem
 
     R = RefProblem(n, n, n)
-    r = R.cg(iters, 0.0)
     flops, _ = model(n)
-    gflops = flops * r["niters"] / r["seconds"] / 1e9
-    return gflops, r["seconds"], r["niters"]
+    secs, its, solves = 0.0, 0, 0
+    while solves == 0 or secs < min_seconds:
+        r = R.cg(iters, 0.0)
+        secs += r["seconds"]
+        its = r["niters"]
+        solves += 1
+    per = secs / solves
+    return flops * its / per / 1e9, per, its, solves
 
 
 def host_threads():
     return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def cpu_baseline(args):
+    """configs[0] (32^3, 50 CG_ref iterations, generated b, x0 = 0) is the
+    primary CPU figure, repeated for about 10 s; a 128^3 x 10-iteration sample
+    shows the reference at a size whose working set leaves the caches."""
+    facts = cpu_facts()
+    out = {"unit": "GFLOP/s", "cores": host_threads(), "kind": "reference", **facts}
+    try:
+        g, per, its, solves = cpu_baseline_sample(32, 50, min_seconds=10.0)
+        out.update(value=g, sample=f"CG_ref (reference src/*_ref.cpp, OpenMP, {host_threads()} threads) on 32^3 "
+                                   f"(the reference's CPU-runnable case): {its} iterations from x0=0, generated b, "
+                                   f"{solves} solves of {per * 1e3:.1f} ms")
+        g2, per2, its2, _ = cpu_baseline_sample(128, 10)
+        out["sample_128"] = {"value": g2, "unit": "GFLOP/s", "iterations": its2, "seconds": per2}
+    except Exception as e:
+        out.update(value=None, sample=f"unavailable: {e}")
+    return out
 
 
 # ------------------------------------------------------------ reference arm
@@ -236,7 +321,8 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (HPCG generator)", "impl": "reference",
         "config": {"workload": f"HPCG {nx}^3 FP64 MG-PCG (4 levels), generated b, x0=0", "grid": [nx, nx, nx],
                    "mg_levels": 4, "parallelism": "replicas"},
-        "cpu_baseline": {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample,
+                         **cpu_facts()},
         "e2e": {"value": gflops, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "setup_s": setup_s,
     }
@@ -291,6 +377,19 @@ def job_gflops(world: int, flops_per_iter: float, iters: int, seconds_per_step: 
 
 # ------------------------------------------------------------------ our arm
 
+def attach_ref_residuals(obj, values: dict, errors: dict):
+    """Replace every `ref_check_tag` in the result tree by the residual the
+    reference-operator checker returned for it (`rel_residual_ref_spmv`)."""
+    if isinstance(obj, dict):
+        tag = obj.pop("ref_check_tag", None)
+        if tag is not None:
+            obj["rel_residual_ref_spmv"] = values.get(tag)
+            if tag in errors:
+                obj["ref_check_error"] = errors[tag]
+        for v in obj.values():
+            attach_ref_residuals(v, values, errors)
+
+
 def run_ours(args):
     import torch
     import rochpcg_b200 as R
@@ -313,8 +412,25 @@ def run_ours(args):
         return run_mixed_only(args, R, barrier)
 
     nx = args.nx
+    grid = (nx, nx, nx)
+    # host-side check of every solve with the reference's own SpMV (rank 0):
+    # the worker builds the reference problem while the GPU works
+    checker = None
+    if rank == 0 and not args.lite and not args.no_refcheck:
+        from oracle.residual_check import RefResidualChecker
+
+        checker = RefResidualChecker(threads=max(1, host_threads() // 2))
+        checker.prepare(grid)
+
+    def refcheck(tag, grid_, rhs, x_natural):
+        if checker is not None:
+            checker.submit(tag, grid_, rhs, x_natural)
+            return tag
+        return None
+
     P = R.Problem(nx)
     flops_it, bytes_it = P.model()
+    alg_bytes_it = fp64_algorithmic_bytes_per_iter(P.rows)
     m = P.rows[0]
     stream = torch.cuda.ExternalStream(P.stream_handle)
 
@@ -339,6 +455,7 @@ def run_ours(args):
     value = job_gflops(world, flops_it, iters, ms_step * 1e-3)
     rel = runs[-1]["normr"] / runs[-1]["normr0"]
     true_rel = P.true_residual()
+    fp64_tag = refcheck("fp64_256", grid, ("generated",), P.get_x()) if checker else None
     kpi = P.kernels_per_iteration(R.MODE_FP64)
     launches = args.steps * (iters * kpi + 2)
 
@@ -363,6 +480,7 @@ def run_ours(args):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     e2e_val = job_gflops(world, flops_it, re["niters"], e2e_s)
     x_err = float(torch.max(torch.abs(x_host - 1.0)))
+    e2e_tag = refcheck("e2e_fp64_256", grid, ("generated",), x_host.numpy().copy())
 
     # ---- dominant kernel: level-0 full SymGS colour sweep
     nb = P.nblocks[0]
@@ -378,6 +496,7 @@ def run_ours(args):
     spmv_ms = P.time_op("spmv", 20)
     spmv_bytes = m * (27 * 12 + 8 + 8)
     extra_kernels = {"spmv_GBps": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "spmv_ms": spmv_ms,
+                     "spmv_traffic": profile_traffic(f"spmv_{nx}"), "spmv_algorithmic_bytes_per_launch": spmv_bytes,
                      "mg_ms": P.time_op("mg", 5)}
 
     # ---- the same solve on the implicit stencil: FP64 history bit for bit, no matrix reads
@@ -391,6 +510,8 @@ def run_ours(args):
                    "gflops_hpcg_model": flops_it * s_runs[-1]["niters"] / s_min / 1e9,
                    "history_bitwise_equal_to_fp64": bool(np.array_equal(s_runs[-1]["hist"], runs[-1]["hist"])),
                    "speedup_vs_fp64_ell": ms_step * 1e-3 / s_min,
+                   "rel_residual_fp64_true": P.true_residual(),
+                   "ref_check_tag": refcheck("fp64_stencil_256", grid, ("generated",), P.get_x()),
                    "mg_ms": P.time_op("mg_stencil", 5)}
     P.close()
     del P
@@ -398,29 +519,38 @@ def run_ours(args):
     # ---- mixed precision vs FP64 at 320^3, b ~ N(0,1) seed 0
     mixed = None
     if not args.no_mixed:
-        mixed = mixed_comparison(args, R, barrier)
+        mixed = mixed_comparison(args, R, barrier, refcheck=refcheck, checker=checker)
 
     # ---- learned coarse-level smoother vs SymGS at 256^3, b ~ N(0,1) seed 9999
     learned = None
     if not args.no_learned:
-        learned = learned_comparison(args, R, barrier)
+        learned = learned_comparison(args, R, barrier, refcheck=refcheck)
 
-    largest = largest_comparison(args, R, barrier) if args.largest else None
+    # ---- the largest configuration, 560 x 560 x 280
+    largest = None
+    if not args.no_largest:
+        if checker is not None:
+            # free the smaller reference problems before the 87.8M-row one
+            checker.drop(grid)
+            checker.drop((args.mixed_nx,) * 3)
+            checker.drop((args.learned_nx,) * 3)
+        largest = largest_comparison(args, R, barrier, refcheck=refcheck, checker=checker)
 
-    # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1)
+    ref_values, ref_errors = {}, {}
+    if checker is not None:
+        ref_values = checker.results()
+        ref_errors = dict(checker.errors)
+        checker.close()
+
+    # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1),
+    # after the checker has exited so that nothing else uses the host cores
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            n_cpu, it_cpu = 128, 10
-            g, secs, its = cpu_baseline_sample(n_cpu, it_cpu)
-            cpu = {"value": g, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
-                   "sample": f"CG_ref (reference src/*_ref.cpp, OpenMP) on {n_cpu}^3, {its} iterations from x0=0, "
-                             f"{secs:.2f} s"}
-        except Exception as e:
-            cpu = {"value": None, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
-                   "sample": f"unavailable: {e}"}
+        cpu = cpu_baseline(args)
 
     if rank == 0:
+        peak_gbs = measured_peak()[0]
+        alg_gbps = world * alg_bytes_it * iters / (ms_step * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -430,28 +560,43 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (level-0 ELL is %.1f GB)" % (27 * 12 * m / 1e9),
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "time_to_solution_s": ms_step * 1e-3, "iterations": iters, "rel_residual": rel,
-            "rel_residual_fp64_true": true_rel, "hpcg_model_bytes_per_iter": bytes_it,
-            "model_GBps": world * bytes_it * iters / (ms_step * 1e-3) / 1e9,
+            "rel_residual_fp64_true": true_rel, "ref_check_tag": fp64_tag,
+            # this implementation's bytes per iteration (per-kernel algorithmic
+            # bytes) and the bandwidth they imply
+            "algorithmic_bytes_per_iter": alg_bytes_it,
+            "algorithmic_GBps": alg_gbps, "algorithmic_frac_of_hbm": alg_gbps / world / peak_gbs,
+            # the reference's traffic model (src/ReportResults.cpp:163-195):
+            # charges two matrix passes to the zero-guess smoother and nnz*8
+            # bytes of writes to the residual and post-smoother, so it is an
+            # accounting figure, not a bandwidth
+            "hpcg_traffic_model_bytes_per_iter": bytes_it,
+            "hpcg_traffic_model_GBps_not_a_bandwidth": world * bytes_it * iters / (ms_step * 1e-3) / 1e9,
             "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m,
-                    "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err},
+                    "seconds_per_step": e2e_s, "max_abs_x_minus_1": x_err, "ref_check_tag": e2e_tag},
             "roofline": roofline, "kernels": extra_kernels, "fp64_stencil": stencil, "cpu_baseline": cpu,
             "mixed": mixed,
             "learned": learned, "largest": largest,
             "gpu_launches": launches, "clocks": clocks,
         }
+        attach_ref_residuals(line, ref_values, ref_errors)
+        line["ref_spmv_check"] = ("every solve's final x checked on the host with the reference's ComputeSPMV_ref "
+                                  "(oracle/_ref, natural order): rel_residual_ref_spmv = ||b - A x|| / ||b||"
+                                  if checker is not None else "skipped")
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
 
 
-def mixed_comparison(args, R, barrier, steps=2, warmup=1):
+def mixed_comparison(args, R, barrier, steps=2, warmup=1, refcheck=None, checker=None):
     """Mixed precision (320^3 by default): FP64-outer / FP32 V-cycle vs plain
     FP64 on the same n^3 system with b ~ N(0,1) (seed 0), both to args.tol,
     both verified with an FP64 true residual."""
     from rochpcg_b200.rhs import normal_rhs
 
     n3 = args.mixed_nx
+    if checker is not None:
+        checker.prepare((n3, n3, n3))
     Q = R.Problem(n3)
     Q.set_rhs(normal_rhs(Q.rows[0], 0))
     f3, _ = Q.model()
@@ -477,6 +622,8 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
                      "rel_residual_fp64_true": Q.true_residual(),
                      "gflops_hpcg_model": f3 * r3["niters"] / min(ts) / 1e9,
                      "kernels_per_iteration": Q.kernels_per_iteration(mode)}
+        if refcheck is not None:
+            res[name]["ref_check_tag"] = refcheck(f"mixed{n3}_{name}", (n3, n3, n3), ("normal", 0), Q.get_x())
         if mode == R.MODE_LEARNED:
             res[name]["fallback_iteration"] = Q.last_fallback()
             Q.set_smoother(None)
@@ -494,8 +641,12 @@ def mixed_comparison(args, R, barrier, steps=2, warmup=1):
     sw_bytes = rows_c * (4 + 4 + 4) + (m3 - rows_c) * 4
     sp = Q.time_op("spmv_stencil", 10)
     sp_bytes = m3 * (8 + 8 + 8)
+    spm = Q.time_op("spmv_mixed", 10)
     res["kernels"] = {"k32_sweep_ms": sw, "k32_sweep_GBps": sw_bytes / (sw * 1e-3) / 1e9,
                       "k32_sweep_algorithmic_bytes": sw_bytes,
+                      # the mixed CG's outer operator (separable sum)
+                      "k64_spmv_sep_ms": spm, "k64_spmv_sep_GBps": sp_bytes / (spm * 1e-3) / 1e9,
+                      # the ELL-ordered stencil product of the FP64 stencil mode
                       "k64_spmv_stencil_ms": sp, "k64_spmv_stencil_GBps": sp_bytes / (sp * 1e-3) / 1e9,
                       "mg_mixed_ms": Q.time_op("mg_mixed", 5), "mg_fp64_ms": Q.time_op("mg", 3),
                       "mg_fp64_stencil_ms": Q.time_op("mg_stencil", 5)}
@@ -542,7 +693,7 @@ def R_load():
     return R.load()
 
 
-def learned_comparison(args, R, barrier, steps=2):
+def learned_comparison(args, R, barrier, steps=2, refcheck=None):
     """Learned smoother (256^3 by default): levels 2-3 SymGS replaced by the trained conv net (committed
     weights), flexible CG with fallback, vs the plain FP32 V-cycle and FP64, on
     an n^3 system with b ~ N(0,1) (seed 9999), all to args.tol."""
@@ -568,6 +719,8 @@ def learned_comparison(args, R, barrier, steps=2):
                      "rel_residual_fp64_true": Q.true_residual(),
                      "gflops_hpcg_model": f * r["niters"] / min(ts) / 1e9,
                      "kernels_per_iteration": Q.kernels_per_iteration(mode)}
+        if refcheck is not None:
+            res[name]["ref_check_tag"] = refcheck(f"learned{n}_{name}", (n, n, n), ("normal", 9999), Q.get_x())
         if mode == R.MODE_LEARNED:
             res[name]["fallback_iteration"] = Q.last_fallback()
             res[name]["vcycle_ms"] = Q.time_op("mg_learned", 10)
@@ -582,6 +735,9 @@ def learned_comparison(args, R, barrier, steps=2):
     res["learned_first_increase_fallback"] = {"time_to_1e-9_s": r["seconds"], "iterations": r["niters"],
                                               "fallback_iteration": Q.last_fallback(),
                                               "rel_residual_fp64_true": Q.true_residual()}
+    if refcheck is not None:
+        res["learned_first_increase_fallback"]["ref_check_tag"] = refcheck(
+            f"learned{n}_first_increase", (n, n, n), ("normal", 9999), Q.get_x())
     Q.set_fallback()
     Q.set_smoother(None)
     Q.close()
@@ -599,7 +755,7 @@ def learned_comparison(args, R, barrier, steps=2):
     return res
 
 
-def largest_comparison(args, R, barrier):
+def largest_comparison(args, R, barrier, refcheck=None, checker=None):
     """Largest workload: 560 x 560 x 280 (87.8M rows), FP64 outer CG with the FP32
     V-cycle and the learned level-2/3 smoother, against plain mixed and FP64,
     for b ~ N(0,1) seed 7 and for the generated b (exact solution ones), all to
@@ -608,8 +764,12 @@ def largest_comparison(args, R, barrier):
     from rochpcg_b200 import learned as LS
     from rochpcg_b200.rhs import normal_rhs
 
-    Q = R.Problem(560, 560, 280)
+    grid = (560, 560, 280)
+    if checker is not None:
+        checker.prepare(grid)
+    Q = R.Problem(*grid)
     f, bytes64 = Q.model()
+    alg64 = fp64_algorithmic_bytes_per_iter(Q.rows)
     m = Q.rows[0]
     S = LS.Smoother.load()
     out = {"grid": [560, 560, 280], "rows": m}
@@ -625,8 +785,12 @@ def largest_comparison(args, R, barrier):
             res[name] = {"time_to_1e-9_s": r["seconds"], "iterations": r["niters"],
                          "rel_residual_fp64_true": Q.true_residual(),
                          "gflops_hpcg_model": f * r["niters"] / r["seconds"] / 1e9}
+            if refcheck is not None:
+                res[name]["ref_check_tag"] = refcheck(f"largest_{rhs}_{name}", grid,
+                                                      ("normal", 7) if rhs == "seed7" else ("generated",), Q.get_x())
             if mode == R.MODE_FP64:
-                res[name]["model_GBps"] = bytes64 * r["niters"] / r["seconds"] / 1e9
+                res[name]["algorithmic_GBps"] = alg64 * r["niters"] / r["seconds"] / 1e9
+                res[name]["hpcg_traffic_model_GBps_not_a_bandwidth"] = bytes64 * r["niters"] / r["seconds"] / 1e9
             if mode == R.MODE_LEARNED:
                 res[name]["fallback_iteration"] = Q.last_fallback()
                 Q.set_smoother(None)
@@ -676,6 +840,14 @@ def run_profile_case(case: str) -> int:
     elif case == "sweep128":
         P = R.Problem(128)
         print(json.dumps({"symgs_sweep_ms": P.time_op("symgs_sweep", 2)}))
+    elif case == "spmv128":
+        # the FP64 ELL SpMV at 128^3 (2.1M rows, 680 MB of ELL)
+        P = R.Problem(128)
+        print(json.dumps({"spmv_ms": P.time_op("spmv", 2)}))
+    elif case == "mixed128":
+        # the mixed path's level-0 kernels at 128^3: separable outer SpMV, FP32 colour sweeps
+        P = R.Problem(128)
+        print(json.dumps({"spmv_mixed_ms": P.time_op("spmv_mixed", 2), "symgs32_sweep_ms": P.time_op("symgs32_sweep", 1)}))
     elif case == "net64":
         # the learned smoother's evaluation on one 64^3 sample, both odd branches
         # (layer 1 and layer 3 in their one-channel tensor-core forms)

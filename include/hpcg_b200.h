@@ -41,6 +41,7 @@ extern "C" {
 #define HPCGB200_ERR_NOT_STENCIL 5    /* matrix is not the 27-point HPCG stencil (implicit paths) */
 #define HPCGB200_ERR_DEVICE_STATUS 6  /* a device-side check failed (status word set) */
 #define HPCGB200_ERR_NO_DEVICE 7      /* no CUDA device visible */
+#define HPCGB200_ERR_NONFINITE 8      /* a solve ended with a non-finite residual (outputs are filled) */
 
 #define HPCGB200_WIDTH 27
 #define HPCGB200_MAX_COLORS 128       /* src/utils.hpp:48 */
@@ -109,6 +110,11 @@ int hpcgb200_copy_diagonal(int m, const int* ell_col, const double* ell_val, dou
 int hpcgb200_replace_diagonal(int m, const double* diagonal, const int* ell_col, double* ell_val,
                               double* inv_diag, double* diag, void* stream);
 
+/* src/TestCG.cpp:67-95 (kernel_scale_vector_values): TestCG's diagonal
+ * exaggeration, diagonal[i] and b[i] scaled by (gid + 2) * 1e6 where
+ * gid = l2g[i] < 9, else by 1e6 (l2g: the level's local-to-global map). */
+int hpcgb200_testcg_scale(int m, const long long* l2g, double* diagonal, double* b, void* stream);
+
 /* Multigrid transfer indices: inj_f[ic] = perm_f[f2c[ic]], inj_c[ic] = perm_c[ic]
  * (the two gathers src/ComputeRestriction.cpp:100-102 and
  * src/ComputeProlongation.cpp:53-56 do per call, done once). */
@@ -136,6 +142,12 @@ int hpcgb200_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const
 int hpcgb200_restrict_fused(int nc, const int* inj_f, const int* inj_c, int mf, const int* ell_col,
                             const double* ell_val, const double* rf, const double* xf, double* rc, void* stream);
 
+/* src/ComputeRestriction.cpp:59-79,182-197 (ComputeRestriction, the
+ * HPCG_REFERENCE form that reads a precomputed Axf = A xf):
+ * rc[inj_c[i]] = rf[inj_f[i]] - axf[inj_f[i]]. */
+int hpcgb200_restrict(int nc, const int* inj_f, const int* inj_c, const double* rf, const double* axf, double* rc,
+                      void* stream);
+
 /* src/ComputeProlongation.cpp:39-86: xf[inj_f[i]] += xc[inj_c[i]]. */
 int hpcgb200_prolong(int nc, const int* inj_f, const int* inj_c, const double* xc, double* xf, void* stream);
 
@@ -156,8 +168,11 @@ int hpcgb200_dot(int n, const double* x, const double* y, double* result, void* 
  * n <= 16,777,216 (4096 partial sums of 4096-element tiles); larger n returns
  * HPCGB200_ERR_ARG.  All calls share that array: calls that overlap on the
  * GPU race, so serialize them.  The first call on a device looks up the
- * array's address (once per device); make it before any stream capture.
- * Allocates nothing.  Same value as hpcgb200_dot up to summation order. */
+ * array's address (once per CUDA context, so a device reset or a caller's own
+ * driver-API context gets a fresh lookup); make it before any stream capture.
+ * Allocates nothing.  Deterministic for a given n, but its summation order
+ * (one partial per 4096-element tile) is not hpcgb200_dot's, so the two agree
+ * to rounding, not bit for bit. */
 int hpcgb200_dot_noalloc(long long n, const double* x, const double* y, double* result, void* stream);
 
 /* src/ComputeWAXPBY.cpp:63-135 (kernel_waxpby): w = alpha x + beta y with the
@@ -254,12 +269,19 @@ int hpcgb200_problem_get_x(hpcgb200_problem* p, double* host_x_natural);
 
 /* src/CG.cpp:104-200: CG from x = 0 on the problem's b.  mode: HPCGB200_MODE_*.
  * normr_hist (host, may be NULL) gets max_iter+1 entries (normr after the
- * preamble and after each iteration).  seconds: device-timed solve. */
+ * preamble and after each iteration).  seconds: device-timed solve.
+ * A residual that turns non-finite (a NaN or Inf in b or in the operator
+ * data) ends the iterations at once; the outputs are filled and the call
+ * returns HPCGB200_ERR_NONFINITE.  In HPCGB200_MODE_LEARNED a non-finite
+ * network step is a smoother failure instead: the solve restarts from x = 0
+ * with the plain FP32 V-cycle, counting the abandoned iterations in *niters
+ * and reporting the restart as the fallback iteration. */
 int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, double tol, int precond, int* niters,
                         double* normr, double* normr0, double* normr_hist, double* seconds);
 
 /* Same, end to end from HOST memory: copies b_natural in, solves, copies x
- * out (natural order); seconds covers the copies too. */
+ * out (natural order); seconds covers the copies too.  Non-finite residual:
+ * as above. */
 int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const double* b_natural, double* x_natural,
                                 int max_iter, double tol, int* niters, double* normr, double* normr0,
                                 double* seconds);
@@ -285,9 +307,16 @@ int hpcgb200_problem_test_symmetry(hpcgb200_problem* p, int mode, double* depsym
 /* Per-operator calls on the handle's level data (vectors are DEVICE
  * pointers in permuted order), used by the operator parity tests. */
 int hpcgb200_problem_spmv(hpcgb200_problem* p, int level, const double* x, double* y);
-/* y = A x on the implicit stencil (the mixed path's FP64 operator); no
- * reference counterpart; bitwise equal to hpcgb200_problem_spmv. */
+/* y = A x on the implicit stencil in the ELL kernel's summation order (the
+ * FP64 stencil mode's operator and every solve's preamble); no reference
+ * counterpart; bitwise equal to hpcgb200_problem_spmv. */
 int hpcgb200_problem_spmv_stencil(hpcgb200_problem* p, int level, const double* x, double* y);
+/* The mixed path's outer FP64 operator on the implicit stencil: y = A x with
+ * the 27 terms summed as a separable box (x, then y, then z sums), equal to
+ * the ELL product to FP64 rounding (not bit for bit); the product the mixed
+ * and learned CG steps use.  No reference counterpart (src/ComputeSPMV.cpp:
+ * 226-278 is the operator it stands in for). */
+int hpcgb200_problem_spmv_mixed(hpcgb200_problem* p, int level, const double* x, double* y);
 int hpcgb200_problem_symgs(hpcgb200_problem* p, int level, const double* r, double* x);
 int hpcgb200_problem_symgs_zero(hpcgb200_problem* p, int level, const double* r, double* x);
 int hpcgb200_problem_mg(hpcgb200_problem* p, int mode, const double* r, double* x);

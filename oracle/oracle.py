@@ -22,17 +22,35 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libhpcg_ref.so")
+# the same reference sources built without HPCG_CONTIGUOUS_ARRAYS (per-row
+# arrays): the contiguous build computes rows * 27 in 32-bit int
+# (src/GenerateProblem_ref.cpp:115-117) and cannot build grids above that
+REF_ROWS_SO = os.path.join(HERE, "_ref", "libhpcg_ref_rows.so")
+INT_MAX = 0x7FFFFFFF
 COLORED_SO = os.path.join(HERE, "liboracle.so")
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
 
+def reference_tree() -> str | None:
+    """The rocHPCG source tree the reference oracle is compiled from:
+    $HPCG_REFERENCE_DIR, else a directory named ``reference`` beside the
+    repository; None when neither holds ``src/CG_ref.cpp``."""
+    cands = [os.environ.get("HPCG_REFERENCE_DIR"),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isfile(os.path.join(c, "src", "CG_ref.cpp")):
+            return os.path.abspath(c)
+    return None
+
+
 def build(ref: bool = True) -> None:
     """Compile the oracle libraries (the reference one only where its source tree exists)."""
     subprocess.check_call(["make", "-s", "-C", HERE])
-    if ref:
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    tree = reference_tree() if ref else None
+    if tree:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF=" + tree])
 
 
 def _ptr(a: np.ndarray):
@@ -43,15 +61,17 @@ def _ptr(a: np.ndarray):
 # reference CPU path
 
 
-_ref_lib = None
+_ref_libs: dict = {}
 
 
-def ref_lib():
-    global _ref_lib
-    if _ref_lib is None:
-        if not os.path.exists(REF_SO):
-            raise FileNotFoundError(f"{REF_SO} missing: run `make -C oracle ref` where the reference tree exists")
-        L = ctypes.CDLL(REF_SO)
+def ref_lib(rows: bool = False):
+    """The reference CPU library: contiguous arrays (the reference build's
+    setting), or per-row arrays for grids whose 27 * rows exceeds INT_MAX."""
+    so = REF_ROWS_SO if rows else REF_SO
+    if so not in _ref_libs:
+        if not os.path.exists(so):
+            raise FileNotFoundError(f"{so} missing: run `make -C oracle ref` where the reference tree exists")
+        L = ctypes.CDLL(so)
         L.hpcgref_create.restype = ctypes.c_void_p
         L.hpcgref_create.argtypes = [ctypes.c_int] * 4
         L.hpcgref_destroy.argtypes = [ctypes.c_void_p]
@@ -73,8 +93,8 @@ def ref_lib():
                                      ctypes.c_void_p, ctypes.c_void_p]
         L.hpcgref_residual.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _c_dbl_p]
         L.hpcgref_test_norms.argtypes = [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_int_p]
-        _ref_lib = L
-    return _ref_lib
+        _ref_libs[so] = L
+    return _ref_libs[so]
 
 
 class RefProblem:
@@ -82,7 +102,7 @@ class RefProblem:
     SetupHalo_ref + 3 coarse levels, solved by CG_ref."""
 
     def __init__(self, nx: int, ny: int, nz: int, nlevels: int = 4):
-        self.L = ref_lib()
+        self.L = ref_lib(rows=27 * nx * ny * nz > INT_MAX)
         self.h = self.L.hpcgref_create(nx, ny, nz, nlevels)
         if not self.h:
             raise ValueError("hpcgref_create failed")

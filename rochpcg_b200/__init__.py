@@ -25,6 +25,7 @@ MODE_MIXED = 1
 MODE_LEARNED = 2
 MODE_FP64_STENCIL = 3  # FP64 results of MODE_FP64 bit for bit, V-cycle and SpMV on the implicit stencil
 FLAG_KEEP_GENERATED = 1
+ERR_NONFINITE = 8  # a solve ended with a non-finite residual (HPCGB200_ERR_NONFINITE)
 
 _FIELD_DTYPES = {
     "perm": np.int32, "colors": np.int32, "ell_col": np.int32, "ell_val": np.float64, "diag_idx": np.int32,
@@ -148,9 +149,14 @@ class Problem:
         it = ctypes.c_int()
         nr, nr0, sec = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         hist = np.zeros(max_iter + 1)
-        check(self.L, self.L.hpcgb200_problem_cg(self.h, mode, max_iter, tol, int(precond), ctypes.byref(it),
-                                                 ctypes.byref(nr), ctypes.byref(nr0), _p(hist), ctypes.byref(sec)))
-        return dict(niters=it.value, normr=nr.value, normr0=nr0.value, hist=hist[: it.value + 1], seconds=sec.value)
+        rc = self.L.hpcgb200_problem_cg(self.h, mode, max_iter, tol, int(precond), ctypes.byref(it), ctypes.byref(nr),
+                                        ctypes.byref(nr0), _p(hist), ctypes.byref(sec))
+        out = dict(niters=it.value, normr=nr.value, normr0=nr0.value, hist=hist[: it.value + 1], seconds=sec.value)
+        if rc != 0:
+            err = HpcgError(self.L, rc)
+            err.result = out if rc == ERR_NONFINITE else None  # a non-finite end still fills the outputs
+            raise err
+        return out
 
     def solve_host(self, b_natural: np.ndarray, x_out: np.ndarray, max_iter: int, tol: float,
                    mode: int = MODE_FP64) -> dict:
@@ -208,6 +214,12 @@ class Problem:
     def spmv_stencil(self, level: int, x_ptr: int, y_ptr: int):
         check(self.L, self.L.hpcgb200_problem_spmv_stencil(self.h, level, ctypes.c_void_p(x_ptr),
                                                            ctypes.c_void_p(y_ptr)))
+
+    def spmv_mixed(self, level: int, x_ptr: int, y_ptr: int):
+        """The mixed path's outer FP64 operator (separable sum; equal to the ELL
+        product to rounding)."""
+        check(self.L, self.L.hpcgb200_problem_spmv_mixed(self.h, level, ctypes.c_void_p(x_ptr),
+                                                         ctypes.c_void_p(y_ptr)))
 
     def symgs(self, level: int, r_ptr: int, x_ptr: int):
         check(self.L, self.L.hpcgb200_problem_symgs(self.h, level, ctypes.c_void_p(r_ptr), ctypes.c_void_p(x_ptr)))

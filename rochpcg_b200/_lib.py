@@ -30,11 +30,13 @@ SIGNATURES = {
     "hpcgb200_unpermute_vector": (_i, [_i, _vp, _vp, _vp, _vp]),
     "hpcgb200_copy_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "hpcgb200_replace_diagonal": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hpcgb200_testcg_scale": (_i, [_i, _vp, _vp, _vp, _vp]),
     "hpcgb200_transfer_indices": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_spmv": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_symgs": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_symgs_zero": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_restrict_fused": (_i, [_i, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hpcgb200_restrict": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_prolong": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_dot": (_i, [_i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hpcgb200_dot_noalloc": (_i, [_ll, _vp, _vp, _vp, _vp]),
@@ -89,6 +91,7 @@ SIGNATURES = {
     "hpcgb200_problem_test_symmetry": (_i, [_vp, _i, _vp, _vp, _vp]),
     "hpcgb200_problem_spmv": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_spmv_stencil": (_i, [_vp, _i, _vp, _vp]),
+    "hpcgb200_problem_spmv_mixed": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_symgs": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_symgs_zero": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_mg": (_i, [_vp, _i, _vp, _vp]),

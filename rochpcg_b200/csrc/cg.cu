@@ -15,7 +15,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_residual0(int n, const do
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
     {
         const double v = fma(-1.0, Ap[i], b[i]);  // WAXPBY(1, b, -1, Ap): alpha == 1 form
         r[i] = v;
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_rtz(int n, const double* 
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
         s = fma(z[i], r[i], s);
     s = block_sum(s, red);
     double total;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const do
     const double alpha = st->alpha;
     const bool flex = st->flexible != 0;
     double s = 0.0, sf = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
     {
         const double v = fma(-alpha, Ap[i], r[i]);   // ComputeFusedWAXPBYDot(-alpha, Ap, r)
         r[i] = v;

@@ -1190,6 +1190,155 @@ inline dim3 march_grid(const StencilLevel& L)
                 (unsigned)((L.nz + kMZ - 1) / kMZ));
 }
 
+// ---- separable product (the mixed path's outer operator, canonical
+// colouring).  The outer CG of the mixed path needs A p in FP64, not the ELL
+// kernel's summation order, so the 27 neighbours are summed as a separable
+// box: per staged plane the x sums sx = x[-1] + x[0] + x[+1] of the tile's
+// rows and their y halo go to shared memory, the y sums sxy of those give one
+// value per row, and a ring of three sxy values in registers gives the box
+// sum S over z.  y = a_ii x - (S - x): about 7 shared-memory reads per row
+// instead of the 27 of the ELL-ordered march, which is bound by shared-memory
+// bandwidth (27 x 8 B per row).  The result equals the ELL product to FP64
+// rounding (a different association of the same 27 terms).  A block owns a
+// 64 x 4 column of the grid and kSZ planes; two barriers per plane.
+constexpr int kSZ = 32;                                        // z planes per block
+constexpr int kSXh = kMX / 2;                                  // sx row: 64 points, x parity split
+constexpr int kSRows = kMY + 2;                                // tile rows and their y halo
+constexpr int kSPts = kMX * kSRows;                            // 384 x sums per plane
+constexpr int kSPer = (kSPts + kMThreads - 1) / kMThreads;     // 2 per thread
+
+// Slot of the x sum of tile column lx (0..63) on halo row hy (0..5).
+__host__ __device__ constexpr int sx_slot(int lx, int hy) { return (hy * 2 + (lx & 1)) * kSXh + (lx >> 1); }
+
+template <bool kPap>
+__global__ void __launch_bounds__(kMThreads) k64_spmv_sep(const StencilLevel L, const double* __restrict__ diag,
+                                                          const double* __restrict__ p, double* __restrict__ Ap,
+                                                          CGState* st, double* partial, unsigned int* ticket)
+{
+    __shared__ double xs[kPlane];   // staged plane with its one-point halo (66 x 6, x parity split)
+    __shared__ double sxs[kSPts];   // x sums of the 64 x 6 points
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, zb = blockIdx.z * kSZ;  // zb even
+    const int ze = zb + kSZ < L.nz ? zb + kSZ : L.nz;
+
+    // staged positions, as in the march
+    int slot[kMLoads];
+    bool inxy[kMLoads];
+    CanonColumn col[kMLoads];
+#pragma unroll
+    for(int k = 0; k < kMLoads; ++k)
+    {
+        const int e = tid + k * kMThreads;
+        const int hx = e % kPX, hy = e / kPX;
+        const int x = x0 + hx - 1, y = y0 + hy - 1;
+        slot[k] = e < kPlane ? plane_slot(hx, hy) : -1;
+        inxy[k] = e < kPlane && x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+        col[k] = canon_column(L, inxy[k] ? x : 0, inxy[k] ? y : 0);
+    }
+    // x-sum positions: a warp takes one halo row and one x parity
+    int sdst[kSPer], sm[kSPer], s0[kSPer], sp[kSPer];
+#pragma unroll
+    for(int k = 0; k < kSPer; ++k)
+    {
+        const int e = tid + k * kMThreads;
+        const int hy = e >> 6, lx = 2 * (e & 31) + ((e >> 5) & 1);
+        sdst[k] = e < kSPts ? sx_slot(lx, hy) : -1;
+        sm[k] = plane_slot(lx, hy);
+        s0[k] = plane_slot(lx + 1, hy);
+        sp[k] = plane_slot(lx + 2, hy);
+    }
+    // own output column: warp -> (x parity, row), lane -> x
+    const int px = warp & 1, ly = warp >> 1;
+    const int lx = 2 * lane + px;
+    const int x = x0 + lx, y = y0 + ly;
+    const bool mine = x < L.nx && y < L.ny;
+    const int c = plane_slot(lx + 1, ly + 1);
+    const int cm = sx_slot(lx, ly), c0 = sx_slot(lx, ly + 1), cp = sx_slot(lx, ly + 2);
+    const CanonColumn own = canon_column(L, mine ? x : 0, mine ? y : 0);
+
+    double hv[kMLoads];
+    auto load_plane = [&](int z, auto zq) {
+        constexpr int q = decltype(zq)::value;  // z & 1
+#pragma unroll
+        for(int k = 0; k < kMLoads; ++k)
+        {
+            hv[k] = 0.0;
+            if(inxy[k] && z >= 0 && z < L.nz) hv[k] = p[canon_row<q>(col[k], z)];
+        }
+    };
+    using Q0 = std::integral_constant<int, 0>;
+    using Q1 = std::integral_constant<int, 1>;
+
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;  // sxy of planes t-2, t-1, t
+    double xo0 = 0.0, xo1 = 0.0;          // own x of planes t-1, t
+    double s = 0.0;
+    load_plane(zb - 1, Q1{});
+    // plane t: stage it, prefetch plane t+1, finish row plane t-1 (parity of t+1)
+    auto step = [&](int t, auto zq) {
+        constexpr int q = decltype(zq)::value;  // (t + 1) & 1 == (t - 1) & 1
+#pragma unroll
+        for(int k = 0; k < kMLoads; ++k)
+            if(slot[k] >= 0) xs[slot[k]] = hv[k];
+        if(t + 1 <= ze) load_plane(t + 1, zq);
+        const int zo = t - 1;
+        const bool out = mine && zo >= zb;
+        const double d = out ? diag[canon_row<q>(own, zo)] : 0.0;
+        __syncthreads();  // plane t staged
+#pragma unroll
+        for(int k = 0; k < kSPer; ++k)
+            if(sdst[k] >= 0) sxs[sdst[k]] = (xs[sm[k]] + xs[s0[k]]) + xs[sp[k]];
+        const double xn = xs[c];
+        __syncthreads();  // x sums of plane t stored; plane t no longer read
+        r0 = r1;
+        r1 = r2;
+        r2 = (sxs[cm] + sxs[c0]) + sxs[cp];
+        xo0 = xo1;
+        xo1 = xn;
+        if(out)
+        {
+            const double nbr = ((r0 + r1) + r2) - xo0;  // the 26 neighbours of (x, y, zo)
+            const double v = fma(d, xo0, -nbr);
+            Ap[canon_row<q>(own, zo)] = v;
+            if(kPap) s = fma(v, xo0, s);
+        }
+    };
+    for(int t = zb - 1; t <= ze; t += 2)
+    {
+        step(t, Q0{});
+        if(t + 1 <= ze) step(t + 1, Q1{});
+    }
+    if(!kPap) return;
+    s = block_sum(s, red);
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    if(tid == 0)
+    {
+        partial[bid] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == nblocks - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(int k = tid; k < (int)nblocks; k += kMThreads) acc += __ldcg(&partial[k]);
+    acc = block_sum(acc, red);
+    if(tid == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
+inline dim3 sep_grid(const StencilLevel& L)
+{
+    return dim3((unsigned)((L.nx + kMX - 1) / kMX), (unsigned)((L.ny + kMY - 1) / kMY),
+                (unsigned)((L.nz + kSZ - 1) / kSZ));
+}
+
 // ------------------------------------------------------------ set-up kernels
 
 __global__ void k_diag32(int m, const double* __restrict__ diag, float* __restrict__ d32, float* __restrict__ inv32)
@@ -1505,9 +1654,10 @@ static int tile64_blocks(const StencilLevel& L)
 
 size_t stencil_pap_partials(const StencilLevel& L)
 {
-    const dim3 g = march_grid(L);
-    const size_t march = (size_t)g.x * g.y * g.z;
-    return march > (size_t)tile64_blocks(L) ? march : (size_t)tile64_blocks(L);
+    const dim3 g = march_grid(L), gs = sep_grid(L);
+    size_t n = (size_t)g.x * g.y * g.z;
+    n = n > (size_t)gs.x * gs.y * gs.z ? n : (size_t)gs.x * gs.y * gs.z;
+    return n > (size_t)tile64_blocks(L) ? n : (size_t)tile64_blocks(L);
 }
 
 static bool canonical_colours(const StencilLevel& L)
@@ -1527,11 +1677,21 @@ int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const doubl
     return 0;
 }
 
+int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s)
+{
+    if(canonical_colours(L))
+        k64_spmv_sep<false><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+    else
+        k64_spmv_tile<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+    HB_LAUNCHED();
+    return 0;
+}
+
 int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
     if(canonical_colours(L))
-        k64_spmv_march<true><<<march_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
+        k64_spmv_sep<true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
     else
         k64_spmv_tile<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
     HB_LAUNCHED();

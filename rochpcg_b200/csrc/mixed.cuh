@@ -91,9 +91,14 @@ int launch64v_prolong(const StencilLevel& Lf, int nc, const int* inj_c, const do
 // FP64 y = A x on the implicit stencil (bitwise equal to the ELL SpMV: same
 // slot order, fma(-1, x, s) == s - x, fma(a_ii, x_i, s) on the diagonal).
 int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s);
-// Same fused with p.Ap and alpha = rtz / pAp (the CG step of k_cg_spmv_pap);
-// one partial sum per block in `partial` (stencil_pap_partials(L) entries),
-// `ticket` must start at zero and is left at zero.
+// The mixed path's outer operator: y = A x in FP64 with the 27 terms summed
+// as a separable box (x sums, y sums, z sums) -- equal to the ELL product to
+// FP64 rounding, not bit for bit; 7 shared-memory reads per row instead of 27.
+int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s);
+// The separable product fused with p.Ap and alpha = rtz / pAp (the CG step of
+// k_cg_spmv_pap) for the mixed and learned paths; one partial sum per block in
+// `partial` (stencil_pap_partials(L) entries), `ticket` must start at zero and
+// is left at zero.
 size_t stencil_pap_partials(const StencilLevel& L);
 int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);

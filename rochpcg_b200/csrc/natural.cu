@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_nat_dot(int n, const double*
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
         s = __dadd_rn(s, __dmul_rn(x[i], y[i]));
     s = block_sum(s, red);
     double total;

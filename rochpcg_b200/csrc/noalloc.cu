@@ -17,9 +17,14 @@
 //  * Every call, on every stream, uses the same array.  Calls whose kernels
 //    overlap on the GPU race on it: serialize them (one stream, or events).
 //  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture.
+//    cudaGetSymbolAddress (once per CUDA context, with that device current);
+//    make that first call before any stream capture.
+//  * The result is deterministic for a given n (the tile count follows n),
+//    but its summation order differs from hpcgb200_dot's fixed 1184-block
+//    grid, so the two agree to rounding, not bit for bit.
 //  * No cudaMalloc / cudaFree or allocating library call is made.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -79,25 +84,72 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_dot_noalloc(long long n, co
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-NoAllocScratch* g_addr[kMaxDevices] = {};
+// The array's address belongs to the module instance loaded into one CUDA
+// context.  It is cached per context (the driver's unique context id), not
+// per device index: after cudaDeviceReset, or under a caller's own driver-API
+// context, the current context is a different one and gets its own lookup,
+// so a cached address never outlives the module it points into.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of the array on the current device, looked up once.
+constexpr int kMaxContexts = 64;
+std::mutex g_mu;
+unsigned long long g_ctx_id[kMaxContexts] = {};
+NoAllocScratch* g_addr[kMaxContexts] = {};
+int g_cached = 0;
+
+// Unique id of the calling thread's current context (false if there is none
+// yet or the driver does not report ids; the caller then looks the address up
+// without caching it).
+bool current_context_id(unsigned long long* id)
+{
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static bool resolved = false;
+    if(!resolved)
+    {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+           q1 == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(f1);
+        if(cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+           q2 == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnCtxGetId>(f2);
+        resolved = true;
+    }
+    if(!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if(get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of the array in the current context: looked up once per
+// context with that context's device current (the first call on a device).
 int scratch_address(NoAllocScratch** out)
 {
-    int dev = -1;
-    HB_CUDA(cudaGetDevice(&dev));
-    if(dev < 0 || dev >= kMaxDevices) return record_error(HPCGB200_ERR_ARG, "device index %d unsupported", dev);
     std::lock_guard<std::mutex> lock(g_mu);
-    if(!g_addr[dev])
+    unsigned long long id = 0;
+    if(current_context_id(&id))
+        for(int i = 0; i < g_cached; ++i)
+            if(g_ctx_id[i] == id)
+            {
+                *out = g_addr[i];
+                return 0;
+            }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if(e != cudaSuccess || p == nullptr)
+        return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    // the lookup above creates the primary context if there was none yet
+    if(current_context_id(&id) && g_cached < kMaxContexts)
     {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if(e != cudaSuccess || p == nullptr) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-        g_addr[dev] = static_cast<NoAllocScratch*>(p);
+        g_ctx_id[g_cached] = id;
+        g_addr[g_cached] = static_cast<NoAllocScratch*>(p);
+        ++g_cached;
     }
-    *out = g_addr[dev];
+    *out = static_cast<NoAllocScratch*>(p);
     return 0;
 }
 

@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_dot(int n, const double* __r
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
         s = fma(y[i], x[i], s);
     s = block_sum(s, red);
     double total;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_waxpby_dot(int n, double alp
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
     {
         const double v = fma(alpha, x[i], y[i]);
         y[i] = v;
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_inf(int n, const do
 {
     __shared__ double red[32];
     double s = 0.0;
-    for(int i = blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
         s = fmax(s, fabs(v1[i] - v2[i]));
     s = block_max(s, red);
     double total;
@@ -404,6 +404,13 @@ extern "C" int hpcgb200_restrict_fused(int nc, const int* inj_f, const int* inj_
 {
     HB_CHECK_ARG(nc > 0 && mf >= nc && inj_f && inj_c && ell_col && ell_val && rf && xf && rc, "bad arguments");
     return launch_restrict(nc, inj_f, inj_c, mf, ell_col, ell_val, rf, xf, rc, as_stream(stream));
+}
+
+extern "C" int hpcgb200_restrict(int nc, const int* inj_f, const int* inj_c, const double* rf, const double* axf,
+                                 double* rc, void* stream)
+{
+    HB_CHECK_ARG(nc > 0 && inj_f && inj_c && rf && axf && rc, "bad arguments");
+    return launch_restrict_axf(nc, inj_f, inj_c, rf, axf, rc, as_stream(stream));
 }
 
 extern "C" int hpcgb200_prolong(int nc, const int* inj_f, const int* inj_c, const double* xc, double* xf,

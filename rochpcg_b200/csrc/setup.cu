@@ -122,7 +122,7 @@ __global__ void k_count_two(int m, const int* __restrict__ colors, int c1, int c
 {
     __shared__ int red[32];
     int a = 0, b = 0;
-    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    for(long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
     {
         const int c = colors[i];
         a += c == c1;
@@ -529,6 +529,22 @@ __global__ void k_replace_diagonal(int m, const double* __restrict__ diagonal, c
     if(diag) diag[row] = d;
 }
 
+// src/TestCG.cpp:67-95 (kernel_scale_vector_values): TestCG's exaggerated
+// diagonal.  Row i's scale comes from its global id l2g[i]: (gid + 2) * 1e6
+// for the first nine global rows, 1e6 for all others.  TestCG runs it after
+// OptimizeProblem, when rows are colour-permuted but l2g is not, so permuted
+// row i takes the scale of natural row i -- kept as the reference does it.
+__global__ void k_testcg_scale(int m, const long long* __restrict__ l2g, double* __restrict__ diagonal,
+                               double* __restrict__ b)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m) return;
+    const long long gid = l2g[i];
+    const double scale = gid < 9 ? (gid + 2) * 1.0e6 : 1.0e6;
+    diagonal[i] *= scale;
+    b[i] *= scale;
+}
+
 __global__ void k_transfer_indices(int nc, const int* __restrict__ f2c, const int* __restrict__ perm_f,
                                    const int* __restrict__ perm_c, int* __restrict__ inj_f, int* __restrict__ inj_c)
 {
@@ -591,6 +607,14 @@ extern "C" int hpcgb200_replace_diagonal(int m, const double* diagonal, const in
     HB_CHECK_ARG(m > 0 && diagonal && ell_col && ell_val && inv_diag, "bad arguments");
     k_replace_diagonal<<<blocks_for(m, 256), 256, 0, as_stream(stream)>>>(m, diagonal, ell_col, ell_val, inv_diag,
                                                                          diag);
+    HB_LAUNCHED();
+    return 0;
+}
+
+extern "C" int hpcgb200_testcg_scale(int m, const long long* l2g, double* diagonal, double* b, void* stream)
+{
+    HB_CHECK_ARG(m > 0 && l2g && diagonal && b, "bad arguments");
+    k_testcg_scale<<<blocks_for(m, 256), 256, 0, as_stream(stream)>>>(m, l2g, diagonal, b);
     HB_LAUNCHED();
     return 0;
 }

@@ -75,7 +75,8 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     }
     else if(prec != MGPrecision::FP64)
     {
-        // mixed path: the FP64 operator on the implicit stencil (bitwise equal to the ELL product)
+        // mixed path: the FP64 operator on the implicit stencil (separable sum, equal to the ELL product to
+        // FP64 rounding)
         const LevelOpt* o = opt(A);
         HB_RETURN_IF(hb::launch64_cg_spmv_pap_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, st,
                                                       o->pap_partial, o->pap_ticket, s));
@@ -260,26 +261,37 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         if(o->pap_ticket) HB_HOST_CUDA(cudaMemsetAsync(o->pap_ticket, 0, sizeof(unsigned int), s));
         HB_HOST_CUDA(cudaMemsetAsync(o->spmv_ticket, 0, sizeof(unsigned int), s));
 
-        // preamble: p = x; Ap = A p; r = b - Ap; normr = ||r||
-        HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        // the FP32 V-cycles need the stencil on every level; the FP64 stencil
+        // V-cycle takes the ELL kernels on levels without it, only the outer
+        // SpMV needs it on level 0
         if(prec != MGPrecision::FP64)
-        {
-            // the FP32 V-cycles need the stencil on every level; the FP64 stencil
-            // V-cycle takes the ELL kernels on levels without it, only the outer
-            // SpMV needs it on level 0
             for(const SparseMatrix* M = &A; M; M = prec == MGPrecision::FP64_STENCIL ? nullptr : M->Ac)
                 if(!opt(*M) || !opt(*M)->stencil_ok)
                     return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
                                             "stencil CG needs the 27-point stencil in parity colouring on every level");
-            check(hb::launch64_spmv_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, s));
-        }
-        else
+        // preamble: p = x; Ap = A p; r = b - Ap; normr = ||r|| (resets the
+        // device iteration counter and the history)
+        auto preamble = [&] {
+            HB_HOST_CUDA(cudaMemcpyAsync(data.p.d_values, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                         s));
+            if(prec != MGPrecision::FP64)
+                check(hb::launch64_spmv_stencil(o->st, o->diag, data.p.d_values, data.Ap.d_values, s));
+            else
+                check(hb::launch_spmv(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, s));
+            check(hb::launch_cg_residual0(n, b.d_values, data.Ap.d_values, data.r.d_values, st, rt().ws, s));
+            HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
+            HB_HOST_CUDA(cudaStreamSynchronize(s));
+        };
+        // learned mode: keep the initial guess, so that a network step that
+        // makes the residual non-finite costs a restart, not the solution
+        if(prec == MGPrecision::LEARNED)
         {
-            check(hb::launch_spmv(n, o->cc, A.ell_col_ind, A.ell_val, data.p.d_values, data.Ap.d_values, s));
+            if(!o->x0_saved) o->x0_saved = dalloc<double>(n);
+            HB_HOST_CUDA(cudaMemcpyAsync(o->x0_saved, x.d_values, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
         }
-        check(hb::launch_cg_residual0(n, b.d_values, data.Ap.d_values, data.r.d_values, st, rt().ws, s));
-        HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
-        HB_HOST_CUDA(cudaStreamSynchronize(s));
+        preamble();
+        int restart_offset = 0;            // iterations spent before a restart
+        std::vector<double> hist_before;   // their residual history
 
         // Iterations: the learned mode runs until converged or until its
         // smoother fails (a jump or a stall of normr); the plain FP32 V-cycle then takes
@@ -291,7 +303,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             if(!iterate) break;
             if(!graphs_enabled())
             {
-                for(int k = h.k; k <= max_iter; ++k)
+                for(int k = h.k; k <= max_iter - restart_offset; ++k)
                 {
                     check(capture_body(A, data, x, precond, cur, st, 0ULL, s, timed));
                     HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
@@ -308,7 +320,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
                 }
                 else
                 {
-                    for(int k = h.k; k <= max_iter; ++k)
+                    for(int k = h.k; k <= max_iter - restart_offset; ++k)
                     {
                         HB_HOST_CUDA(cudaGraphLaunch(G->exec, s));
                         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
@@ -321,6 +333,26 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             HB_HOST_CUDA(cudaStreamSynchronize(s));
             if(cur != MGPrecision::LEARNED || h.net != 2) break;
             cur = MGPrecision::FP32;
+            if(!std::isfinite(h.normr))
+            {
+                // the network's step poisoned x and r: restart the plain
+                // FP32 V-cycle solve from the initial guess, keeping the
+                // abandoned iterations in the count and the history
+                restart_offset = h.niters;
+                hist_before.resize(restart_offset + 1);
+                HB_HOST_CUDA(cudaMemcpy(hist_before.data(), st->hist, sizeof(double) * (restart_offset + 1),
+                                        cudaMemcpyDeviceToHost));
+                HB_HOST_CUDA(cudaMemcpyAsync(x.d_values, o->x0_saved, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                             s));
+                const int left = max_iter - restart_offset;
+                HB_HOST_CUDA(cudaMemcpyAsync(&st->max_iter, &left, sizeof(int), cudaMemcpyHostToDevice, s));
+                // a fresh solve: no pending direction restart (the fallback
+                // iteration is reported from restart_offset)
+                const int none = 0;
+                HB_HOST_CUDA(cudaMemcpyAsync(&st->fallback_iter, &none, sizeof(int), cudaMemcpyHostToDevice, s));
+                preamble();
+                if(left < 1) break;
+            }
         }
         HB_HOST_CUDA(cudaEventRecord(e1, s));
         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
@@ -331,12 +363,16 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         cudaEventDestroy(e1);
         if(hist)
         {
-            HB_HOST_CUDA(cudaMemcpy(hist, st->hist, sizeof(double) * (h.niters + 1), cudaMemcpyDeviceToHost));
-            for(int k = h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
+            // after a restart: the abandoned iterations, then the restarted
+            // solve's iterations 1.. (its normr0 is the same)
+            for(int k = 0; k <= restart_offset && restart_offset > 0; ++k) hist[k] = hist_before[k];
+            HB_HOST_CUDA(cudaMemcpy(hist + restart_offset + (restart_offset > 0), st->hist + (restart_offset > 0),
+                                    sizeof(double) * (h.niters + 1 - (restart_offset > 0)), cudaMemcpyDeviceToHost));
+            for(int k = restart_offset + h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
         }
-        o->last_fallback_iter = h.fallback_iter;
+        o->last_fallback_iter = restart_offset > 0 ? restart_offset : h.fallback_iter;
         if(prec == MGPrecision::LEARNED) check(smoother_status(*o->smoother, s));
-        niters = h.niters;
+        niters = restart_offset + h.niters;
         normr = h.normr;
         normr0 = h.normr0;
         if(seconds) *seconds = ms * 1e-3;

@@ -165,6 +165,7 @@ static void delete_level_opt(SparseMatrix& A)
     dfree(o->spmv_ticket);
     dfree(o->z32);
     dfree(o->vec_scratch);
+    dfree(o->x0_saved);
     for(auto& g : o->graphs)
     {
         if(g->exec) cudaGraphExecDestroy(g->exec);

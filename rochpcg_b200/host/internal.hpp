@@ -118,6 +118,7 @@ struct LevelOpt
     float* r32 = nullptr;              // FP32 right-hand side of the V-cycle (level 0)
     float* z32 = nullptr;              // FP32 V-cycle result (level 0)
     double* vec_scratch = nullptr;     // one FP64 vector of length m (TestCG / TestSymmetry)
+    double* x0_saved = nullptr;        // learned CG: the initial guess, for a restart after a non-finite step
 
     // learned smoother (level 0 holds it for the hierarchy)
     struct Smoother* smoother = nullptr;

@@ -300,6 +300,15 @@ extern "C" int hpcgb200_problem_get_x(hpcgb200_problem* p, double* host_x_natura
 }
 
 
+// The reference's CG returns 0 whatever the residual became; the problem
+// API reports a non-finite end instead (the outputs are filled first).
+static int finite_or_error(double normr, double normr0, int niters)
+{
+    if(std::isfinite(normr) && std::isfinite(normr0)) return 0;
+    return hb::record_error(HPCGB200_ERR_NONFINITE, "CG ended with a non-finite residual (normr0 = %g, normr = %g "
+                            "after %d iterations): check b and the operator data", normr0, normr, niters);
+}
+
 extern "C" int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, double tol, int precond, int* niters,
                                    double* normr, double* normr0, double* normr_hist, double* seconds)
 {
@@ -307,8 +316,9 @@ extern "C" int hpcgb200_problem_cg(hpcgb200_problem* p, int mode, int max_iter, 
     if(!mode_ok(mode)) return hb::record_error(HPCGB200_ERR_ARG, "bad mode");
     return guarded([&] {
         CudaZeroVector(p->x);
-        return run_cg(p->A, p->data, p->b, p->x, max_iter, tol, *niters, *normr, *normr0, precond != 0, prec_of(mode),
-                      flexible_of(mode), normr_hist, seconds);
+        const int r = run_cg(p->A, p->data, p->b, p->x, max_iter, tol, *niters, *normr, *normr0, precond != 0,
+                             prec_of(mode), flexible_of(mode), normr_hist, seconds);
+        return r ? r : finite_or_error(*normr, *normr0, *niters);
     });
 }
 
@@ -334,7 +344,7 @@ extern "C" int hpcgb200_problem_solve_host(hpcgb200_problem* p, int mode, const 
         HB_HOST_CUDA(cudaMemcpyAsync(x_natural, tmp, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         HB_HOST_CUDA(cudaStreamSynchronize(s));
         if(seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        return 0;
+        return finite_or_error(*normr, *normr0, *niters);
     });
 }
 
@@ -471,6 +481,17 @@ extern "C" int hpcgb200_problem_spmv_stencil(hpcgb200_problem* p, int level, con
     });
 }
 
+extern "C" int hpcgb200_problem_spmv_mixed(hpcgb200_problem* p, int level, const double* x, double* y)
+{
+    SparseMatrix* M = level_of(p, level);
+    if(!M || !x || !y) return hb::record_error(HPCGB200_ERR_ARG, "bad arguments");
+    return guarded([&] {
+        const LevelOpt* o = opt(*M);
+        if(!o->stencil_ok) return hb::record_error(HPCGB200_ERR_NOT_STENCIL, "level %d is not the verified stencil", level);
+        return hb::launch64_spmv_sep(o->st, o->diag, x, y, rt().stream);
+    });
+}
+
 extern "C" int hpcgb200_problem_symgs(hpcgb200_problem* p, int level, const double* r, double* x)
 {
     SparseMatrix* M = level_of(p, level);
@@ -550,11 +571,12 @@ extern "C" int hpcgb200_problem_time_op(hpcgb200_problem* p, const char* op, int
             HB_RETURN_IF(smoother_ready(A, rt().stream));
             f = [&] { return ComputeMG_Learned(A, r, z); };
         }
-        else if(o == "symgs32_sweep" || o == "spmv_stencil")
+        else if(o == "symgs32_sweep" || o == "spmv_stencil" || o == "spmv_mixed")
         {
             const LevelOpt* lo = opt(A);
             if(!lo->stencil_ok) return hb::record_error(HPCGB200_ERR_NOT_STENCIL, "level 0 is not the verified stencil");
             if(o == "spmv_stencil") f = [&, lo] { return hb::launch64_spmv_stencil(lo->st, lo->diag, p->data.p.d_values, p->data.Ap.d_values, s); };
+            else if(o == "spmv_mixed") f = [&, lo] { return hb::launch64_spmv_sep(lo->st, lo->diag, p->data.p.d_values, p->data.Ap.d_values, s); };
             else
             {
                 // one FP32 SymGS step on level 0 (15 colour launches), averaged per launch

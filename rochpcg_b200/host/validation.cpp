@@ -26,23 +26,10 @@ int TestCG_B200(SparseMatrix& A, CGData& data, Vector& b, Vector& x, TestCGData&
 
         // kernel_scale_vector_values (src/TestCG.cpp:67-95) runs after
         // OptimizeProblem and indexes d_localToGlobalMap -- which is not
-        // permuted -- with the permuted row id, so permuted row i is scaled by
-        // (l2g[i] + 2) * 1e6 if l2g[i] < 9 and by 1e6 otherwise; on one rank
-        // l2g[i] = i.  Reproduced as is.
-        std::vector<double> hd(m), hb(m);
-        HB_HOST_CUDA(cudaMemcpyAsync(hd.data(), origDiagA.d_values, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
-        HB_HOST_CUDA(cudaMemcpyAsync(hb.data(), b.d_values, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
-        HB_HOST_CUDA(cudaStreamSynchronize(s));
-        for(local_int_t i = 0; i < m; ++i)
-        {
-            const long long gid = i;
-            const double sc = gid < 9 ? (gid + 2) * 1.0e6 : 1.0e6;
-            hd[i] *= sc;
-            hb[i] *= sc;
-        }
-        HB_HOST_CUDA(cudaMemcpyAsync(exaggeratedDiagA.d_values, hd.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
-        HB_HOST_CUDA(cudaMemcpyAsync(b.d_values, hb.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
-        HB_HOST_CUDA(cudaStreamSynchronize(s));
+        // permuted -- with the permuted row id; reproduced as is, on the device.
+        CudaCopyVector(origDiagA, exaggeratedDiagA);
+        if(!A.d_localToGlobalMap) throw Error(HPCGB200_ERR_ARG, "TestCG: level has no local-to-global map");
+        check(hpcgb200_testcg_scale(m, A.d_localToGlobalMap, exaggeratedDiagA.d_values, b.d_values, s));
         CudaReplaceMatrixDiagonal(A, exaggeratedDiagA);
 
         int niters = 0;

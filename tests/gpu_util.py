@@ -29,3 +29,28 @@ def sync(P):
 
 def host(t) -> np.ndarray:
     return t.cpu().numpy()
+
+
+class _DeviceArray:
+    """A raw device allocation of the library, seen by torch through the CUDA
+    array interface (no copy)."""
+
+    def __init__(self, ptr: int, n: int, dtype):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": np.dtype(dtype).str, "data": (ptr, False),
+                                         "version": 3}
+
+
+def dev_field(P, name: str, level: int, dtype):
+    """Torch view of a problem's DEVICE array (compared on the GPU, so the
+    full-size tests need no host copy of the library's arrays)."""
+    import ctypes
+
+    import torch
+
+    from rochpcg_b200 import check
+
+    nbytes = ctypes.c_size_t()
+    check(P.L, P.L.hpcgb200_problem_field_bytes(P.h, level, name.encode(), ctypes.byref(nbytes)))
+    n = nbytes.value // np.dtype(dtype).itemsize
+    sync(P)
+    return torch.as_tensor(_DeviceArray(P.device_ptr(name, level), n, dtype), device="cuda")

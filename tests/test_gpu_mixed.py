@@ -76,6 +76,44 @@ def test_stencil_spmv_equals_ell_spmv_bitwise(dims):
         assert np.array_equal(host(y2), O.levels[l].spmv(x))
 
 
+@pytest.mark.parametrize("dims", [(16, 16, 16), (16, 24, 32), (24, 40, 56), (72, 40, 48), (56, 56, 40),
+                                  (136, 12, 66)])
+def test_mixed_outer_spmv_equals_ell_to_rounding(dims):
+    """The mixed path's outer operator sums the 27 terms as a separable box
+    (x, y, then z sums) instead of the ELL slot order: per row it must equal
+    the ELL product to FP64 rounding, |y - y_ell| <= 64 eps (a_ii |x_i| +
+    sum_j |x_j|), on grids whose sizes are not multiples of the kernel's
+    64 x 4 x 32 blocks, on every level (coarse levels without the canonical
+    colouring take the ELL-ordered stencil kernel)."""
+    if dims == (136, 12, 66):
+        import rochpcg_b200 as R
+
+        P = R.Problem(*dims, nlevels=2)
+        nl = 2
+    else:
+        P, _ = problems(*dims)
+        nl = 4
+    eps = np.finfo(np.float64).eps
+    for l in range(nl):
+        m = P.rows[l]
+        x = np.random.default_rng(90 + l).uniform(-1, 1, m)
+        xd = to_dev(x)
+        y1 = torch.empty(m, dtype=torch.float64, device="cuda")
+        y2 = torch.empty_like(y1)
+        ya = torch.empty_like(y1)
+        xa = xd.abs()
+        torch.cuda.synchronize()
+        P.spmv(l, xd.data_ptr(), y1.data_ptr())
+        P.spmv_mixed(l, xd.data_ptr(), y2.data_ptr())
+        P.spmv(l, xa.data_ptr(), ya.data_ptr())  # a_ii |x_i| - sum |x_j|
+        sync(P)
+        d = torch.from_numpy(P.field("diag", l)).cuda()
+        bound = 64 * eps * (2 * d * xa - ya)  # a_ii |x_i| + sum_j |x_j|
+        assert torch.all((y1 - y2).abs() <= bound), l
+    if dims == (136, 12, 66):
+        P.close()
+
+
 @pytest.mark.parametrize("mode_name", ["MODE_MIXED", "MODE_FP64_STENCIL"])
 def test_direct_launches_equal_graph(mode_name, monkeypatch):
     """The solve as one graph (kernels back to back, no programmatic launch)

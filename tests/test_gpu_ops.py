@@ -72,6 +72,44 @@ def test_restriction_prolongation_bitwise(dims):
 
 
 @pytest.mark.parametrize("dims", GRIDS)
+def test_restriction_reference_form(dims):
+    """ComputeRestriction in its HPCG_REFERENCE form
+    (src/ComputeRestriction.cpp:59-79,182-197): Axf = A xf by the SpMV, then
+    rc = rf - Axf at the injected points, through hpcgb200_restrict.  Bit for
+    bit against the restatement (rf - A xf of the ELL product at inj_f), and to
+    rounding against the reference's own ComputeSPMV_ref +
+    ComputeRestriction_ref in natural order (another summation order)."""
+    import ctypes
+
+    import rochpcg_b200 as R
+    from oracle.oracle import RefProblem
+
+    P, O = problems(*dims)
+    lib = R.load()
+    ref = RefProblem(*dims)
+    for l in range(3):
+        F, C = O.levels[l], O.levels[l + 1]
+        rf, xf = rand(F.m, 90 + l), rand(F.m, 95 + l)
+        rfd, xfd = to_dev(rf), to_dev(xf)
+        axf = torch.empty_like(xfd)
+        rcd = torch.full((C.m,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        P.spmv(l, xfd.data_ptr(), axf.data_ptr())
+        vp = ctypes.c_void_p
+        assert lib.hpcgb200_restrict(C.m, vp(P.device_ptr("inj_f", l)), vp(P.device_ptr("inj_c", l)),
+                                     vp(rfd.data_ptr()), vp(axf.data_ptr()), vp(rcd.data_ptr()),
+                                     vp(P.stream_handle)) == 0
+        sync(P)
+        inj_f = F.perm[F.f2c]
+        want = np.empty(C.m)
+        want[C.perm] = rf[inj_f] - F.spmv(xf)[inj_f]
+        got = host(rcd)
+        assert np.array_equal(got, want)
+        nat = ref.restriction(l, F.unpermute(rf), F.unpermute(xf))
+        assert np.allclose(C.unpermute(got), nat, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("dims", GRIDS)
 def test_mg_vcycle_bitwise(dims):
     """The whole 4-level V-cycle has no reduction: bit-exact."""
     P, O = problems(*dims)
