@@ -729,7 +729,7 @@ def learned_comparison(args, R, barrier, steps=2, refcheck=None):
     res["speedup_learned_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
     res["speedup_learned_vs_mixed"] = res["mixed"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
     # the literal rule: fall back at the first iteration that does not reduce the FP64 residual norm
-    Q.set_fallback(jump=1.0, stall=10 ** 6, window=16, rate=0.0)
+    Q.set_fallback_rule("first-increase")
     Q.cg(args.max_iter, args.tol, mode=R.MODE_LEARNED)
     r = Q.cg(args.max_iter, args.tol, mode=R.MODE_LEARNED)
     res["learned_first_increase_fallback"] = {"time_to_1e-9_s": r["seconds"], "iterations": r["niters"],
@@ -738,7 +738,7 @@ def learned_comparison(args, R, barrier, steps=2, refcheck=None):
     if refcheck is not None:
         res["learned_first_increase_fallback"]["ref_check_tag"] = refcheck(
             f"learned{n}_first_increase", (n, n, n), ("normal", 9999), Q.get_x())
-    Q.set_fallback()
+    Q.set_fallback_rule("default")
     Q.set_smoother(None)
     Q.close()
     meta = S.meta

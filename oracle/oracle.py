@@ -23,8 +23,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libhpcg_ref.so")
 # the same reference sources built without HPCG_CONTIGUOUS_ARRAYS (per-row
-# arrays): the contiguous build computes rows * 27 in 32-bit int
-# (src/GenerateProblem_ref.cpp:115-117) and cannot build grids above that
+# arrays) and with NDEBUG: the contiguous build computes rows * 27 in 32-bit
+# int (src/GenerateProblem_ref.cpp:115-117), and the int nonzero count's
+# overflow check (:204) aborts above 2^31 nonzeros; this build serves the grids
+# past those limits (560 x 560 x 280), where only ComputeSPMV_ref is called
 REF_ROWS_SO = os.path.join(HERE, "_ref", "libhpcg_ref_rows.so")
 INT_MAX = 0x7FFFFFFF
 COLORED_SO = os.path.join(HERE, "liboracle.so")

@@ -254,6 +254,17 @@ class Problem:
         """Failure rule of the learned solve (see hpcgb200_problem_set_fallback)."""
         check(self.L, self.L.hpcgb200_problem_set_fallback(self.h, jump, stall, window, rate))
 
+    # named failure rules of the learned solve: "first-increase" falls back at
+    # the first iteration that does not reduce the FP64 residual norm (the
+    # literal rule); "default" on a jump (x2), a 16-iteration stall without a
+    # new minimum, or less than 20 % reduction over 16 iterations (PCG's
+    # residual norm is not monotone, so single small increases are tolerated)
+    FALLBACK_RULES = {"first-increase": (1.0, 10 ** 6, 16, 0.0), "default": (2.0, 16, 16, 0.8)}
+
+    def set_fallback_rule(self, name: str):
+        """Select a named failure rule of the learned solve (FALLBACK_RULES)."""
+        self.set_fallback(*self.FALLBACK_RULES[name])
+
     def last_fallback(self) -> int:
         """Iteration at which the last MODE_LEARNED solve fell back to SymGS (0: never)."""
         it = ctypes.c_int()

@@ -39,14 +39,18 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_residual0(int n, const do
     }
 }
 
+// Z: the preconditioner output's type -- double, or float for the FP32
+// V-cycles, whose output is read as is ((double)z32 is exact, so the sums are
+// the ones an FP64 copy of z would give, without writing or reading that copy).
+template <typename Z>
 __global__ void __launch_bounds__(kReduceThreads) k_cg_rtz(int n, const double* __restrict__ r,
-                                                           const double* __restrict__ z, CGState* st,
+                                                           const Z* __restrict__ z, CGState* st,
                                                            ReduceScratch* ws)
 {
     __shared__ double red[32];
     double s = 0.0;
     for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
-        s = fma(z[i], r[i], s);
+        s = fma((double)z[i], r[i], s);
     s = block_sum(s, red);
     double total;
     if(grid_reduce(s, ws, kReduceBlocks, &total))
@@ -68,7 +72,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_rtz(int n, const double* 
     }
 }
 
-__global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const double* __restrict__ z, double* __restrict__ p,
+template <typename Z>
+__global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const Z* __restrict__ z, double* __restrict__ p,
                                                      const CGState* __restrict__ st)
 {
     const int i = blockIdx.x * kBS + threadIdx.x;
@@ -77,8 +82,9 @@ __global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const double* __rest
     // back: p = z (a restart: the old directions belong to the other
     // preconditioner)
     const bool restart = st->k == 1 || (st->fallback_iter > 0 && st->k == st->fallback_iter + 1);
-    if(restart) p[i] = fma(0.0, z[i], z[i]);         // WAXPBY(1, z, 0, z)
-    else p[i] = fma(st->beta, p[i], z[i]);          // WAXPBY(1, z, beta, p)
+    const double zi = (double)z[i];
+    if(restart) p[i] = fma(0.0, zi, zi);            // WAXPBY(1, z, 0, z)
+    else p[i] = fma(st->beta, p[i], zi);           // WAXPBY(1, z, beta, p)
 }
 
 // Ap = A p (one row per thread, colour-interleaved blocks as k_spmv) and
@@ -160,10 +166,11 @@ __global__ void __launch_bounds__(kBS) k_cg_pap_chunks(ColorChunks cc, const dou
     }
 }
 
+template <typename Z>
 __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const double* __restrict__ p,
                                                                  const double* __restrict__ Ap,
                                                                  double* __restrict__ r, double* __restrict__ x,
-                                                                 const double* __restrict__ z, CGState* st,
+                                                                 const Z* __restrict__ z, CGState* st,
                                                                  ReduceScratch* ws)
 {
     __shared__ double red[32];
@@ -176,7 +183,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const do
         r[i] = v;
         s = fma(v, v, s);
         x[i] = fma(alpha, p[i], x[i]);               // WAXPBY(1, x, alpha, p)
-        if(flex) sf = fma(z[i], v, sf);
+        if(flex) sf = fma((double)z[i], v, sf);
     }
     double t1, t2;
     bool last;
@@ -205,7 +212,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const do
 // the WHILE node ends after at most max_iter iterations whatever the
 // reductions produced.  src/CG.cpp:148: continue while k <= max_iter &&
 // normr/normr0 > tol (a NaN residual compares false and ends the loop).
-__global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watch_net)
+__device__ __forceinline__ void cg_loop_control(CGState* st, unsigned long long cond, int watch_net)
 {
     const int k = st->k;
     st->niters = k;
@@ -231,6 +238,94 @@ __global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watc
     unsigned go = (k + 1 <= st->max_iter) && (st->normr / st->normr0 > st->tol);
     if(watch_net && st->net == 2) go = 0;
     if(cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, go);
+}
+
+__global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watch_net)
+{
+    cg_loop_control(st, cond, watch_net);
+}
+
+// ------------------------------------------------------- two-kernel CG step
+// src/CG.cpp:148-184 as two kernels.  Step 1 (persistent, cooperative):
+// r.z over each block's row range, grid barrier, beta (every block sums the
+// per-block partials in index order, so all agree), p = z + beta p, grid
+// barrier, Ap = A p with the p.Ap partials, alpha from the last block.  Step
+// 2: r -= alpha Ap, x += alpha p, ||r|| (and the flexible-CG term), the last
+// block also running the loop control.  p is read and written through L2
+// only in the p update, so no SM holds a stale line of it when the product
+// gathers it after the barrier.
+
+// Step 1 with the ELL product (colour-interleaved chunks, one row per thread).
+template <typename Z>
+__global__ void __launch_bounds__(kBS) k_cg_step1_ell(int n, ColorChunks cc, const int* __restrict__ ell_col,
+                                                      const double* __restrict__ ell_val, const double* __restrict__ r,
+                                                      const Z* __restrict__ z, double* __restrict__ p,
+                                                      double* __restrict__ Ap, CGState* st, double* partial,
+                                                      unsigned int* ticket, GridBarrier* gb)
+{
+    if(!step1_rz_p(n, r, z, p, st, partial, gb)) return;
+    double s = 0.0;
+    for(int c = blockIdx.x; c < cc.nchunks(); c += gridDim.x)
+    {
+        int row;
+        if(!cc.row_of(c, threadIdx.x, row)) continue;
+        double sum = 0.0;
+#pragma unroll
+        for(int q = 0; q < kWidth; ++q)
+        {
+            const size_t idx = (size_t)q * n + row;
+            const int col = ld_stream(ell_col + idx);
+            const double v = ld_stream(ell_val + idx);
+            if(col >= 0 && col < n) sum = fma(v, p[col], sum);
+        }
+        Ap[row] = sum;
+        s = fma(sum, p[row], s);
+    }
+    step1_alpha(s, st, partial, ticket);
+}
+
+// Step 2: the r/x update of k_cg_update_xr with the loop control in its last block.
+template <typename Z>
+__global__ void __launch_bounds__(kReduceThreads) k_cg_step2(int n, const double* __restrict__ p,
+                                                             const double* __restrict__ Ap, double* __restrict__ r,
+                                                             double* __restrict__ x, const Z* __restrict__ z,
+                                                             CGState* st, ReduceScratch* ws, unsigned long long cond,
+                                                             int watch_net)
+{
+    __shared__ double red[32];
+    const double alpha = st->alpha;
+    const bool flex = st->flexible != 0;
+    double s = 0.0, sf = 0.0;
+    for(long long i = (long long)blockIdx.x * kReduceThreads + threadIdx.x; i < n; i += kReduceBlocks * kReduceThreads)
+    {
+        const double v = fma(-alpha, Ap[i], r[i]);
+        r[i] = v;
+        s = fma(v, v, s);
+        x[i] = fma(alpha, p[i], x[i]);
+        if(flex) sf = fma((double)z[i], v, sf);
+    }
+    double t1, t2;
+    bool last;
+    if(flex)
+    {
+        s = block_sum(s, red);
+        sf = block_sum(sf, red);
+        last = grid_reduce2(s, sf, ws, kReduceBlocks, &t1, &t2);
+    }
+    else
+    {
+        s = block_sum(s, red);
+        last = grid_reduce(s, ws, kReduceBlocks, &t1);
+        t2 = 0.0;
+    }
+    if(last)
+    {
+        const double nr = sqrt(t1);
+        st->normr = nr;
+        st->rtz_flex = t2;
+        st->hist[st->k] = nr;
+        cg_loop_control(st, cond, watch_net);
+    }
 }
 
 __global__ void k_cg_timer(CGState* st, int phase)
@@ -261,16 +356,34 @@ int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGS
     return 0;
 }
 
-int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s)
+template <typename Z>
+static int rtz_impl(int n, const double* r, const Z* z, CGState* st, ReduceScratch* ws, cudaStream_t s)
 {
-    k_cg_rtz<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, st, ws);
+    k_cg_rtz<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, st, ws);
     HB_LAUNCHED();
     return 0;
 }
 
+int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s)
+{
+    return rtz_impl(n, r, z, st, ws, s);
+}
+
+int launch_cg_rtz(int n, const double* r, const float* z, CGState* st, ReduceScratch* ws, cudaStream_t s)
+{
+    return rtz_impl(n, r, z, st, ws, s);
+}
+
 int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s)
 {
-    k_cg_update_p<<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
+    k_cg_update_p<double><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_update_p(int n, const float* z, double* p, const CGState* st, cudaStream_t s)
+{
+    k_cg_update_p<float><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
     HB_LAUNCHED();
     return 0;
 }
@@ -292,14 +405,68 @@ int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const do
     return 0;
 }
 
-int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+template <typename Z>
+static int update_xr_impl(int n, const double* p, const double* Ap, double* r, double* x, const Z* z, CGState* st,
+                          ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    k_cg_update_xr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
+    k_cg_update_xr<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
     HB_LAUNCHED();
     k_cg_loop_control<<<1, 1, 0, s>>>(st, cond, watch_net);
     HB_LAUNCHED();
     return 0;
+}
+
+int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+{
+    return update_xr_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+}
+
+int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const float* z,
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+{
+    return update_xr_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+}
+
+// ---- two-kernel CG step
+template <typename Z>
+static int step1_ell_impl(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
+                          const Z* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
+                          cudaStream_t s)
+{
+    static const int grid = resident_grid(k_cg_step1_ell<Z>, kBS, kReduceBlocks);
+    if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "CG step: no resident grid");
+    HB_CUDA(launch_coop(k_cg_step1_ell<Z>, grid, kBS, s, n, cc, ell_col, ell_val, r, z, p, Ap, st, ws->partial,
+                        &ws->ticket, gb));
+    return 0;
+}
+
+int launch_cg_step1_ell(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
+                        const double* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
+                        cudaStream_t s)
+{
+    return step1_ell_impl(n, cc, ell_col, ell_val, r, z, p, Ap, st, ws, gb, s);
+}
+
+template <typename Z>
+static int step2_impl(int n, const double* p, const double* Ap, double* r, double* x, const Z* z, CGState* st,
+                      ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+{
+    k_cg_step2<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws, cond, watch_net);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const double* z, CGState* st,
+                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+{
+    return step2_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+}
+
+int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const float* z, CGState* st,
+                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+{
+    return step2_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
 }
 
 int launch_cg_timer(CGState* st, int phase, cudaStream_t s)

@@ -37,6 +37,87 @@ struct CGState
     double hist[1];       // normr after preamble and after each iteration (max_iter+1 entries)
 };
 
+// ---- device helpers of the two-kernel CG step (k_cg_step1_* kernels)
+// Per-block row range of the vector phases (a multiple of 32 rows, so that
+// no 256-byte line is shared by two blocks' writes).
+__device__ __forceinline__ void step_rows(long long n, long long& lo, long long& hi)
+{
+    const long long per = (((n + gridDim.x - 1) / gridDim.x) + 31) & ~31ll;
+    lo = (long long)blockIdx.x * per;
+    hi = lo + per < n ? lo + per : n;
+}
+
+// Phase 1 and 2 of step 1: beta from r.z, then p = z + beta p.  Returns false
+// when a barrier timed out.
+template <typename Z>
+__device__ __forceinline__ bool step1_rz_p(long long n, const double* __restrict__ r, const Z* __restrict__ z,
+                                           double* __restrict__ p, CGState* st, double* partial, GridBarrier* gb)
+{
+    __shared__ double red[32];
+    __shared__ double sh_beta;
+    const int tid = threadIdx.x;
+    long long lo, hi;
+    step_rows(n, lo, hi);
+    const int k = st->k;
+    const bool restart = k == 1 || (st->fallback_iter > 0 && k == st->fallback_iter + 1);
+    const double old_rtz = st->rtz, rtz_flex = st->rtz_flex;
+    const bool flex = st->flexible != 0;
+    double s = 0.0;
+    for(long long i = lo + tid; i < hi; i += blockDim.x) s = fma((double)z[i], r[i], s);
+    s = block_sum(s, red);
+    if(tid == 0) partial[blockIdx.x] = s;
+    if(!grid_barrier(gb, gridDim.x, &st->status)) return false;
+    double acc = 0.0;
+    for(int i = tid; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(&partial[i]);
+    acc = block_sum(acc, red);
+    if(tid == 0)
+    {
+        const double beta = k == 1 ? 0.0 : (flex ? acc - rtz_flex : acc) / old_rtz;
+        sh_beta = beta;
+        if(blockIdx.x == 0)
+        {
+            if(k != 1) st->oldrtz = old_rtz;
+            st->rtz = acc;
+            st->beta = beta;
+        }
+    }
+    __syncthreads();
+    const double beta = sh_beta;
+    for(long long i = lo + tid; i < hi; i += blockDim.x)
+    {
+        const double zi = (double)z[i];
+        __stcg(p + i, restart ? fma(0.0, zi, zi) : fma(beta, __ldcg(p + i), zi));
+    }
+    return grid_barrier(gb, gridDim.x, &st->status);
+}
+
+// The last block to arrive forms pAp (partials in block order) and alpha.
+__device__ __forceinline__ void step1_alpha(double s, CGState* st, double* partial, unsigned int* ticket)
+{
+    __shared__ double red[32];
+    __shared__ bool last;
+    s = block_sum(s, red);
+    if(threadIdx.x == 0)
+    {
+        partial[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for(int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(&partial[i]);
+    acc = block_sum(acc, red);
+    if(threadIdx.x == 0)
+    {
+        *ticket = 0;
+        st->pAp = acc;
+        st->alpha = st->rtz / acc;
+    }
+}
+
+
 // Phases of an instrumented CG iteration (the reference's times[] slots 1, 2, 3, 5).
 enum CGPhase
 {
@@ -61,10 +142,13 @@ inline size_t cg_state_bytes(int max_iter) { return sizeof(CGState) + sizeof(dou
 // k = 1; returns whether iterations are needed through state.
 int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGState* st, ReduceScratch* ws,
                         cudaStream_t s);
-// rtz = r.z, beta = rtz/oldrtz (k>1), oldrtz kept.
+// rtz = r.z, beta = rtz/oldrtz (k>1), oldrtz kept.  The float forms read
+// the FP32 V-cycles' output directly (every value widened exactly).
 int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
+int launch_cg_rtz(int n, const double* r, const float* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
 // p = z (k == 1) or p = z + beta p.
 int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s);
+int launch_cg_update_p(int n, const float* z, double* p, const CGState* st, cudaStream_t s);
 // Ap = A p and alpha = rtz / (p.Ap); `partial` holds cc.nchunks() per-block
 // sums, `ticket` must start at zero and is left at zero.
 int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
@@ -81,6 +165,23 @@ int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const do
 // normr marks it failed (net = 2); with watch_net the loop then also ends.
 int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
                         CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const float* z,
+                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+
+// Two-kernel CG step (src/CG.cpp:148-184).  Step 1 (persistent, cooperative,
+// two bounded grid barriers): rtz = r.z and beta, p = z + beta p, Ap = A p
+// with pAp and alpha; it uses ws's partials and ticket (left at zero) and the
+// grid barrier gb (count zero before the launch, left at zero).  Step 2:
+// r -= alpha Ap, x += alpha p, normr, then the loop control (as
+// launch_cg_update_xr, in one kernel).  A barrier that times out sets
+// st->status.
+int launch_cg_step1_ell(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
+                        const double* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
+                        cudaStream_t s);
+int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const double* z, CGState* st,
+                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const float* z, CGState* st,
+                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
 
 // One thread: adds the time since the previous stamp to phase_ns[phase]
 // (phase kPhaseStart only stamps).  Kernels on one stream run in order, so

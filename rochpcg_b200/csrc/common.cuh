@@ -32,6 +32,33 @@ int cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Prolongation fused into a coarse level's smoother: the pass that gives a
+// row its final value of the coarse solve also adds it into the finer level,
+// xf[pro_f[row]] += x_new -- what src/ComputeProlongation.cpp:39-59 does
+// after the coarse level returns (the fine vector is not touched while the
+// coarse level runs, and each coarse row has one injected fine row).
+// xf == nullptr: this pass does no prolongation.
+template <typename T>
+struct Prolong
+{
+    T* xf = nullptr;
+    const int* pro_f = nullptr;  // coarse permuted row -> fine permuted row
+    __device__ __forceinline__ void add(int row, T v) const
+    {
+        if(xf) xf[pro_f[row]] += v;
+    }
+    // four consecutive rows (row0 % 4 == 0)
+    __device__ __forceinline__ void add4(int row0, const T (&v)[4]) const
+    {
+        if(!xf) return;
+        const int4 f = *reinterpret_cast<const int4*>(pro_f + row0);
+        xf[f.x] += v[0];
+        xf[f.y] += v[1];
+        xf[f.z] += v[2];
+        xf[f.w] += v[3];
+    }
+};
+
 // ---- programmatic dependent launch
 // launch_pdl() starts a kernel whose blocks may become resident while the
 // previous kernel of the stream is still finishing (once every block of that
@@ -66,6 +93,71 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, c
     const bool capturing = cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
     cfg.numAttrs = pdl_enabled() && !capturing ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Programmatic dependent launch for the learned smoother's kernels, inside
+// graphs too: each of them starts its dependents at entry, runs its prologue
+// (weights to shared memory, barriers, tensor memory) while the previous
+// kernel finishes, and waits (pdl_wait) before it touches that kernel's
+// output.  256^3 learned V-cycle 0.784 -> 0.773 ms, solve 0.178 -> 0.176 s
+// (A/B on one box); HPCGB200_NET_PDL=0 turns it off.
+inline bool net_pdl_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("HPCGB200_NET_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl_net(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  Args&&... args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = net_pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Cooperative launch (every block resident at once, or the launch fails):
+// for the persistent kernels whose blocks meet at grid barriers.  Valid in
+// stream capture (the graph's kernel node keeps the attribute).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_coop(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s,
+                               Args&&... args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Blocks of `kernel` that fit on the device at once (SMs x resident blocks
+// per SM), at most `cap`.
+template <typename K>
+inline int resident_grid(K kernel, int block, int cap)
+{
+    int dev = 0, sms = 0, per = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0) != cudaSuccess) return 0;
+    const int g = sms * per;
+    return g < cap ? g : cap;
 }
 
 }  // namespace hb
@@ -105,6 +197,11 @@ __device__ __forceinline__ void pdl_begin()
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+
+// The two halves of pdl_begin() for kernels with a prologue that does not
+// read the previous kernel's output (no-ops without the launch attribute).
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Streaming (read-once) loads for matrix data: evict-first in L2 so that the
 // vectors gathered by the stencil stay resident.
@@ -200,6 +297,57 @@ __device__ __forceinline__ bool grid_reduce(double block_partial, ReduceScratch*
         *total = acc;
     }
     return threadIdx.x == 0;
+}
+
+// Grid-wide barrier of a persistent kernel launched cooperatively (every
+// block resident).  Generation counting: a block reads the generation, then
+// arrives; the last to arrive resets the count and bumps the generation; the
+// others wait for the bump.  The wait is bounded (about a second): on time-out
+// it sets *status and returns false, so a kernel launched without its blocks
+// co-resident ends with an error instead of hanging.  Starts and ends with
+// count == 0.
+struct GridBarrier
+{
+    unsigned int count;
+    unsigned int gen;
+};
+
+constexpr long long kBarrierSpins = 1ll << 24;  // x 64 ns of back-off
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int nblocks, int* status)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if(threadIdx.x == 0)
+    {
+        ok = 1;
+        volatile unsigned int* gen = &gb->gen;
+        const unsigned int g = *gen;
+        __threadfence();
+        if(atomicAdd(&gb->count, 1u) == nblocks - 1)
+        {
+            gb->count = 0;
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        }
+        else
+        {
+            long long spins = 0;
+            while(*gen == g)
+            {
+                if(++spins > kBarrierSpins)
+                {
+                    atomicExch(status, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
 }
 
 // Two sums at once (same protocol as grid_reduce).

@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
              const __nv_bfloat16* __restrict__ act, PermMap pm, int* status)
 {
     extern __shared__ unsigned char smem_raw[];
+    pdl_launch_dependents();  // the next kernel may start its prologue
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sA = smem;                                   // kStages x kStageBytes
     unsigned char* sW = smem + kStages * kStageBytes;           // weights
@@ -353,6 +354,7 @@ __global__ void __launch_bounds__(kConvThreads, HB_CONV_CTAS)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tholder;
+    pdl_wait();  // from here on the previous kernel's output is read
 
     if(warp == 0 && lane == 0)
     {
@@ -601,6 +603,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 PermMap pm, int* status)
 {
     extern __shared__ unsigned char smem_raw[];
+    pdl_launch_dependents();  // the next kernel may start its prologue
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sA = smem;                                       // k3Stages x k3StageBytes
     unsigned char* sW = smem + k3Stages * k3StageBytes;             // + and - weight tiles
@@ -649,6 +652,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tholder;
+    pdl_wait();  // from here on the previous kernel's output is read
     constexpr uint32_t kBoxTx = (uint32_t)(k3Rows * kRowBytes) * (kPair ? 2u : 1u);
 
     if(warp == 0 && lane == 0)
@@ -1106,6 +1110,7 @@ __global__ void k_embed_scalar_level(PermMap pm, int nz, int ny, int nx, const f
                                      const float* __restrict__ x, const float* __restrict__ diag32,
                                      __nv_bfloat16* __restrict__ s1)
 {
+    pdl_begin();
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= (long)nz * ny * nx) return;
     const int z = (int)(p / ((long)ny * nx));
@@ -1169,6 +1174,7 @@ __global__ void __launch_bounds__(k1Threads) k_layer1_tc(ConvGrid g, const Tin* 
                                                          __nv_bfloat16* __restrict__ a1, int* status)
 {
     extern __shared__ unsigned char smem_raw[];
+    pdl_launch_dependents();  // the next kernel may start its prologue
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sA = smem;                           // k1Z im2col planes
     unsigned char* sW = sA + k1Z * k1PlaneBytes;        // weights
@@ -1190,6 +1196,7 @@ __global__ void __launch_bounds__(k1Threads) k_layer1_tc(ConvGrid g, const Tin* 
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tholder;
+    pdl_wait();  // from here on the previous kernel's output is read
 
     const long n = g.points();
     const int tx = (g.nx + k1X - 1) / k1X, ty = (g.ny + k1Y - 1) / k1Y, tz = (g.nz + k1Z - 1) / k1Z;
@@ -1469,9 +1476,8 @@ static int conv_launch(const ConvGrid& g, const void* in, const void* wB, void* 
     const long tiles = (long)g.nb * ((g.nx + kOX - 1) / kOX) * ((g.ny + kTY - 1) / kTY) * ((g.nz + kTZ - 1) / kTZ);
     const long cap = (long)HB_CONV_CTAS * sm_count();
     const int grid = (int)(tiles < cap ? tiles : cap);
-    k_conv16<kOut><<<grid, kConvThreads, kConvSmem, s>>>(map, g, (const __nv_bfloat16*)wB, out,
-                                                         (const __nv_bfloat16*)act, pm, status);
-    HB_LAUNCHED();
+    HB_CUDA(launch_pdl_net(k_conv16<kOut>, dim3(grid), dim3(kConvThreads), (size_t)kConvSmem, s, map, g,
+                           (const __nv_bfloat16*)wB, out, (const __nv_bfloat16*)act, pm, status));
     return 0;
 }
 
@@ -1508,8 +1514,8 @@ static int layer3_launch(const ConvGrid& g, const void* a2, const float* w3, flo
     const long tiles = (long)g.nb * ((g.nx + k3X - 1) / k3X) * ((g.ny + k3Y - 1) / k3Y) * ((g.nz + k3Z - 1) / k3Z);
     const long cap = sm_count();
     const int grid = (int)(tiles < cap ? tiles : cap);
-    k_layer3_tc<kOut, kPair><<<grid, kConvThreads, k3Smem, s>>>(map, g, w3, out, pm, status);
-    HB_LAUNCHED();
+    HB_CUDA(launch_pdl_net(k_layer3_tc<kOut, kPair>, dim3(grid), dim3(kConvThreads), (size_t)k3Smem, s, map, g, w3,
+                           out, pm, status));
     return 0;
 }
 
@@ -1585,9 +1591,8 @@ int launch_embed_scalar_level(const PermMap& pm, int nz, int ny, int nx, const f
                               const float* diag32, void* s1, cudaStream_t s)
 {
     const long n = (long)nz * ny * nx;
-    k_embed_scalar_level<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pm, nz, ny, nx, r, x, diag32,
-                                                                     (__nv_bfloat16*)s1);
-    HB_LAUNCHED();
+    HB_CUDA(launch_pdl_net(k_embed_scalar_level, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, s, pm, nz, ny, nx, r,
+                           x, diag32, (__nv_bfloat16*)s1));
     return 0;
 }
 
@@ -1605,8 +1610,8 @@ static int layer1_launch(const ConvGrid& g, const Tin* in, const float* w1, __nv
     const long tiles = (long)g.nb * ((g.nx + k1X - 1) / k1X) * ((g.ny + k1Y - 1) / k1Y) * ((g.nz + k1Z - 1) / k1Z);
     const long cap = (long)k1CtasPerSm * sm_count();
     const int grid = (int)(tiles < cap ? tiles : cap);
-    k_layer1_tc<Tin, kPair><<<grid, k1Threads, k1Smem, s>>>(g, in, w1, a1, status);
-    HB_LAUNCHED();
+    HB_CUDA(launch_pdl_net(k_layer1_tc<Tin, kPair>, dim3(grid), dim3(k1Threads), (size_t)k1Smem, s, g, in, w1, a1,
+                           status));
     return 0;
 }
 

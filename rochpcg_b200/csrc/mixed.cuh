@@ -63,12 +63,14 @@ int launch_diag32(int m, const double* diag, float* diag32, float* inv_diag32, c
 // Zero-guess symmetric GS (forward colours 0..n-1, backward n-2..0).  When
 // r64 is non-null the forward sweeps read the FP64 residual and also store
 // its float value into r32 (fusing the down-conversion).
+// pro: the prolongation into the finer level, fused into the passes that
+// finalize rows (colour n-1's forward pass, every backward pass).
 int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float* inv_diag32, const double* r64,
-                        float* r32, float* x, cudaStream_t s);
+                        float* r32, float* x, cudaStream_t s, Prolong<float> pro = {});
 // Full symmetric GS step.  When z64 is non-null every row's final value is
 // also stored as double there (fusing the up-conversion).
 int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* r, float* x, double* z64,
-                   cudaStream_t s);
+                   cudaStream_t s, Prolong<float> pro = {});
 // rc[inj_c[i]] = rf[inj_f[i]] - (A xf)[inj_f[i]].
 int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const int* inj_c, const float* diag32,
                       const float* rf, const float* xf, float* rc, cudaStream_t s);
@@ -82,8 +84,9 @@ int launch32_prolong(const StencilLevel& Lf, int nc, const int* inj_f, const int
 // multiple of 4 (else HPCGB200_ERR_ARG).
 bool stencil_vec4(const StencilLevel& L);
 int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double* inv_diag, const double* r,
-                         double* x, cudaStream_t s);
-int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double* r, double* x, cudaStream_t s);
+                         double* x, cudaStream_t s, Prolong<double> pro = {});
+int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double* r, double* x, cudaStream_t s,
+                    Prolong<double> pro = {});
 int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const double* diag, const double* rf,
                        const double* xf, double* rc, cudaStream_t s);
 int launch64v_prolong(const StencilLevel& Lf, int nc, const int* inj_c, const double* xc, double* xf, cudaStream_t s);
@@ -100,6 +103,10 @@ int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x
 // `partial` (stencil_pap_partials(L) entries), `ticket` must start at zero and
 // is left at zero.
 size_t stencil_pap_partials(const StencilLevel& L);
+// Step 1 of the two-kernel CG step (launch_cg_step1_ell) with the separable
+// product, for the FP32 V-cycles' output z; canonical colouring only.
+int launch_cg_step1_sep(const StencilLevel& L, const double* diag, const double* r, const float* z, double* p,
+                        double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s);
 int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
 

@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kBS) k_spmv(int m, ColorChunks cc, const int* 
 __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset, const int* __restrict__ ell_col,
                                                      const double* __restrict__ ell_val,
                                                      const double* __restrict__ inv_diag,
-                                                     const double* __restrict__ r, double* x)
+                                                     const double* __restrict__ r, double* x, Prolong<double> pro)
 {
     const int gid = blockIdx.x * kBS + threadIdx.x;
     if(gid >= size) return;
@@ -107,7 +107,9 @@ __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset
     const double sum = ell_row_sum(
         m, row, ell_col, ell_val, x, r[row], -1.0, [](int) { return true; },
         [m, row](int col) { return col >= 0 && col < m && col != row; });
-    x[row] = sum * inv_diag[row];
+    const double v = sum * inv_diag[row];
+    x[row] = v;
+    pro.add(row, v);
 }
 
 // src/ComputeSYMGS.cpp:238-295 (kernel_pointwise_mult + kernel_forward_sweep_0):
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
                                                     const double* __restrict__ ell_val,
                                                     const int* __restrict__ diag_idx,
                                                     const double* __restrict__ inv_diag,
-                                                    const double* __restrict__ r, double* x)
+                                                    const double* __restrict__ r, double* x, Prolong<double> pro)
 {
     const int gid = blockIdx.x * kBS + threadIdx.x;
     if(gid >= size) return;
@@ -131,14 +133,17 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
             m, row, ell_col, ell_val, x, sum, -1.0, [diag](int p) { return p < diag; },
             [offset](int col) { return col >= 0 && col < offset; });
     }
-    x[row] = sum * inv_diag[row];
+    const double v = sum * inv_diag[row];
+    x[row] = v;
+    pro.add(row, v);
 }
 
 // src/ComputeSYMGS.cpp:297-341 (kernel_backward_sweep_0).
 __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset, const int* __restrict__ ell_col,
                                                     const double* __restrict__ ell_val,
                                                     const int* __restrict__ diag_idx, const double* __restrict__ diag,
-                                                    const double* __restrict__ inv_diag, double* x)
+                                                    const double* __restrict__ inv_diag, double* x,
+                                                    Prolong<double> pro)
 {
     const int gid = blockIdx.x * kBS + threadIdx.x;
     if(gid >= size) return;
@@ -147,7 +152,9 @@ __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset,
     const double sum = ell_row_sum(
         m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, [d](int p) { return p > d; },
         [offset, m](int col) { return col >= offset && col < m; });
-    x[row] = sum * inv_diag[row];
+    const double v = sum * inv_diag[row];
+    x[row] = v;
+    pro.add(row, v);
 }
 
 // ---------------------------------------------------------- restriction
@@ -257,21 +264,25 @@ int launch_spmv(int m, const ColorChunks& cc, const int* ell_col, const double* 
     return 0;
 }
 
+// A colour's rows are final after its backward pass, or after its forward
+// pass when the backward sweep (colours ublocks..0) does not revisit it: the
+// passes that carry the fused prolongation.
 int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
-                 const double* ell_val, const double* inv_diag, const double* r, double* x, cudaStream_t s)
+                 const double* ell_val, const double* inv_diag, const double* r, double* x, cudaStream_t s,
+                 Prolong<double> pro)
 {
     for(int i = 0; i < nblocks; ++i)
     {
         if(sizes[i] <= 0) continue;
         k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, inv_diag,
-                                                                 r, x);
+                                                                 r, x, i > ublocks ? pro : Prolong<double>{});
         HB_LAUNCHED();
     }
     for(int i = ublocks; i >= 0; --i)
     {
         if(sizes[i] <= 0) continue;
         k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, inv_diag,
-                                                                 r, x);
+                                                                 r, x, pro);
         HB_LAUNCHED();
     }
     return 0;
@@ -279,22 +290,36 @@ int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* o
 
 int launch_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                       const double* ell_val, const int* diag_idx, const double* diag, const double* inv_diag,
-                      const double* r, double* x, cudaStream_t s)
+                      const double* r, double* x, cudaStream_t s, Prolong<double> pro)
 {
     for(int i = 0; i < nblocks; ++i)
     {
         if(sizes[i] <= 0) continue;
         k_symgs_fwd0<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx,
-                                                                inv_diag, r, x);
+                                                                inv_diag, r, x, i > ublocks ? pro : Prolong<double>{});
         HB_LAUNCHED();
     }
     for(int i = ublocks; i >= 0; --i)
     {
         if(sizes[i] <= 0) continue;
         k_symgs_bwd0<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx,
-                                                                diag, inv_diag, x);
+                                                                diag, inv_diag, x, pro);
         HB_LAUNCHED();
     }
+    return 0;
+}
+
+__global__ void k_prolong_map(int nc, const int* __restrict__ inj_f, const int* __restrict__ inj_c,
+                              int* __restrict__ pro_f)
+{
+    const int ic = blockIdx.x * kBS + threadIdx.x;
+    if(ic < nc) pro_f[inj_c[ic]] = inj_f[ic];
+}
+
+int launch_prolong_map(int nc, const int* inj_f, const int* inj_c, int* pro_f, cudaStream_t s)
+{
+    k_prolong_map<<<(nc + kBS - 1) / kBS, kBS, 0, s>>>(nc, inj_f, inj_c, pro_f);
+    HB_LAUNCHED();
     return 0;
 }
 

@@ -31,11 +31,16 @@ ColorChunks make_chunks(int m, int ncolors, const int* offsets);
 
 int launch_spmv(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* x, double* y,
                 cudaStream_t s);
+// pro: the prolongation into the finer level fused into the passes that
+// finalize rows (used on coarse levels; empty by default).
 int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
-                 const double* ell_val, const double* inv_diag, const double* r, double* x, cudaStream_t s);
+                 const double* ell_val, const double* inv_diag, const double* r, double* x, cudaStream_t s,
+                 Prolong<double> pro = {});
 int launch_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                       const double* ell_val, const int* diag_idx, const double* diag, const double* inv_diag,
-                      const double* r, double* x, cudaStream_t s);
+                      const double* r, double* x, cudaStream_t s, Prolong<double> pro = {});
+// pro_f[inj_c[ic]] = inj_f[ic]: coarse permuted row -> injected fine permuted row.
+int launch_prolong_map(int nc, const int* inj_f, const int* inj_c, int* pro_f, cudaStream_t s);
 int launch_restrict(int nc, const int* inj_f, const int* inj_c, int mf, const int* ell_col, const double* ell_val,
                     const double* rf, const double* xf, double* rc, cudaStream_t s);
 int launch_restrict_axf(int nc, const int* inj_f, const int* inj_c, const double* rf, const double* axf, double* rc,

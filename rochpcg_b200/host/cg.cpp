@@ -24,6 +24,7 @@ namespace hpcg_b200 {
 
 static void ensure_state(LevelOpt* o, int max_iter)
 {
+    if(!o->step_barrier) o->step_barrier = dalloc<hb::GridBarrier>(1);
     if(o->cg_state && o->cg_state_iters >= max_iter) return;
     const int cap = max_iter < 1024 ? 1024 : max_iter;
     dfree(o->cg_state);
@@ -38,6 +39,24 @@ static void ensure_state(LevelOpt* o, int max_iter)
     o->graphs.clear();
 }
 
+// The CG step after the preconditioner as two kernels (rtz + p update + SpMV
+// + pAp, then r/x update + normr + loop control) or five (rtz, p update,
+// SpMV + pAp, r/x update, loop control).  Measured on B200 (A/B on one box):
+// mixed 320^3 0.3800 vs 0.3826 s, so the FP32 V-cycle modes take two by
+// default; FP64 ELL 256^3 0.6889 vs 0.6893 s, a wash, so it keeps five, whose
+// reduction partitions the FP64 stencil mode shares for its bit-identical
+// history.  HPCGB200_CG_STEP=2 / =5 selects two / five kernels for every mode
+// that has both (untimed bodies only; the phase-timed body keeps five).
+static bool cg_step2_for(MGPrecision prec)
+{
+    static const int forced = [] {
+        const char* e = std::getenv("HPCGB200_CG_STEP");
+        return e && e[0] == '2' ? 2 : (e && e[0] == '5' ? 5 : 0);
+    }();
+    if(forced) return forced == 2;
+    return prec == MGPrecision::FP32 || prec == MGPrecision::LEARNED;
+}
+
 // timed: phase timers around the operators (reference times[] slots: MG,
 // r.z -> dot, p update -> WAXPBY, SpMV with p.Ap -> SpMV, r/x update with
 // ||r|| -> WAXPBY).
@@ -47,12 +66,18 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     const int n = A.localNumberOfRows;
     auto stamp = [&](int phase) { return timed ? hb::launch_cg_timer(st, phase, s) : 0; };
     HB_RETURN_IF(stamp(hb::kPhaseStart));
+    // the FP32 V-cycles' output is read in FP32 by the CG kernels (z32)
+    const float* z32 = nullptr;
     if(precond)
     {
         if(prec == MGPrecision::FP64) HB_RETURN_IF(ComputeMG(A, data.r, data.z));
         else if(prec == MGPrecision::FP64_STENCIL) HB_RETURN_IF(ComputeMG_Stencil(A, data.r, data.z));
-        else if(prec == MGPrecision::FP32) HB_RETURN_IF(ComputeMG_Mixed(A, data.r, data.z));
-        else HB_RETURN_IF(ComputeMG_Learned(A, data.r, data.z));
+        else
+        {
+            if(prec == MGPrecision::FP32) HB_RETURN_IF(mg_mixed_to(A, data.r.d_values, nullptr, s));
+            else HB_RETURN_IF(mg_learned_to(A, data.r.d_values, nullptr, s));
+            z32 = opt(A)->z32;
+        }
     }
     else
     {
@@ -61,9 +86,27 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
         if(e != cudaSuccess) return hb::cuda_error(e, "copy r to z", __FILE__, __LINE__);
     }
     HB_RETURN_IF(stamp(hb::kPhaseMG));
-    HB_RETURN_IF(hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
+    const int watch = prec == MGPrecision::LEARNED ? 1 : 0;
+    if(!timed && cg_step2_for(prec) && (prec == MGPrecision::FP64 || z32))
+    {
+        LevelOpt* o = opt(A);
+        if(z32)
+            HB_RETURN_IF(hb::launch_cg_step1_sep(o->st, o->diag, data.r.d_values, z32, data.p.d_values,
+                                                 data.Ap.d_values, st, rt().ws, o->step_barrier, s));
+        else
+            HB_RETURN_IF(hb::launch_cg_step1_ell(n, o->cc, A.ell_col_ind, A.ell_val, data.r.d_values,
+                                                 data.z.d_values, data.p.d_values, data.Ap.d_values, st, rt().ws,
+                                                 o->step_barrier, s));
+        return z32 ? hb::launch_cg_step2(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values, z32, st,
+                                         rt().ws, cond, watch, s)
+                   : hb::launch_cg_step2(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
+                                         data.z.d_values, st, rt().ws, cond, watch, s);
+    }
+    HB_RETURN_IF(z32 ? hb::launch_cg_rtz(n, data.r.d_values, z32, st, rt().ws, s)
+                     : hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
     HB_RETURN_IF(stamp(hb::kPhaseDot));
-    HB_RETURN_IF(hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
+    HB_RETURN_IF(z32 ? hb::launch_cg_update_p(n, z32, data.p.d_values, st, s)
+                     : hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
     HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
     if(prec == MGPrecision::FP64_STENCIL)
     {
@@ -88,9 +131,10 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
                                             o->spmv_partial, o->spmv_ticket, s));
     }
     HB_RETURN_IF(stamp(hb::kPhaseSpmv));
-    HB_RETURN_IF(hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
-                                         data.z.d_values, st, rt().ws, cond, prec == MGPrecision::LEARNED ? 1 : 0,
-                                         s));
+    HB_RETURN_IF(z32 ? hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values, z32,
+                                               st, rt().ws, cond, watch, s)
+                     : hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
+                                               data.z.d_values, st, rt().ws, cond, watch, s));
     // (the r/x update kernel launches the loop control after itself; its
     // stamp below also covers that one-thread kernel)
     HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
@@ -256,8 +300,9 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
         HB_HOST_CUDA(cudaEventCreate(&e1));
         HB_HOST_CUDA(cudaEventRecord(e0, s));
         HB_HOST_CUDA(cudaMemcpyAsync(st, &h, offsetof(hb::CGState, hist), cudaMemcpyHostToDevice, s));
-        // fresh reduction tickets for every solve
+        // fresh reduction tickets and grid barrier for every solve
         HB_HOST_CUDA(cudaMemsetAsync(&rt().ws->ticket, 0, sizeof(unsigned int), s));
+        HB_HOST_CUDA(cudaMemsetAsync(o->step_barrier, 0, sizeof(hb::GridBarrier), s));
         if(o->pap_ticket) HB_HOST_CUDA(cudaMemsetAsync(o->pap_ticket, 0, sizeof(unsigned int), s));
         HB_HOST_CUDA(cudaMemsetAsync(o->spmv_ticket, 0, sizeof(unsigned int), s));
 
@@ -370,6 +415,9 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
                                     sizeof(double) * (h.niters + 1 - (restart_offset > 0)), cudaMemcpyDeviceToHost));
             for(int k = restart_offset + h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
         }
+        if(h.status)
+            return hb::record_error(HPCGB200_ERR_DEVICE_STATUS, "CG: a grid barrier of the CG step timed out (%d)",
+                                    h.status);
         o->last_fallback_iter = restart_offset > 0 ? restart_offset : h.fallback_iter;
         if(prec == MGPrecision::LEARNED) check(smoother_status(*o->smoother, s));
         niters = restart_offset + h.niters;

@@ -158,6 +158,7 @@ static void delete_level_opt(SparseMatrix& A)
     dfree(o->diag32);
     dfree(o->inv_diag32);
     dfree(o->cg_state);
+    dfree(o->step_barrier);
     dfree(o->r32);
     dfree(o->pap_partial);
     dfree(o->pap_ticket);
@@ -204,6 +205,7 @@ void DeleteMatrix(SparseMatrix& A)
         {
             dfree(mo->inj_f);
             dfree(mo->inj_c);
+            dfree(mo->pro_f);
             dfree(mo->rc32);
             dfree(mo->xc32);
             delete mo;

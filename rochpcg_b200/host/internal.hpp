@@ -110,6 +110,7 @@ struct LevelOpt
     // level-0 solver state
     hb::CGState* cg_state = nullptr;
     int cg_state_iters = 0;
+    hb::GridBarrier* step_barrier = nullptr;  // the two-kernel CG step's grid barrier (zeroed per solve)
     std::vector<std::unique_ptr<CGGraph>> graphs;
     double* pap_partial = nullptr;     // per-block partial sums of the stencil SpMV + p.Ap (level 0)
     unsigned int* pap_ticket = nullptr;
@@ -137,15 +138,29 @@ struct MGOpt
 {
     int* inj_f = nullptr;              // permuted fine row of coarse point i
     int* inj_c = nullptr;              // permuted coarse row of coarse point i
+    int* pro_f = nullptr;              // coarse permuted row -> injected fine permuted row (fused prolongation)
     float* rc32 = nullptr;
     float* xc32 = nullptr;
 };
+
+// Whether the V-cycles carry the prolongation in the coarse level's final
+// smoother passes (HPCGB200_FUSED_PROLONG=1) or run it as a launch of its own
+// after the coarse solve (default: measured faster on B200, the scattered
+// read-modify-writes in the coarse passes cost more than the launch they
+// save: 320^3 mixed V-cycle 1.291 vs 1.318 ms); both give the same bits.
+bool fused_prolongation();
 
 inline LevelOpt* opt(const SparseMatrix& A) { return static_cast<LevelOpt*>(A.optimizationData); }
 inline MGOpt* mgopt(const SparseMatrix& A) { return A.mgData ? static_cast<MGOpt*>(A.mgData->optimizationData) : nullptr; }
 
 // Operators on raw FP32 level data (mixed V-cycle), defined in operators.cpp.
-int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s);
+// pro: where this level's final values are prolongated (the finer level's x),
+// fused into the level's last smoother passes; empty on level 0.
+int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s, hb::Prolong<float> pro = {});
+// Level-0 FP32 V-cycles (mixed, learned) from the FP64 residual r64: the
+// result is left in opt(A)->z32, and also written to z64 when it is not null.
+int mg_mixed_to(const SparseMatrix& A, const double* r64, double* z64, cudaStream_t s);
+int mg_learned_to(const SparseMatrix& A, const double* r64, double* z64, cudaStream_t s);
 
 // Kernel launches of one CG iteration (captures the iteration graph if it
 // does not exist yet; nothing is launched), defined in cg.cpp.

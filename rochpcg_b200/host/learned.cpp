@@ -230,14 +230,19 @@ int smoother_ready(const SparseMatrix& A, cudaStream_t s)
     return smoother_prepare(*o->smoother, s);
 }
 
-// FP32 V-cycle below level 0 with the learned levels (same recursion as mg_fp32).
+// FP32 V-cycle below level 0 with the learned levels (same recursion as
+// mg_fp32).  A SymGS level takes the prolongation into the finer level in its
+// final passes (`pro`); below a learned level, or from one, it is a launch
+// of its own (the network is the level's last operation).
 static int mg_fp32_learned(const SparseMatrix& A, int level, Smoother& S, int first, int coarse_steps, const float* r,
-                           float* x, cudaStream_t s)
+                           float* x, cudaStream_t s, hb::Prolong<float> pro = {})
 {
     const LevelOpt* o = opt(A);
     const bool learned = level >= first;
     if(learned) HB_RETURN_IF(smoother_level_apply(S, *o, r, x, false, s));
-    else HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s));
+    else
+        HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s,
+                                             A.mgData ? hb::Prolong<float>{} : pro));
     if(!A.mgData)
     {
         // coarsest level: further learned Richardson steps x += N(r - A x)
@@ -246,20 +251,22 @@ static int mg_fp32_learned(const SparseMatrix& A, int level, Smoother& S, int fi
     }
     const MGOpt* mo = mgopt(A);
     const int nc = A.Ac->localNumberOfRows;
+    const bool separate_prolong = level + 1 >= first || !fused_prolongation();
     HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
-    HB_RETURN_IF(mg_fp32_learned(*A.Ac, level + 1, S, first, coarse_steps, mo->rc32, mo->xc32, s));
-    HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
+    HB_RETURN_IF(mg_fp32_learned(*A.Ac, level + 1, S, first, coarse_steps, mo->rc32, mo->xc32, s,
+                                 separate_prolong ? hb::Prolong<float>{} : hb::Prolong<float>{x, mo->pro_f}));
+    if(separate_prolong) HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
     if(learned) return smoother_level_apply(S, *o, r, x, true, s);
-    return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
+    return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s, pro);
 }
 
 }  // namespace hpcg_b200
 
-int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
+namespace hpcg_b200 {
+
+int mg_learned_to(const SparseMatrix& A, const double* r64, double* z64, cudaStream_t s)
 {
-    try
     {
-        ensure_runtime();
         const LevelOpt* o = opt(A);
         if(!o || !o->smoother)
             return hb::record_error(HPCGB200_ERR_ARG, "learned V-cycle: no smoother attached to the problem");
@@ -269,7 +276,6 @@ int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
                                         "learned V-cycle needs the 27-point stencil in parity colouring on every level");
         Smoother& S = *o->smoother;
         const int first = o->smoother_first_level;
-        cudaStream_t s = rt().stream;
         const int m = A.localNumberOfRows;
         if(first <= 0) return hb::record_error(HPCGB200_ERR_ARG, "learned V-cycle: the fine level keeps SymGS");
         // operand tiles are refreshed outside graph capture (a captured cycle
@@ -277,14 +283,27 @@ int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         HB_HOST_CUDA(cudaStreamIsCapturing(s, &cs));
         if(cs == cudaStreamCaptureStatusNone) HB_RETURN_IF(smoother_ready(A, s));
-        HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r.d_values, o->r32, o->z32, s));
-        if(!A.mgData) return hb::launch_cast_f2d(m, o->z32, x.d_values, s);
+        HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r64, o->r32, o->z32, s));
+        if(!A.mgData) return z64 ? hb::launch_cast_f2d(m, o->z32, z64, s) : 0;
         const MGOpt* mo = mgopt(A);
         const int nc = A.Ac->localNumberOfRows;
         HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
-        HB_RETURN_IF(mg_fp32_learned(*A.Ac, 1, S, first, o->smoother_coarse_steps, mo->rc32, mo->xc32, s));
-        HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
-        return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
+        const bool separate_prolong = first <= 1 || !fused_prolongation();
+        HB_RETURN_IF(mg_fp32_learned(*A.Ac, 1, S, first, o->smoother_coarse_steps, mo->rc32, mo->xc32, s,
+                                     separate_prolong ? hb::Prolong<float>{} : hb::Prolong<float>{o->z32, mo->pro_f}));
+        if(separate_prolong) HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
+        return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, z64, s);
+    }
+}
+
+}  // namespace hpcg_b200
+
+int ComputeMG_Learned(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    try
+    {
+        ensure_runtime();
+        return mg_learned_to(A, r.d_values, x.d_values, rt().stream);
     }
     catch(const Error& e)
     {

@@ -2,6 +2,8 @@
 // signature and semantics of its rocHPCG counterpart (cited per function)
 // and launches on the runtime stream; scalar-returning ones block for the
 // result exactly like the reference (which syncs after every dot product).
+#include <cstdlib>
+
 #include "hpcg_b200.h"
 #include "internal.hpp"
 
@@ -86,64 +88,121 @@ int ComputeProlongation(const SparseMatrix& Af, Vector& xf)
     });
 }
 
-// src/ComputeMG.cpp:64-102.
-int ComputeMG(const SparseMatrix& A, const Vector& r, Vector& x)
-{
-    if(A.mgData)
-    {
-        int ierr = ComputeSYMGSZeroGuess(A, r, x);
-        if(ierr) return ierr;
-        for(int i = 1; i < A.mgData->numberOfPresmootherSteps; ++i)
-            if((ierr = ComputeSYMGS(A, r, x))) return ierr;
-        if((ierr = ComputeFusedSpMVRestriction(A, r, x))) return ierr;
-        if((ierr = ComputeMG(*A.Ac, *A.mgData->rc, *A.mgData->xc))) return ierr;
-        if((ierr = ComputeProlongation(A, x))) return ierr;
-        for(int i = 0; i < A.mgData->numberOfPostsmootherSteps; ++i)
-            if((ierr = ComputeSYMGS(A, r, x))) return ierr;
-        return 0;
-    }
-    return ComputeSYMGSZeroGuess(A, r, x);
-}
-
 namespace hpcg_b200 {
 
-// FP32 V-cycle on level data, same recursion as ComputeMG.
-int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s)
+bool fused_prolongation()
 {
-    const LevelOpt* o = opt(A);
-    HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s));
-    if(!A.mgData) return 0;
-    const MGOpt* mo = mgopt(A);
-    const int nc = A.Ac->localNumberOfRows;
-    HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
-    HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
-    HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
-    return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s);
+    static const bool on = [] {
+        const char* e = std::getenv("HPCGB200_FUSED_PROLONG");
+        return e && e[0] == '1';
+    }();
+    return on;
 }
 
 }  // namespace hpcg_b200
 
-// FP32 V-cycle preconditioner for FP64 vectors: the level-0 zero-guess sweep
-// reads r in FP64 (storing its float copy), the post-smoother writes z in FP64.
-int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x)
+namespace {
+
+// ComputeMG's recursion with the prolongation fused into the coarse level:
+// `pro` (the finer level's x and the row map) rides on this level's last
+// smoother passes -- the post-smoother's last step, or the zero-guess step of
+// the coarsest level -- instead of a ComputeProlongation launch after it.
+int mg64_ell(const SparseMatrix& A, const Vector& r, Vector& x, hb::Prolong<double> pro)
 {
-    return guarded([&] {
-        const LevelOpt* o = opt(A);
-        for(const SparseMatrix* M = &A; M; M = M->Ac)
-            if(!opt(*M) || !opt(*M)->stencil_ok)
-                return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
-                                        "mixed V-cycle needs the 27-point stencil in parity colouring on every level");
-        cudaStream_t s = rt().stream;
-        const int m = A.localNumberOfRows;
-        HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r.d_values, o->r32, o->z32, s));
-        if(!A.mgData) return hb::launch_cast_f2d(m, o->z32, x.d_values, s);
-        const MGOpt* mo = mgopt(A);
-        const int nc = A.Ac->localNumberOfRows;
-        HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
+    cudaStream_t s = rt().stream;
+    const int m = A.localNumberOfRows;
+    auto zero_guess = [&](hb::Prolong<double> p) {
+        return hb::launch_symgs_zero(m, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind, A.ell_val,
+                                     A.diag_idx, opt(A)->diag, A.inv_diag, r.d_values, x.d_values, s, p);
+    };
+    auto full = [&](hb::Prolong<double> p) {
+        ExchangeHalo(A, x);
+        return hb::launch_symgs(m, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind, A.ell_val, A.inv_diag,
+                                r.d_values, x.d_values, s, p);
+    };
+    if(!A.mgData) return zero_guess(pro);
+    const int pre = A.mgData->numberOfPresmootherSteps, post = A.mgData->numberOfPostsmootherSteps;
+    HB_RETURN_IF(zero_guess(post == 0 ? pro : hb::Prolong<double>{}));
+    for(int i = 1; i < pre; ++i) HB_RETURN_IF(full({}));
+    HB_RETURN_IF(ComputeFusedSpMVRestriction(A, r, x));
+    // src/ComputeMG.cpp:86-90: coarse solve, then ComputeProlongation -- here
+    // carried out by the coarse level's final passes
+    if(fused_prolongation())
+        HB_RETURN_IF(mg64_ell(*A.Ac, *A.mgData->rc, *A.mgData->xc, hb::Prolong<double>{x.d_values, mgopt(A)->pro_f}));
+    else
+    {
+        HB_RETURN_IF(mg64_ell(*A.Ac, *A.mgData->rc, *A.mgData->xc, {}));
+        HB_RETURN_IF(ComputeProlongation(A, x));
+    }
+    for(int i = 0; i < post; ++i) HB_RETURN_IF(full(i == post - 1 ? pro : hb::Prolong<double>{}));
+    return 0;
+}
+
+}  // namespace
+
+// src/ComputeMG.cpp:64-102.
+int ComputeMG(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] { return mg64_ell(A, r, x, {}); });
+}
+
+namespace hpcg_b200 {
+
+// FP32 V-cycle on level data, same recursion as ComputeMG (the prolongation
+// into the finer level fused into this level's final passes).
+int mg_fp32(const SparseMatrix& A, const float* r, float* x, cudaStream_t s, hb::Prolong<float> pro)
+{
+    const LevelOpt* o = opt(A);
+    if(!A.mgData)
+        return hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s, pro);
+    HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, nullptr, const_cast<float*>(r), x, s));
+    const MGOpt* mo = mgopt(A);
+    const int nc = A.Ac->localNumberOfRows;
+    HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, r, x, mo->rc32, s));
+    if(fused_prolongation()) HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s, hb::Prolong<float>{x, mo->pro_f}));
+    else
+    {
+        HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
+        HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, x, s));
+    }
+    return hb::launch32_symgs(o->st, o->inv_diag32, r, x, nullptr, s, pro);
+}
+
+}  // namespace hpcg_b200
+
+namespace hpcg_b200 {
+
+// FP32 V-cycle preconditioner for FP64 vectors: the level-0 zero-guess sweep
+// reads r in FP64 (storing its float copy); the result stays in the level's
+// z32, and its post-smoother also writes the FP64 copy z64 when one is asked
+// for (the CG iteration reads z32 itself).
+int mg_mixed_to(const SparseMatrix& A, const double* r64, double* z64, cudaStream_t s)
+{
+    const LevelOpt* o = opt(A);
+    for(const SparseMatrix* M = &A; M; M = M->Ac)
+        if(!opt(*M) || !opt(*M)->stencil_ok)
+            return hb::record_error(HPCGB200_ERR_NOT_STENCIL,
+                                    "mixed V-cycle needs the 27-point stencil in parity colouring on every level");
+    const int m = A.localNumberOfRows;
+    HB_RETURN_IF(hb::launch32_symgs_zero(o->st, o->diag32, o->inv_diag32, r64, o->r32, o->z32, s));
+    if(!A.mgData) return z64 ? hb::launch_cast_f2d(m, o->z32, z64, s) : 0;
+    const MGOpt* mo = mgopt(A);
+    const int nc = A.Ac->localNumberOfRows;
+    HB_RETURN_IF(hb::launch32_restrict(o->st, nc, mo->inj_f, mo->inj_c, o->diag32, o->r32, o->z32, mo->rc32, s));
+    if(fused_prolongation()) HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s, hb::Prolong<float>{o->z32, mo->pro_f}));
+    else
+    {
         HB_RETURN_IF(mg_fp32(*A.Ac, mo->rc32, mo->xc32, s));
         HB_RETURN_IF(hb::launch32_prolong(o->st, nc, mo->inj_f, mo->inj_c, mo->xc32, o->z32, s));
-        return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, x.d_values, s);
-    });
+    }
+    return hb::launch32_symgs(o->st, o->inv_diag32, o->r32, o->z32, z64, s);
+}
+
+}  // namespace hpcg_b200
+
+int ComputeMG_Mixed(const SparseMatrix& A, const Vector& r, Vector& x)
+{
+    return guarded([&] { return mg_mixed_to(A, r.d_values, x.d_values, rt().stream); });
 }
 
 namespace {
@@ -157,14 +216,16 @@ bool stencil_vec_level(const SparseMatrix& A)
 // ComputeMG's recursion (1 zero-guess pre-smoothing step, fused restriction,
 // coarse solve, prolongation, 1 post-smoothing step) per level on the
 // implicit-stencil kernels or, where the bricks are not 4-aligned, the ELL ones.
-int mg64_stencil(const SparseMatrix& A, const double* r, double* x, cudaStream_t s)
+int mg64_stencil(const SparseMatrix& A, const double* r, double* x, cudaStream_t s, hb::Prolong<double> pro)
 {
     const LevelOpt* o = opt(A);
     const bool vec = stencil_vec_level(A);
-    if(vec) HB_RETURN_IF(hb::launch64v_symgs_zero(o->st, o->diag, A.inv_diag, r, x, s));
+    // the coarsest level's zero-guess step is its last: it carries `pro`
+    const hb::Prolong<double> pz = A.mgData ? hb::Prolong<double>{} : pro;
+    if(vec) HB_RETURN_IF(hb::launch64v_symgs_zero(o->st, o->diag, A.inv_diag, r, x, s, pz));
     else
         HB_RETURN_IF(hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets,
-                                           A.ell_col_ind, A.ell_val, A.diag_idx, o->diag, A.inv_diag, r, x, s));
+                                           A.ell_col_ind, A.ell_val, A.diag_idx, o->diag, A.inv_diag, r, x, s, pz));
     if(!A.mgData) return 0;
     const MGOpt* mo = mgopt(A);
     const int nc = A.Ac->localNumberOfRows;
@@ -174,12 +235,17 @@ int mg64_stencil(const SparseMatrix& A, const double* r, double* x, cudaStream_t
     else
         HB_RETURN_IF(hb::launch_restrict(nc, mo->inj_f, mo->inj_c, A.localNumberOfRows, A.ell_col_ind, A.ell_val, r, x,
                                          rc, s));
-    HB_RETURN_IF(mg64_stencil(*A.Ac, rc, xc, s));
-    if(vec) HB_RETURN_IF(hb::launch64v_prolong(o->st, nc, mo->inj_c, xc, x, s));
-    else HB_RETURN_IF(hb::launch_prolong(nc, mo->inj_f, mo->inj_c, xc, x, s));
-    if(vec) return hb::launch64v_symgs(o->st, A.inv_diag, r, x, s);
+    // coarse solve with the prolongation into x fused into its final passes
+    if(fused_prolongation()) HB_RETURN_IF(mg64_stencil(*A.Ac, rc, xc, s, hb::Prolong<double>{x, mo->pro_f}));
+    else
+    {
+        HB_RETURN_IF(mg64_stencil(*A.Ac, rc, xc, s, {}));
+        if(vec) HB_RETURN_IF(hb::launch64v_prolong(o->st, nc, mo->inj_c, xc, x, s));
+        else HB_RETURN_IF(hb::launch_prolong(nc, mo->inj_f, mo->inj_c, xc, x, s));
+    }
+    if(vec) return hb::launch64v_symgs(o->st, A.inv_diag, r, x, s, pro);
     return hb::launch_symgs(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind, A.ell_val,
-                            A.inv_diag, r, x, s);
+                            A.inv_diag, r, x, s, pro);
 }
 
 }  // namespace
@@ -190,7 +256,7 @@ int ComputeMG_Stencil(const SparseMatrix& A, const Vector& r, Vector& x)
         for(const SparseMatrix* M = &A; M; M = M->Ac)
             if(M->mgData && (M->mgData->numberOfPresmootherSteps != 1 || M->mgData->numberOfPostsmootherSteps != 1))
                 return hb::record_error(HPCGB200_ERR_ARG, "stencil V-cycle: 1 pre- and 1 post-smoothing step only");
-        return mg64_stencil(A, r.d_values, x.d_values, rt().stream);
+        return mg64_stencil(A, r.d_values, x.d_values, rt().stream, {});
     });
 }
 

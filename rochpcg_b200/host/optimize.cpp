@@ -126,6 +126,8 @@ int OptimizeProblem(SparseMatrix& A, CGData& data, Vector& b, Vector& x, Vector&
             mo->inj_c = dalloc<int>(nc);
             check(hpcgb200_transfer_indices(nc, M->mgData->d_f2cOperator, M->perm, M->Ac->perm, mo->inj_f, mo->inj_c,
                                             s));
+            mo->pro_f = dalloc<int>(nc);
+            check(hb::launch_prolong_map(nc, mo->inj_f, mo->inj_c, mo->pro_f, s));
             if(opt(*M)->stencil_ok && opt(*M->Ac)->stencil_ok)
             {
                 mo->rc32 = dalloc<float>(nc);
