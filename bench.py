@@ -71,8 +71,8 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
-    ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "vcycle256", "mixed320",
-                                               "net64"],
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "mixed192", "vcycle256",
+                                               "mixed320", "net64"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--no-largest", action="store_true",
                     help="skip the largest workload (560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs)")
@@ -723,9 +723,9 @@ def learned_comparison(args, R, barrier, steps=2, refcheck=None):
             res[name]["ref_check_tag"] = refcheck(f"learned{n}_{name}", (n, n, n), ("normal", 9999), Q.get_x())
         if mode == R.MODE_LEARNED:
             res[name]["fallback_iteration"] = Q.last_fallback()
-            res[name]["vcycle_ms"] = Q.time_op("mg_learned", 10)
+            res[name]["vcycle_ms_graph"] = Q.time_op("graph:mg_learned", 20)  # as the solver runs it
         elif mode == R.MODE_MIXED:
-            res[name]["vcycle_ms"] = Q.time_op("mg_mixed", 10)
+            res[name]["vcycle_ms_graph"] = Q.time_op("graph:mg_mixed", 20)
     res["speedup_learned_vs_fp64"] = res["fp64"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
     res["speedup_learned_vs_mixed"] = res["mixed"]["time_to_1e-9_s"] / res["learned"]["time_to_1e-9_s"]
     # the literal rule: fall back at the first iteration that does not reduce the FP64 residual norm
@@ -844,9 +844,9 @@ def run_profile_case(case: str) -> int:
         # the FP64 ELL SpMV at 128^3 (2.1M rows, 680 MB of ELL)
         P = R.Problem(128)
         print(json.dumps({"spmv_ms": P.time_op("spmv", 2)}))
-    elif case == "mixed128":
-        # the mixed path's level-0 kernels at 128^3: separable outer SpMV, FP32 colour sweeps
-        P = R.Problem(128)
+    elif case in ("mixed128", "mixed192"):
+        # the mixed path's level-0 kernels: separable outer SpMV, FP32 colour sweeps
+        P = R.Problem(128 if case == "mixed128" else 192)
         print(json.dumps({"spmv_mixed_ms": P.time_op("spmv_mixed", 2), "symgs32_sweep_ms": P.time_op("symgs32_sweep", 1)}))
     elif case == "net64":
         # the learned smoother's evaluation on one 64^3 sample, both odd branches

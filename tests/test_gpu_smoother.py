@@ -3,10 +3,15 @@ whole network against the conv-net oracle, training pairs against the
 coloured-path oracle, training on the device, and the learned V-cycle inside
 flexible CG with its fallback to SymGS.
 
-Gradient tolerance: both sides use the same BF16 rounding points and FP32
-accumulation; they differ by summation order, which can move a value across a
-BF16 rounding boundary or flip a ReLU mask at a near-zero pre-activation, so
-each layer's gradient must agree to 2 % in relative L2 norm (cosine > 0.999).
+Tolerances: both sides use the same BF16 rounding points and FP32
+accumulation and differ only by summation order.  That moves a few values
+across a BF16 rounding boundary (one BF16 ulp, 2^-8 relative, for that
+element) or flips a ReLU mask at a near-zero pre-activation; every other
+element agrees to FP32 rounding.  Measured on B200 over the parametrizations
+below plus a 2 x 32^3 odd case, the worst errors were 3.5e-5 (forward,
+relative L2), 3.6e-4 (forward, max-abs relative to the largest output),
+6.5e-4 (gradient, relative L2, layer 1) and 8e-7 (loss); the bounds are about
+five times those: 2e-4, 2e-3, 3e-3 and 1e-5.
 """
 import ctypes
 
@@ -62,8 +67,8 @@ def test_forward_matches_oracle(dims, nb, odd):
         return 0.5 * (yp - O.net_forward(dims, w1, w2, w3, -v)[0]) if odd else yp
 
     ref = np.concatenate([net(r[b * per:(b + 1) * per]) for b in range(nb)])
-    assert np.linalg.norm(got - ref) <= 1e-2 * np.linalg.norm(ref)
-    assert np.max(np.abs(got - ref)) <= 5e-2 * np.max(np.abs(ref))
+    assert np.linalg.norm(got - ref) <= 2e-4 * np.linalg.norm(ref)
+    assert np.max(np.abs(got - ref)) <= 2e-3 * np.max(np.abs(ref))
 
 
 @pytest.mark.parametrize("dims,nb,odd,kind", [((6, 9, 20), 2, False, 0), ((12, 12, 12), 3, False, 0),
@@ -94,10 +99,10 @@ def test_gradients_match_oracle(dims, nb, odd, kind):
         lb, gb = O.net_loss_grad(dims, w1, w2, w3, r[sl], e[sl], odd=odd, kind=kind)
         ref_loss += scale * lb
         ref += scale * np.concatenate(gb)
-    assert abs(loss - ref_loss) <= 1e-3 * ref_loss
+    assert abs(loss - ref_loss) <= 1e-5 * ref_loss
     for a, b in zip(layers(got), layers(ref)):
-        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b)
-        assert np.dot(a, b) >= 0.999 * np.linalg.norm(a) * np.linalg.norm(b)
+        assert np.linalg.norm(a - b) <= 3e-3 * np.linalg.norm(b)
+        assert np.dot(a, b) >= 0.99999 * np.linalg.norm(a) * np.linalg.norm(b)
     # structural zeros stay zero: layer 1 has one input channel, layer 3 one output channel
     g1 = layers(got)[0].reshape(27, 16, 16)
     g3 = layers(got)[2].reshape(27, 16, 16)
