@@ -71,8 +71,8 @@ def parse():
     ap.add_argument("--lite", action="store_true",
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
-    ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "mixed192", "vcycle256",
-                                               "mixed320", "net64"],
+    ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "mixed192", "cg128",
+                                               "cgmixed192", "vcycle256", "mixed320", "net64"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--no-largest", action="store_true",
                     help="skip the largest workload (560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs)")
@@ -844,6 +844,12 @@ def run_profile_case(case: str) -> int:
         # the FP64 ELL SpMV at 128^3 (2.1M rows, 680 MB of ELL)
         P = R.Problem(128)
         print(json.dumps({"spmv_ms": P.time_op("spmv", 2)}))
+    elif case in ("cg128", "cgmixed192"):
+        # two CG iterations (FP64 ELL at 128^3, or mixed at 192^3); run with HPCGB200_GRAPH=0 so that a
+        # profiler sees the kernels as launches
+        P = R.Problem(128 if case == "cg128" else 192)
+        r = P.cg(2, 0.0, mode=R.MODE_FP64 if case == "cg128" else R.MODE_MIXED)
+        print(json.dumps({"niters": r["niters"], "normr": r["normr"]}))
     elif case in ("mixed128", "mixed192"):
         # the mixed path's level-0 kernels: separable outer SpMV, FP32 colour sweeps
         P = R.Problem(128 if case == "mixed128" else 192)

@@ -101,15 +101,8 @@ __global__ void __launch_bounds__(kBS) k_cg_spmv_pap(int m, ColorChunks cc, cons
     int row;
     if(cc.row_of(blockIdx.x, threadIdx.x, row))
     {
-        double sum = 0.0;
-#pragma unroll
-        for(int q = 0; q < kWidth; ++q)
-        {
-            const size_t idx = (size_t)q * m + row;
-            const int col = ld_stream(ell_col + idx);
-            const double v = ld_stream(ell_val + idx);
-            if(col >= 0 && col < m) sum = fma(v, __ldg(p + col), sum);
-        }
+        // the SpMV row kernel (its grouped loads; the same fma order, so the same Ap)
+        const double sum = spmv_row(m, row, ell_col, ell_val, p);
         Ap[row] = sum;
         s = sum * p[row];
     }
@@ -269,15 +262,7 @@ __global__ void __launch_bounds__(kBS) k_cg_step1_ell(int n, ColorChunks cc, con
     {
         int row;
         if(!cc.row_of(c, threadIdx.x, row)) continue;
-        double sum = 0.0;
-#pragma unroll
-        for(int q = 0; q < kWidth; ++q)
-        {
-            const size_t idx = (size_t)q * n + row;
-            const int col = ld_stream(ell_col + idx);
-            const double v = ld_stream(ell_val + idx);
-            if(col >= 0 && col < n) sum = fma(v, p[col], sum);
-        }
+        const double sum = spmv_row(n, row, ell_col, ell_val, p);
         Ap[row] = sum;
         s = fma(sum, p[row], s);
     }

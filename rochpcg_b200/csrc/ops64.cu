@@ -35,52 +35,6 @@ ColorChunks make_chunks(int m, int ncolors, const int* offsets)
     return cc;
 }
 
-// ------------------------------------------------------------ row kernel core
-
-// sum <- fma(s * a_p, x[col_p], sum) over the ELL slots p of `row` in slot
-// order, for the slots with use_slot(p) and columns with use_col(col).  The
-// slots are processed 9 at a time: the column/value loads of a group are
-// issued together (predicated), then its gathers, then its fmas, so a row
-// costs 2 dependent memory round trips per group instead of 2 per slot.
-template <typename SlotPred, typename ColPred>
-__device__ __forceinline__ double ell_row_sum(int m, int row, const int* __restrict__ ell_col,
-                                              const double* __restrict__ ell_val, const double* x, double sum,
-                                              double s, SlotPred use_slot, ColPred use_col)
-{
-    constexpr int G = 9;
-#pragma unroll
-    for(int g = 0; g < kWidth; g += G)
-    {
-        int col[G];
-        double v[G], xv[G];
-#pragma unroll
-        for(int q = 0; q < G; ++q)
-        {
-            const int p = g + q;
-            const size_t idx = (size_t)p * m + row;
-            const bool u = use_slot(p);
-            col[q] = u ? ld_stream(ell_col + idx) : -1;
-            v[q] = u ? ld_stream(ell_val + idx) : 0.0;
-        }
-#pragma unroll
-        for(int q = 0; q < G; ++q) xv[q] = use_col(col[q]) ? x[col[q]] : 0.0;
-#pragma unroll
-        for(int q = 0; q < G; ++q)
-            if(use_col(col[q])) sum = fma(s * v[q], xv[q], sum);
-    }
-    return sum;
-}
-
-// ---------------------------------------------------------------- SpMV
-
-__device__ __forceinline__ double spmv_row(int m, int row, const int* __restrict__ ell_col,
-                                           const double* __restrict__ ell_val, const double* __restrict__ x)
-{
-    return ell_row_sum(
-        m, row, ell_col, ell_val, x, 0.0, 1.0, [](int) { return true; },
-        [m](int col) { return col >= 0 && col < m; });
-}
-
 // src/ComputeSPMV.cpp:130-170.  Blocks are interleaved over colours (block b
 // works on colour b % ncolors) so the eight blocks that gather from the same
 // neighbourhood of x run together and share it in L2.
@@ -104,9 +58,8 @@ __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset
     const int gid = blockIdx.x * kBS + threadIdx.x;
     if(gid >= size) return;
     const int row = gid + offset;
-    const double sum = ell_row_sum(
-        m, row, ell_col, ell_val, x, r[row], -1.0, [](int) { return true; },
-        [m, row](int col) { return col >= 0 && col < m && col != row; });
+    const double sum = ell_row_sum(m, row, ell_col, ell_val, x, r[row], -1.0, 0, kWidth,
+                                   [m, row](int col) { return col >= 0 && col < m && col != row; });
     const double v = sum * inv_diag[row];
     x[row] = v;
     pro.add(row, v);
@@ -129,9 +82,8 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
     if(offset > 0)
     {
         const int diag = diag_idx[row];
-        sum = ell_row_sum(
-            m, row, ell_col, ell_val, x, sum, -1.0, [diag](int p) { return p < diag; },
-            [offset](int col) { return col >= 0 && col < offset; });
+        sum = ell_row_sum(m, row, ell_col, ell_val, x, sum, -1.0, 0, diag,
+                          [offset](int col) { return col >= 0 && col < offset; });
     }
     const double v = sum * inv_diag[row];
     x[row] = v;
@@ -149,9 +101,8 @@ __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset,
     if(gid >= size) return;
     const int row = gid + offset;
     const int d = diag_idx[row];
-    const double sum = ell_row_sum(
-        m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, [d](int p) { return p > d; },
-        [offset, m](int col) { return col >= offset && col < m; });
+    const double sum = ell_row_sum(m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, d + 1, kWidth,
+                                   [offset, m](int col) { return col >= offset && col < m; });
     const double v = sum * inv_diag[row];
     x[row] = v;
     pro.add(row, v);
@@ -168,9 +119,8 @@ __global__ void __launch_bounds__(kBS) k_restrict(int nc, const int* __restrict_
     const int ic = blockIdx.x * kBS + threadIdx.x;
     if(ic >= nc) return;
     const int row = inj_f[ic];
-    const double sum = ell_row_sum(
-        mf, row, ell_col, ell_val, xf, rf[row], -1.0, [](int) { return true; },
-        [mf](int col) { return col >= 0 && col < mf; });
+    const double sum = ell_row_sum(mf, row, ell_col, ell_val, xf, rf[row], -1.0, 0, kWidth,
+                                   [mf](int col) { return col >= 0 && col < mf; });
     rc[inj_c[ic]] = sum;
 }
 
