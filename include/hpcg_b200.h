@@ -175,6 +175,15 @@ int hpcgb200_dot(int n, const double* x, const double* y, double* result, void* 
  * to rounding, not bit for bit. */
 int hpcgb200_dot_noalloc(long long n, const double* x, const double* y, double* result, void* stream);
 
+/* No reference counterpart: self-test of the bounded grid barrier that the
+ * persistent CG step uses.  The blocks of one cooperative launch (a resident
+ * grid, reported in *blocks) meet at a barrier; with absent_block >= 0 that
+ * block returns without arriving, so the others' waits run out after about a
+ * second and set *status = 1 (*passed counts the blocks that got through).
+ * With absent_block = -1 every block passes and *status stays 0.  Allocates
+ * and synchronizes the device (not for a hot path). */
+int hpcgb200_selftest_grid_barrier(int absent_block, int* status, int* passed, int* blocks);
+
 /* src/ComputeWAXPBY.cpp:63-135 (kernel_waxpby): w = alpha x + beta y with the
  * reference's alpha==1 / beta==1 fma forms. */
 int hpcgb200_waxpby(int n, double alpha, const double* x, double beta, const double* y, double* w, void* stream);

@@ -40,6 +40,7 @@ SIGNATURES = {
     "hpcgb200_prolong": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "hpcgb200_dot": (_i, [_i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hpcgb200_dot_noalloc": (_i, [_ll, _vp, _vp, _vp, _vp]),
+    "hpcgb200_selftest_grid_barrier": (_i, [_i, _vp, _vp, _vp]),
     "hpcgb200_waxpby": (_i, [_i, _d, _vp, _d, _vp, _vp, _vp]),
     "hpcgb200_waxpby_dot": (_i, [_i, _d, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hpcgb200_residual_inf": (_i, [_i, _vp, _vp, _vp, _vp, _sz, _vp]),

@@ -248,6 +248,16 @@ __global__ void k_cg_loop_control(CGState* st, unsigned long long cond, int watc
 // only in the p update, so no SM holds a stale line of it when the product
 // gathers it after the barrier.
 
+// Self-test of the bounded grid barrier: the blocks of a cooperative launch
+// meet at one barrier; block `absent` (if >= 0) returns without arriving, so
+// the others' waits run out (about a second) and set *status.
+__global__ void k_barrier_selftest(GridBarrier* gb, int absent, int* status, int* passed)
+{
+    if((int)blockIdx.x == absent) return;
+    const bool ok = grid_barrier(gb, gridDim.x, status);
+    if(threadIdx.x == 0 && ok) atomicAdd(passed, 1);
+}
+
 // Step 1 with the ELL product (colour-interleaved chunks, one row per thread).
 template <typename Z>
 __global__ void __launch_bounds__(kBS) k_cg_step1_ell(int n, ColorChunks cc, const int* __restrict__ ell_col,
@@ -476,3 +486,35 @@ int launch_cast_f2d(int n, const float* in, double* out, cudaStream_t s)
 }
 
 }  // namespace hb
+
+using namespace hb;
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" int hpcgb200_selftest_grid_barrier(int absent_block, int* status, int* passed, int* blocks)
+{
+    HB_CHECK_ARG(status && passed && blocks, "null argument");
+    const int grid = resident_grid(k_barrier_selftest, 128, 2 * 148);
+    if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "no resident grid");
+    HB_CHECK_ARG(absent_block < grid, "absent_block beyond the grid");
+    struct Scratch
+    {
+        GridBarrier gb;
+        int status, passed;
+    };
+    Scratch* d = nullptr;
+    HB_CUDA(cudaMalloc(&d, sizeof(Scratch)));
+    int rc = 0;
+    cudaError_t e = cudaMemset(d, 0, sizeof(Scratch));
+    if(e == cudaSuccess) e = launch_coop(k_barrier_selftest, grid, 128, nullptr, &d->gb, absent_block, &d->status,
+                                         &d->passed);
+    if(e == cudaSuccess) e = cudaDeviceSynchronize();
+    Scratch h{};
+    if(e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(Scratch), cudaMemcpyDeviceToHost);
+    if(e != cudaSuccess) rc = cuda_error(e, "grid barrier self-test", __FILE__, __LINE__);
+    cudaFree(d);
+    *status = h.status;
+    *passed = h.passed;
+    *blocks = grid;
+    return rc;
+}

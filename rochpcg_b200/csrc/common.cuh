@@ -302,17 +302,25 @@ __device__ __forceinline__ bool grid_reduce(double block_partial, ReduceScratch*
 // Grid-wide barrier of a persistent kernel launched cooperatively (every
 // block resident).  Generation counting: a block reads the generation, then
 // arrives; the last to arrive resets the count and bumps the generation; the
-// others wait for the bump.  The wait is bounded (about a second): on time-out
-// it sets *status and returns false, so a kernel launched without its blocks
-// co-resident ends with an error instead of hanging.  Starts and ends with
-// count == 0.
+// others wait for the bump.  The wait is bounded by time (one second of the
+// global timer, and an iteration cap besides): on time-out it sets *status
+// and returns false, so a kernel whose blocks cannot all arrive ends with an
+// error instead of hanging.  Starts and ends with count == 0.
 struct GridBarrier
 {
     unsigned int count;
     unsigned int gen;
 };
 
-constexpr long long kBarrierSpins = 1ll << 24;  // x 64 ns of back-off
+constexpr unsigned long long kBarrierTimeoutNs = 1000000000ull;
+constexpr long long kBarrierSpins = 1ll << 26;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int nblocks, int* status)
 {
@@ -332,10 +340,11 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int nbloc
         }
         else
         {
+            const unsigned long long t0 = global_ns();
             long long spins = 0;
             while(*gen == g)
             {
-                if(++spins > kBarrierSpins)
+                if(++spins > kBarrierSpins || global_ns() - t0 > kBarrierTimeoutNs)
                 {
                     atomicExch(status, 1);
                     ok = 0;

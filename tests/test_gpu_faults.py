@@ -82,3 +82,26 @@ def test_nan_in_learned_weights_falls_back_and_restarts():
     assert P.true_residual() <= 2e-9
     P.set_smoother(None)
     P.close()
+
+
+def test_grid_barrier_wait_runs_out_and_reports():
+    """The persistent CG step's grid barrier waits at most about a second: when
+    one block never arrives (a flag that nothing sets), the others give up,
+    the status word says so, and the context stays usable (a full barrier then
+    passes).  No GPU fault, trap or hang is involved."""
+    import ctypes
+    import time
+
+    L = R.load()
+    st, passed, blocks = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
+    t0 = time.perf_counter()
+    assert L.hpcgb200_selftest_grid_barrier(0, ctypes.byref(st), ctypes.byref(passed), ctypes.byref(blocks)) == 0
+    elapsed = time.perf_counter() - t0
+    assert blocks.value > 1
+    assert st.value == 1 and passed.value == 0
+    assert elapsed < 10.0
+    assert L.hpcgb200_selftest_grid_barrier(-1, ctypes.byref(st), ctypes.byref(passed), ctypes.byref(blocks)) == 0
+    assert st.value == 0 and passed.value == blocks.value
+    P = R.Problem(16)  # the context is fine
+    assert P.cg(50, 1e-9)["normr"] / P.cg(50, 1e-9)["normr0"] <= 1e-9
+    P.close()
