@@ -42,6 +42,7 @@ extern "C" {
 #define HPCGB200_ERR_DEVICE_STATUS 6  /* a device-side check failed (status word set) */
 #define HPCGB200_ERR_NO_DEVICE 7      /* no CUDA device visible */
 #define HPCGB200_ERR_NONFINITE 8      /* a solve ended with a non-finite residual (outputs are filled) */
+#define HPCGB200_ERR_COMM 9           /* communication between ranks failed or timed out */
 
 #define HPCGB200_WIDTH 27
 #define HPCGB200_MAX_COLORS 128       /* src/utils.hpp:48 */
@@ -517,6 +518,87 @@ int hpcgb200_benchmark_run(const hpcgb200_benchmark_params* params, hpcgb200_ben
  * json[capacity] (NUL-terminated; *length = bytes without the NUL, also when
  * json is NULL or too small, which returns HPCGB200_ERR_WORKSPACE). */
 int hpcgb200_benchmark_report(hpcgb200_benchmark_result* result, char* json, size_t capacity, size_t* length);
+
+/* ------------------------------------------------ domain decomposition
+ * One rank's sub-brick of a problem split over size = npx*npy*npz ranks (one
+ * GPU each), the reference's multi-rank path: src/GenerateGeometry.cpp,
+ * src/SetupHalo.cpp, src/ExchangeHalo.cpp and the halo halves of
+ * src/ComputeSPMV.cpp, src/ComputeSYMGS.cpp, src/ComputeRestriction.cpp,
+ * src/ComputeDotProduct.cpp (FP64 ELL path).  Every rank holds the same local
+ * brick nx*ny*nz; the global grid is (npx*nx) x (npy*ny) x (npz*nz). */
+
+/* src/ComputeOptimalShapeXYZ.cpp:94-157: the process grid for size ranks
+ * (host only). */
+int hpcgb200_dist_shape(int size, int* npx, int* npy, int* npz);
+
+/* src/SetupHalo.cpp:135-651 on the host (no device needed): the halo plan of
+ * `rank` for a local brick nx*ny*nz (npx/npy/npz <= 0: hpcgb200_dist_shape).
+ * hpcgb200_halo_plan_info fills info[16] = {m, externals, neighbours,
+ * send entries, halo rows, halo width, halo entries, npx, npy, npz, ipx,
+ * ipy, ipz, nx, ny, nz}; hpcgb200_halo_plan_copy copies one field to the
+ * host: "nbr_rank", "nbr_slot", "recv_len", "recv_off", "send_len",
+ * "send_off", "send_rows", "halo_rows", "halo_ptr", "halo_cols" (int32) or
+ * "recv_gid" (int64), bytes = its exact size. */
+typedef struct hpcgb200_halo_plan hpcgb200_halo_plan;
+int hpcgb200_halo_plan_create(int nx, int ny, int nz, int size, int rank, int npx, int npy, int npz,
+                              hpcgb200_halo_plan** out);
+int hpcgb200_halo_plan_info(const hpcgb200_halo_plan* plan, int* info);
+int hpcgb200_halo_plan_copy(const hpcgb200_halo_plan* plan, const char* field, void* host, size_t bytes);
+int hpcgb200_halo_plan_destroy(hpcgb200_halo_plan* plan);
+
+/* src/main.cpp:183-210 + src/OptimizeProblem.cpp for one rank: generates and
+ * optimizes the rank's brick on every level (the single-rank colouring,
+ * permutation and ELL of the brick), then adds the external columns after
+ * each row's local ones and lowers the generated b by the row's external
+ * count.  npx/npy/npz <= 0: hpcgb200_dist_shape(size). */
+typedef struct hpcgb200_dist hpcgb200_dist;
+int hpcgb200_dist_create(int nx, int ny, int nz, int nlevels, int size, int rank, int npx, int npy, int npz,
+                         hpcgb200_dist** out);
+int hpcgb200_dist_destroy(hpcgb200_dist* d);
+/* info[20]: the 16 plan values of `level`, then size, rank, levels, colours;
+ * *nnz = nonzeros of the rank's rows on that level, external ones included. */
+int hpcgb200_dist_info(const hpcgb200_dist* d, int level, int* info, long long* nnz);
+/* The plan fields above, or device data: "ell_col", "ell_val", "perm",
+ * "send_perm", "halo_prow", "halo_col", "halo_pc" (any level), "b", "x"
+ * (level 0: b permuted, x permuted with its external tail). */
+int hpcgb200_dist_copy_field(const hpcgb200_dist* d, int level, const char* field, void* host, size_t bytes);
+/* b in the rank's natural row order (NULL: the generated b again); the
+ * rank's part of the solution in natural order. */
+int hpcgb200_dist_set_rhs(hpcgb200_dist* d, const double* host_b_natural);
+int hpcgb200_dist_get_x(hpcgb200_dist* d, double* host_x_natural);
+
+/* NCCL transport (one process per GPU).  1 if libnccl.so.2 can be opened.
+ * Rank 0 makes the communicator id (bytes = 128) and every rank passes it to
+ * hpcgb200_dist_attach_nccl (collective over the ranks).  A solve that makes
+ * no progress for $HPCGB200_DIST_TIMEOUT_S seconds (600) aborts the
+ * communicator and returns HPCGB200_ERR_COMM. */
+int hpcgb200_dist_nccl_available(void);
+int hpcgb200_dist_nccl_id(void* id, size_t bytes);
+int hpcgb200_dist_attach_nccl(hpcgb200_dist* d, const void* id, size_t bytes);
+
+/* Operators and CG over a group of ranks: either every rank of the
+ * decomposition in this process (n == size, one device: the exchange is a
+ * device copy per neighbour), or one rank with a communicator (n == 1).
+ * Vectors are device arrays in each rank's permuted order; x-type vectors
+ * (the ones the halo exchange fills) hold the rank's local rows followed by
+ * its external columns.  Each call returns when its work is complete.
+ *   spmv     y = A x                 (src/ComputeSPMV.cpp:226-278)
+ *   symgs    one symmetric sweep     (src/ComputeSYMGS.cpp:369-404)
+ *   restrict rc = R(rf - A xf)       (src/ComputeRestriction.cpp:199-237; level < levels-1)
+ *   mg       x = M r, the V-cycle    (src/ComputeMG.cpp:64-102)
+ *   cg       the preconditioned CG on the ranks' generated (or set) b from
+ *            x = 0 (src/CG.cpp:104-200); normr_hist (max_iter+1) may be NULL;
+ *            *seconds = device time of the solve on the group's stream. */
+int hpcgb200_dist_group_spmv(hpcgb200_dist* const* ranks, int n, int level, double* const* x, double* const* y);
+int hpcgb200_dist_group_symgs(hpcgb200_dist* const* ranks, int n, int level, double* const* r, double* const* x);
+int hpcgb200_dist_group_restrict(hpcgb200_dist* const* ranks, int n, int level, double* const* rf,
+                                 double* const* xf, double* const* rc);
+int hpcgb200_dist_group_mg(hpcgb200_dist* const* ranks, int n, double* const* r, double* const* x);
+int hpcgb200_dist_group_cg(hpcgb200_dist* const* ranks, int n, int max_iter, double tol, int precond, int* niters,
+                           double* normr, double* normr0, double* normr_hist, double* seconds);
+/* hpcgb200_dist_group_cg with the one rank d (a communicator attached, or size 1). */
+int hpcgb200_dist_cg(hpcgb200_dist* d, int max_iter, double tol, int precond, int* niters, double* normr,
+                     double* normr0, double* normr_hist, double* seconds);
 
 #ifdef __cplusplus
 }

@@ -95,8 +95,34 @@ def ref_lib(rows: bool = False):
                                      ctypes.c_void_p, ctypes.c_void_p]
         L.hpcgref_residual.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _c_dbl_p]
         L.hpcgref_test_norms.argtypes = [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_int_p]
+        L.hpcgref_optimal_shape.argtypes = [ctypes.c_int, _c_int_p, _c_int_p, _c_int_p]
+        L.hpcgref_optimal_shape.restype = None
+        L.hpcgref_rank_problem.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p] * 5
         _ref_libs[so] = L
     return _ref_libs[so]
+
+
+def ref_optimal_shape(size: int) -> tuple[int, int, int]:
+    """The reference's own process grid (src/ComputeOptimalShapeXYZ.cpp)."""
+    L = ref_lib()
+    x, y, z = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    L.hpcgref_optimal_shape(size, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z))
+    return x.value, y.value, z.value
+
+
+def ref_rank_problem(size: int, rank: int, nx: int, ny: int, nz: int) -> dict:
+    """Rank `rank` of a `size`-rank run as the reference generates it
+    (src/GenerateGeometry.cpp + src/GenerateProblem_ref.cpp): per natural row
+    the GLOBAL column ids (-1 padded), values, nonzero count and b."""
+    L = ref_lib()
+    m = nx * ny * nz
+    gcols = np.empty((m, 27), np.int64)
+    vals = np.empty((m, 27), np.float64)
+    nnz = np.empty(m, np.int8)
+    b = np.empty(m, np.float64)
+    grid = np.zeros(6, np.int32)
+    assert L.hpcgref_rank_problem(size, rank, nx, ny, nz, _ptr(gcols), _ptr(vals), _ptr(nnz), _ptr(b), _ptr(grid)) == 0
+    return {"gcols": gcols, "vals": vals, "nnz": nnz, "b": b, "grid": tuple(int(v) for v in grid)}
 
 
 class RefProblem:
@@ -393,6 +419,141 @@ class ColoredProblem:
 
 # --------------------------------------------------------------------------
 # learned smoother (conv net) restatement
+
+
+def _dist_lib():
+    L = colored_lib()
+    if not getattr(L, "_od_ready", False):
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.od_shape.argtypes = [ci, _c_int_p, _c_int_p, _c_int_p]
+        L.od_create.argtypes = [ci] * 8
+        L.od_create.restype = vp
+        L.od_destroy.argtypes = [vp]
+        L.od_level_info.argtypes = [vp, ci, ci, vp]
+        for name in ("od_level_perm", "od_level_ext_gid"):
+            getattr(L, name).argtypes = [vp, ci, ci, vp]
+        L.od_level_ell.argtypes = [vp, ci, ci, vp, vp]
+        L.od_level_b.argtypes = [vp, ci, vp]
+        L.od_exchange.argtypes = [vp, ci, vp]
+        for name in ("od_spmv", "od_symgs", "od_symgs_zero"):
+            getattr(L, name).argtypes = [vp, ci, vp, vp]
+        L.od_restrict.argtypes = [vp, ci, vp, vp, vp]
+        L.od_mg.argtypes = [vp, vp, vp]
+        L.od_cg.argtypes = [vp, ci, ctypes.c_double, ci, vp, vp, _c_int_p, _c_dbl_p, _c_dbl_p, vp]
+        for name in ("od_shape", "od_destroy", "od_level_info", "od_level_perm", "od_level_ext_gid", "od_level_ell",
+                     "od_level_b", "od_exchange", "od_spmv", "od_symgs", "od_symgs_zero", "od_restrict", "od_mg",
+                     "od_cg"):
+            getattr(L, name).restype = None
+        L._od_ready = True
+    return L
+
+
+def od_shape(size: int) -> tuple[int, int, int]:
+    L = _dist_lib()
+    x, y, z = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    L.od_shape(size, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z))
+    return x.value, y.value, z.value
+
+
+def _vec_ptrs(vs):
+    return (ctypes.c_void_p * len(vs))(*[v.ctypes.data for v in vs])
+
+
+class DistOracle:
+    """Every rank of a decomposed problem (oracle/distributed.c): per-rank
+    level data and the operators over all ranks, vectors as lists of numpy
+    arrays in each rank's permuted order (x-type ones with the external tail)."""
+
+    def __init__(self, size: int, nx: int, ny: int, nz: int, nlevels: int = 4, grid=None):
+        self.L = _dist_lib()
+        npx, npy, npz = grid if grid else (0, 0, 0)
+        self.h = self.L.od_create(size, npx, npy, npz, nx, ny, nz, nlevels)
+        if not self.h:
+            raise ValueError("od_create: process grid does not match size")
+        self.size, self.nlevels = size, nlevels
+        self.info = []
+        for r in range(size):
+            per = []
+            for l in range(nlevels):
+                v = np.zeros(8, np.int32)
+                self.L.od_level_info(self.h, r, l, _ptr(v))
+                per.append(dict(zip(("m", "next", "nblocks", "ublocks", "nhalo", "nx", "ny", "nz"),
+                                    (int(a) for a in v))))
+                per[-1]["ncols"] = per[-1]["m"] + per[-1]["next"]
+            self.info.append(per)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.od_destroy(self.h)
+            self.h = None
+
+    def perm(self, rank: int, level: int = 0) -> np.ndarray:
+        out = np.empty(self.info[rank][level]["m"], np.int32)
+        self.L.od_level_perm(self.h, rank, level, _ptr(out))
+        return out
+
+    def ell(self, rank: int, level: int = 0):
+        m = self.info[rank][level]["m"]
+        col = np.empty((27, m), np.int32)
+        val = np.empty((27, m), np.float64)
+        self.L.od_level_ell(self.h, rank, level, _ptr(col), _ptr(val))
+        return col, val
+
+    def ext_gid(self, rank: int, level: int = 0) -> np.ndarray:
+        out = np.empty(self.info[rank][level]["next"], np.int64)
+        self.L.od_level_ext_gid(self.h, rank, level, _ptr(out))
+        return out
+
+    def b(self, rank: int) -> np.ndarray:
+        out = np.empty(self.info[rank][0]["m"], np.float64)
+        self.L.od_level_b(self.h, rank, _ptr(out))
+        return out
+
+    def _xs(self, level, xs):
+        out = []
+        for r, x in enumerate(xs):
+            v = np.zeros(self.info[r][level]["ncols"])
+            v[:len(x)] = x
+            out.append(v)
+        return out
+
+    def spmv(self, level: int, xs):
+        xs = self._xs(level, xs)
+        ys = [np.empty(self.info[r][level]["m"]) for r in range(self.size)]
+        self.L.od_spmv(self.h, level, _vec_ptrs(xs), _vec_ptrs(ys))
+        return ys
+
+    def symgs(self, level: int, rs, xs):
+        rs = [np.ascontiguousarray(r, np.float64) for r in rs]
+        xs = self._xs(level, xs)
+        self.L.od_symgs(self.h, level, _vec_ptrs(rs), _vec_ptrs(xs))
+        return [x[:self.info[r][level]["m"]] for r, x in enumerate(xs)]
+
+    def restrict(self, level: int, rfs, xfs):
+        rfs = [np.ascontiguousarray(r, np.float64) for r in rfs]
+        xfs = self._xs(level, xfs)
+        rcs = [np.empty(self.info[r][level + 1]["m"]) for r in range(self.size)]
+        self.L.od_restrict(self.h, level, _vec_ptrs(rfs), _vec_ptrs(xfs), _vec_ptrs(rcs))
+        return rcs
+
+    def mg(self, rs):
+        rs = [np.ascontiguousarray(r, np.float64) for r in rs]
+        xs = [np.zeros(self.info[r][0]["ncols"]) for r in range(self.size)]
+        self.L.od_mg(self.h, _vec_ptrs(rs), _vec_ptrs(xs))
+        return [x[:self.info[r][0]["m"]] for r, x in enumerate(xs)]
+
+    def cg(self, max_iter: int, tol: float, precond: bool = True, bs=None) -> dict:
+        xs = [np.zeros(self.info[r][0]["m"]) for r in range(self.size)]
+        hist = np.zeros(max_iter + 1)
+        it = ctypes.c_int()
+        nr, nr0 = ctypes.c_double(), ctypes.c_double()
+        bptr = None
+        if bs is not None:
+            bs = [np.ascontiguousarray(b, np.float64) for b in bs]
+            bptr = _vec_ptrs(bs)
+        self.L.od_cg(self.h, max_iter, tol, 1 if precond else 0, bptr, _vec_ptrs(xs), ctypes.byref(it),
+                     ctypes.byref(nr), ctypes.byref(nr0), _ptr(hist))
+        return {"niters": it.value, "normr": nr.value, "normr0": nr0.value, "hist": hist[:it.value + 1], "x": xs}
 
 
 def bf16(a: np.ndarray) -> np.ndarray:

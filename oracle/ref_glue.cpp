@@ -40,6 +40,7 @@
 #include "ComputeRestriction_ref.hpp"
 #include "ComputeProlongation_ref.hpp"
 #include "TestNorms.hpp"
+#include "ComputeOptimalShapeXYZ.hpp"
 
 // Globals the reference headers declare (src/utils.hpp:38-45, src/hpcg.hpp).
 std::ofstream HPCG_fout;
@@ -306,6 +307,47 @@ int hpcgref_test_norms(const double* values, int n, double* mean, double* varian
     *mean = d.mean;
     *variance = d.variance;
     *pass = d.pass ? 1 : 0;
+    return 0;
+}
+
+// The reference's own process grid for `size` ranks (src/ComputeOptimalShapeXYZ.cpp).
+void hpcgref_optimal_shape(int size, int* npx, int* npy, int* npz)
+{
+    int x = 0, y = 0, z = 0;
+    ComputeOptimalShapeXYZ(size, x, y, z);
+    *npx = x, *npy = y, *npz = z;
+}
+
+// Rank `rank` of a `size`-rank run with local brick nx*ny*nz, as the
+// reference generates it (src/GenerateGeometry.cpp + src/GenerateProblem_ref.cpp
+// with the geometry's global offsets): per natural row its GLOBAL column ids
+// (row-major 27 slots, -1 padded), values, nonzero count and b; grid[6] =
+// {npx, npy, npz, ipx, ipy, ipz}.  The MPI sum of the nonzero count is not
+// needed for these arrays.  (The generated problem is not released: a test
+// oracle's process memory.)
+int hpcgref_rank_problem(int size, int rank, int nx, int ny, int nz, long long* gcols, double* vals,
+                         signed char* nnz_in_row, double* b, int* grid)
+{
+    Geometry* geom = new Geometry;
+    GenerateGeometry(size, rank, 1, 0, 0, 0, nx, ny, nz, 0, 0, 0, geom);
+    SparseMatrix A;
+    InitializeSparseMatrix(A, geom);
+    Vector vb, vx, vxe;
+    GenerateProblem_ref(A, &vb, &vx, &vxe);
+    const local_int_t m = A.localNumberOfRows;
+    for(local_int_t i = 0; i < m; ++i)
+    {
+        const int nnz = A.nonzerosInRow[i];
+        nnz_in_row[i] = (signed char)nnz;
+        for(int j = 0; j < 27; ++j)
+        {
+            gcols[(size_t)i * 27 + j] = j < nnz ? (long long)A.mtxIndG[i][j] : -1;
+            vals[(size_t)i * 27 + j] = j < nnz ? A.matrixValues[i][j] : 0.0;
+        }
+        b[i] = vb.values[i];
+    }
+    grid[0] = geom->npx, grid[1] = geom->npy, grid[2] = geom->npz;
+    grid[3] = geom->ipx, grid[4] = geom->ipy, grid[5] = geom->ipz;
     return 0;
 }
 

@@ -99,6 +99,27 @@ SIGNATURES = {
     "hpcgb200_problem_restrict": (_i, [_vp, _i, _vp, _vp, _vp]),
     "hpcgb200_problem_prolong": (_i, [_vp, _i, _vp, _vp]),
     "hpcgb200_problem_time_op": (_i, [_vp, _cp, _i, _vp]),
+    # domain decomposition
+    "hpcgb200_dist_shape": (_i, [_i, _vp, _vp, _vp]),
+    "hpcgb200_halo_plan_create": (_i, [_i, _i, _i, _i, _i, _i, _i, _i, _vp]),
+    "hpcgb200_halo_plan_info": (_i, [_vp, _vp]),
+    "hpcgb200_halo_plan_copy": (_i, [_vp, _cp, _vp, _sz]),
+    "hpcgb200_halo_plan_destroy": (_i, [_vp]),
+    "hpcgb200_dist_create": (_i, [_i, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
+    "hpcgb200_dist_destroy": (_i, [_vp]),
+    "hpcgb200_dist_info": (_i, [_vp, _i, _vp, _vp]),
+    "hpcgb200_dist_copy_field": (_i, [_vp, _i, _cp, _vp, _sz]),
+    "hpcgb200_dist_set_rhs": (_i, [_vp, _vp]),
+    "hpcgb200_dist_get_x": (_i, [_vp, _vp]),
+    "hpcgb200_dist_nccl_available": (_i, []),
+    "hpcgb200_dist_nccl_id": (_i, [_vp, _sz]),
+    "hpcgb200_dist_attach_nccl": (_i, [_vp, _vp, _sz]),
+    "hpcgb200_dist_group_spmv": (_i, [_vp, _i, _i, _vp, _vp]),
+    "hpcgb200_dist_group_symgs": (_i, [_vp, _i, _i, _vp, _vp]),
+    "hpcgb200_dist_group_restrict": (_i, [_vp, _i, _i, _vp, _vp, _vp]),
+    "hpcgb200_dist_group_mg": (_i, [_vp, _i, _vp, _vp]),
+    "hpcgb200_dist_group_cg": (_i, [_vp, _i, _i, _d, _i, _vp, _vp, _vp, _vp, _vp]),
+    "hpcgb200_dist_cg": (_i, [_vp, _i, _d, _i, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -19,8 +19,25 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libhpcgb200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nccl_include() -> list[str]:
+    """nccl.h for the decomposed solver's types (the library itself is
+    opened at run time): the NCCL wheel's headers, else the system ones."""
+    try:
+        import nvidia.nccl as nc
+
+        for d in nc.__path__:
+            inc = os.path.join(d, "include")
+            if os.path.isfile(os.path.join(inc, "nccl.h")):
+                return ["-I" + inc]
+    except ImportError:
+        pass
+    return []
+
+
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3",
-              "-I" + os.path.join(ROOT, "include")] + ARCH
+              "-I" + os.path.join(ROOT, "include")] + _nccl_include() + ARCH
 
 
 def nvcc() -> str:
@@ -74,7 +91,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     objs = [_obj(s) for s in srcs]
     if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         tmp = LIB + ".tmp"
-        cmd = [cc] + ARCH + ["-shared", "-o", tmp] + objs + ["-Xlinker", "--no-undefined"]
+        cmd = [cc] + ARCH + ["-shared", "-o", tmp] + objs + ["-ldl", "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

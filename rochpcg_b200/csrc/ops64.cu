@@ -50,7 +50,11 @@ __global__ void __launch_bounds__(kBS) k_spmv(int m, ColorChunks cc, const int* 
 // ---------------------------------------------------------------- SymGS
 
 // src/ComputeSYMGS.cpp:113-151 (kernel_symgs_sweep): rows of one colour.
-__global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset, const int* __restrict__ ell_col,
+// Columns below ncols take part: the local columns (ncols = m; also
+// kernel_symgs_interior, :153-188), or the local and the external ones of a
+// rank of a decomposed problem (ncols = m + externals).
+__global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int ncols, int size, int offset,
+                                                     const int* __restrict__ ell_col,
                                                      const double* __restrict__ ell_val,
                                                      const double* __restrict__ inv_diag,
                                                      const double* __restrict__ r, double* x, Prolong<double> pro)
@@ -59,7 +63,7 @@ __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int size, int offset
     if(gid >= size) return;
     const int row = gid + offset;
     const double sum = ell_row_sum(m, row, ell_col, ell_val, x, r[row], -1.0, 0, kWidth,
-                                   [m, row](int col) { return col >= 0 && col < m && col != row; });
+                                   [ncols, row](int col) { return col >= 0 && col < ncols && col != row; });
     const double v = sum * inv_diag[row];
     x[row] = v;
     pro.add(row, v);
@@ -224,17 +228,28 @@ int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* o
     for(int i = 0; i < nblocks; ++i)
     {
         if(sizes[i] <= 0) continue;
-        k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, inv_diag,
-                                                                 r, x, i > ublocks ? pro : Prolong<double>{});
+        k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, m, sizes[i], offsets[i], ell_col, ell_val,
+                                                                 inv_diag, r, x,
+                                                                 i > ublocks ? pro : Prolong<double>{});
         HB_LAUNCHED();
     }
     for(int i = ublocks; i >= 0; --i)
     {
         if(sizes[i] <= 0) continue;
-        k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, inv_diag,
-                                                                 r, x, pro);
+        k_symgs_sweep<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, m, sizes[i], offsets[i], ell_col, ell_val,
+                                                                 inv_diag, r, x, pro);
         HB_LAUNCHED();
     }
+    return 0;
+}
+
+int launch_sweep_color(int m, int ncols, int size, int offset, const int* ell_col, const double* ell_val,
+                       const double* inv_diag, const double* r, double* x, cudaStream_t s)
+{
+    if(size <= 0) return 0;
+    k_symgs_sweep<<<(size + kBS - 1) / kBS, kBS, 0, s>>>(m, ncols, size, offset, ell_col, ell_val, inv_diag, r, x,
+                                                         Prolong<double>{});
+    HB_LAUNCHED();
     return 0;
 }
 

@@ -85,6 +85,10 @@ int launch_spmv(int m, const ColorChunks& cc, const int* ell_col, const double* 
 int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                  const double* ell_val, const double* inv_diag, const double* r, double* x, cudaStream_t s,
                  Prolong<double> pro = {});
+// One colour of kernel_symgs_sweep with the columns below ncols (the
+// decomposed problem's sweeps; launch_symgs uses ncols = m).
+int launch_sweep_color(int m, int ncols, int size, int offset, const int* ell_col, const double* ell_val,
+                       const double* inv_diag, const double* r, double* x, cudaStream_t s);
 int launch_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                       const double* ell_val, const int* diag_idx, const double* diag, const double* inv_diag,
                       const double* r, double* x, cudaStream_t s, Prolong<double> pro = {});
