@@ -80,6 +80,11 @@ def parse():
                     help="skip the host check of each solve's x with the reference's ComputeSPMV_ref")
     ap.add_argument("--learned-nx", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: independent replicas of the 1-GPU run instead of the decomposed solve")
+    ap.add_argument("--emulate-ranks", type=int, default=0,
+                    help="1 GPU: drive R ranks of the decomposed solve from this process (exchange by device "
+                         "copies) to exercise the decomposed path; not a multi-GPU measurement")
     return ap.parse_args()
 
 
@@ -879,12 +884,131 @@ def run_profile_case(case: str) -> int:
     return 0
 
 
+# ------------------------------------------------------------ decomposed solve
+
+def dist_launches_per_iter(P) -> int:
+    """Our kernels per CG iteration of one rank of the decomposed solve (NCCL's
+    own kernels not counted): per MG level the zero-guess colours, pack +
+    interior + halo of the restriction, the prolongation, pack + colour 0 +
+    halo + the other sweeps; CG: 2 dots, p update, pack + SpMV + halo, x/r update."""
+    n = 0
+    L = P.levels
+    for l, lv in enumerate(L):
+        nb = lv["nblocks"]
+        n += 2 * nb - 1
+        if l + 1 < len(L):
+            n += 3 + 1 + (3 + (nb - 1) + (nb - 1))
+    return n + 2 + 1 + 3 + 1
+
+
+def dist_model(nx: int, grid, nlevels: int = 4):
+    """HPCG flop model of the GLOBAL problem (src/ReportResults.cpp:134-195 with
+    the global row and nonzero counts)."""
+    from rochpcg_b200 import hpcg_model
+
+    dims = [(grid[0] * (nx >> l), grid[1] * (nx >> l), grid[2] * (nx >> l)) for l in range(nlevels)]
+    return hpcg_model(dims, [stencil_nnz(d) for d in dims]), dims
+
+
+def run_dist(args, world: int, rank: int, local: int, emulate: int = 0):
+    """The decomposed FP64 MG-PCG: every rank one nx^3 brick of the global grid
+    (HPCG's weak scaling), halos over NCCL (or, emulated, device copies)."""
+    import torch
+    from rochpcg_b200 import dist as D
+
+    os.environ.setdefault("HPCGB200_DIST_TIMEOUT_S", "180")
+    nranks = emulate or world
+    pg = init_dist(world, local, "nccl") if not emulate else None
+    if pg is None:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    nx = args.nx
+    grid = D.shape(nranks)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    if emulate:
+        ranks = [D.DistProblem(nx, nx, nx, nranks, r) for r in range(nranks)]
+        solve = lambda: D.group_cg(ranks, args.max_iter, args.tol)  # noqa: E731
+        mine = ranks[0]
+    else:
+        mine = D.DistProblem(nx, nx, nx, world, rank)
+        barrier()
+        D.attach_nccl(mine, pg)
+        ranks = [mine]
+        solve = lambda: mine.cg(args.max_iter, args.tol)  # noqa: E731
+    (flops_it, _), gdims = dist_model(nx, grid)
+    for _ in range(args.warmup):
+        solve()
+    barrier()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    runs = [solve() for _ in range(args.steps)]
+    barrier()
+    clocks = sampler.stop()
+    sec = max_over(pg, sum(r["seconds"] for r in runs) / args.steps, "cuda")
+    iters = runs[-1]["niters"]
+    value = flops_it * iters / sec / 1e9
+    rel = runs[-1]["normr"] / runs[-1]["normr0"]
+    xerr = max(float(np.max(np.abs(P.get_x() - 1.0))) for P in ranks)
+    xerr = max_over(pg, xerr, "cuda")
+    # end to end through the rank API: b from host memory, x back to host memory
+    m = mine.levels[0]["m"]
+    nat_b = [P.field("b")[P.field("perm")] for P in ranks]
+    x_host = np.empty(m)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for P, b in zip(ranks, nat_b):
+            P.set_rhs(b)
+        re = solve()
+        for P in ranks:
+            x_host = P.get_x()
+    barrier()
+    e2e_s = max_over(pg, (time.perf_counter() - t0) / args.steps, "cuda")
+    launches = args.steps * nranks * (iters * dist_launches_per_iter(mine) + 6)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (HPCG problem generator, b for x*=1)",
+            "config": {"workload": f"HPCG domain decomposition, {nranks} ranks of {nx}^3 (global "
+                                   f"{gdims[0][0]}x{gdims[0][1]}x{gdims[0][2]}), FP64 MG-PCG to {args.tol:g}",
+                       "grid": list(gdims[0]), "local_grid": [nx, nx, nx], "process_grid": list(grid),
+                       "mg_levels": 4, "rhs": "generated (exact solution ones), x0=0",
+                       "l2": "inputs larger than L2 (level-0 ELL of one rank is %.1f GB)" % (27 * 12 * m / 1e9),
+                       "parallelism": (f"emulated {nranks} ranks on 1 GPU (device-copy exchange)" if emulate else
+                                       f"domain decomposition {grid[0]}x{grid[1]}x{grid[2]}, halo exchange and "
+                                       f"dot allreduce over NCCL")},
+            "decomposed": True, "emulated": bool(emulate),
+            "time_to_solution_s": sec, "iterations": iters, "rel_residual": rel, "max_abs_x_minus_1": xerr,
+            "e2e": {"value": flops_it * re["niters"] / e2e_s / 1e9, "unit": "GFLOP/s",
+                    "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * m, "seconds_per_step": e2e_s},
+            "roofline": None, "roofline_note": "per-kernel roofline is reported by the 1-GPU run",
+            "cpu_baseline": None, "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line))
+    for P in ranks:
+        P.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_case:
         return run_profile_case(args.profile_case)
     if args.impl == "reference":
         return run_reference(args)
+    world, rank, local = ranks()
+    if args.emulate_ranks > 1 and world == 1:
+        return run_dist(args, 1, 0, 0, emulate=args.emulate_ranks)
+    if world > 1 and not args.replicas:
+        return run_dist(args, world, rank, local)
     return run_ours(args)
 
 

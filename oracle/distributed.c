@@ -180,8 +180,13 @@ static int build_level(od_level* A, int rank, int npx, int npy, int npz, int nx,
         free(colors), free(cols), free(vals), free(nnz), free(dslot), free(hash);
         return -1;
     }
-    A->nblocks = nb;
-    A->ublocks = nb - 2; /* MultiColoring.cpp:316,350-352 */
+    /* Sweeps over the colour VALUES 0..maxc (the by-value blocks; the
+     * reference's nblocks counts JPL rounds, which on bricks that need fewer
+     * than 8 colours can be below the largest value drawn -- its round-order
+     * sizes[] then straddle colours); ublocks one below the last, as
+     * MultiColoring.cpp:316,350-352. */
+    A->nblocks = maxc + 1;
+    A->ublocks = maxc - 1;
     A->ncolors = nb > maxc + 1 ? nb : maxc + 1;
     A->sizes = calloc((size_t)A->ncolors, sizeof(int));
     A->offsets = calloc((size_t)A->ncolors + 1, sizeof(int));

@@ -181,8 +181,10 @@ Group make_group(hpcgb200_dist* const* ranks, int n)
     G.nlevels = (int)G.R[0]->L.size();
     if(n == 1)
     {
-        G.use_nccl = size > 1;
-        if(G.use_nccl && !G.R[0]->comm)
+        // a rank with a communicator always goes through NCCL (for one rank:
+        // no exchange, a one-rank allreduce)
+        G.use_nccl = G.R[0]->comm != nullptr;
+        if(size > 1 && !G.use_nccl)
             throw Error(HPCGB200_ERR_ARG, "a rank of a decomposed problem solves alone only with a communicator "
                                           "(hpcgb200_dist_attach_nccl), or drive all ranks as one group");
         return G;
