@@ -24,6 +24,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -106,6 +107,14 @@ void check_nccl(ncclResult_t r, const char* what)
     throw Error(HPCGB200_ERR_COMM, buf);
 }
 
+// Steady CG iterations as one CUDA graph launch each (HPCGB200_DIST_GRAPH=0:
+// direct launches).
+bool dist_graphs()
+{
+    const char* e = std::getenv("HPCGB200_DIST_GRAPH");
+    return !e || std::atoi(e) != 0;
+}
+
 double dist_timeout_s()
 {
     const char* e = std::getenv("HPCGB200_DIST_TIMEOUT_S");
@@ -154,6 +163,12 @@ struct hpcgb200_dist
     ncclComm_t comm = nullptr;
     cudaStream_t comm_stream = nullptr;
     cudaEvent_t ev_packed = nullptr, ev_recv = nullptr, ev_sync = nullptr;
+    unsigned long long serial = 0;                    // process-unique id (graph cache keys)
+    // cached CUDA graph of one steady CG iteration of a group whose first rank
+    // is this one: the group's serials and the preconditioner flag as its key
+    std::vector<unsigned long long> graph_key;
+    bool graph_precond = false;
+    cudaGraphExec_t graph_exec = nullptr;
 };
 
 namespace hpcg_b200 {
@@ -436,6 +451,43 @@ std::vector<double*> vecs(Group& G, F&& f)
     return v;
 }
 
+// The cached graph of the group's steady iteration (captured by `body` on
+// first use; the cache sits in the group's first rank, keyed on the ranks'
+// serial numbers, which are never reused).
+template <typename F>
+cudaGraphExec_t steady_graph(Group& G, bool precond, F&& body)
+{
+    hpcgb200_dist* d0 = G.R[0];
+    std::vector<unsigned long long> key;
+    for(auto* d : G.R) key.push_back(d->serial);
+    if(d0->graph_exec && d0->graph_key == key && d0->graph_precond == precond) return d0->graph_exec;
+    if(d0->graph_exec)
+    {
+        HB_HOST_CUDA(cudaStreamSynchronize(G.s));
+        cudaGraphExecDestroy(d0->graph_exec);
+        d0->graph_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    HB_HOST_CUDA(cudaStreamBeginCapture(G.s, cudaStreamCaptureModeThreadLocal));
+    try
+    {
+        body();
+    }
+    catch(...)
+    {
+        cudaStreamEndCapture(G.s, &g);
+        if(g) cudaGraphDestroy(g);
+        throw;
+    }
+    HB_HOST_CUDA(cudaStreamEndCapture(G.s, &g));
+    const cudaError_t e = cudaGraphInstantiate(&d0->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(e, "cudaGraphInstantiate (decomposed CG iteration)");
+    d0->graph_key = key;
+    d0->graph_precond = precond;
+    return d0->graph_exec;
+}
+
 // src/CG.cpp:104-200 over the group; every rank computes the same scalars.
 void cg(Group& G, int max_iter, double tol, bool precond, int& niters, double& normr, double& normr0, double* hist,
         double* seconds)
@@ -461,9 +513,9 @@ void cg(Group& G, int max_iter, double tol, bool precond, int& niters, double& n
     normr = std::sqrt(read_slot(G, hb::kDistRr));
     normr0 = normr;
     if(hist) hist[0] = normr;
-    niters = 0;
-    for(int k = 1; k <= max_iter && normr / normr0 > tol; ++k)
-    {
+    // one iteration's work (src/CG.cpp:143-176), ending with r.r summed over
+    // the ranks and copied to the first rank's pinned mirror
+    auto iteration = [&](bool first) {
         if(precond) mg(G, 0, rs, zs);
         else
             each(G, [&](hpcgb200_dist* d, int) {
@@ -475,7 +527,7 @@ void cg(Group& G, int max_iter, double tol, bool precond, int& niters, double& n
         });
         allreduce(G, hb::kDistRtzNew);
         each(G, [&](hpcgb200_dist* d, int) {
-            return hb::launch_dist_update_p(d->L[0].m, k == 1, d->z, d->p, d->sc, G.s);
+            return hb::launch_dist_update_p(d->L[0].m, first ? 1 : 0, d->z, d->p, d->sc, G.s);
         });
         spmv(G, 0, ps, Aps);
         each(G, [&](hpcgb200_dist* d, int) {
@@ -486,7 +538,20 @@ void cg(Group& G, int max_iter, double tol, bool precond, int& niters, double& n
             return hb::launch_dist_update_xr(d->L[0].m, d->p, d->Ap, d->x, d->r, d->sc, rt().ws, G.s);
         });
         allreduce(G, hb::kDistRr);
-        normr = std::sqrt(read_slot(G, hb::kDistRr));
+        hpcgb200_dist* d0 = G.R[0];
+        HB_HOST_CUDA(cudaMemcpyAsync(d0->h_sc + hb::kDistRr, d0->sc + hb::kDistRr, sizeof(double),
+                                     cudaMemcpyDeviceToHost, G.s));
+    };
+    niters = 0;
+    for(int k = 1; k <= max_iter && normr / normr0 > tol; ++k)
+    {
+        // the first iteration runs launch by launch: it differs (p = z) and it
+        // makes every exchange once, so that all peer connections exist before
+        // the steady iteration is captured
+        if(k == 1 || !dist_graphs()) iteration(k == 1);
+        else HB_HOST_CUDA(cudaGraphLaunch(steady_graph(G, precond, [&] { iteration(false); }), G.s));
+        wait_stream(G);
+        normr = std::sqrt(G.R[0]->h_sc[hb::kDistRr]);
         if(hist) hist[k] = normr;
         niters = k;
         if(!std::isfinite(normr)) break;
@@ -575,6 +640,7 @@ void destroy(hpcgb200_dist* D)
 {
     if(!D) return;
     if(rt().initialized) cudaStreamSynchronize(rt().stream);
+    if(D->graph_exec) cudaGraphExecDestroy(D->graph_exec);  // before its communicator goes
     for(auto& Lv : D->L)
     {
         dfree(Lv.send_perm);
@@ -718,9 +784,11 @@ extern "C" int hpcgb200_dist_create(int nx, int ny, int nz, int nlevels, int siz
     if(size < 1 || rank < 0 || rank >= size) return hb::record_error(HPCGB200_ERR_ARG, "bad size/rank");
     if(npx <= 0 || npy <= 0 || npz <= 0) optimal_shape(size, npx, npy, npz);
     if(npx * npy * npz != size) return hb::record_error(HPCGB200_ERR_ARG, "process grid does not match size");
+    static std::atomic<unsigned long long> next_serial{1};
     auto* D = new hpcgb200_dist;
     D->size = size;
     D->rank = rank;
+    D->serial = next_serial++;
     int rc = hpcgb200_problem_create(nx, ny, nz, nlevels, &D->local);
     if(rc)
     {

@@ -11,8 +11,11 @@ waits for another), checked against the multi-rank oracle
 * CG: the same initial residual and iteration count as the oracle (+-1), the
   history within 1e-6 while the residual is well above rounding, the solution
   of the generated problem all ones;
-* one rank with a one-rank NCCL communicator gives the group result bit for
-  bit (the allreduce of one rank is the identity).
+* the steady iterations as a cached CUDA graph give the direct launches'
+  history bit for bit;
+* one rank with a one-rank NCCL communicator (its allreduce captured in the
+  graph) gives the group result bit for bit (the allreduce of one rank is the
+  identity).
 """
 import numpy as np
 import pytest
@@ -136,6 +139,18 @@ def test_cg_matches_oracle(case):
     assert got["normr"] / got["normr0"] <= 1e-9
     for P in R:
         np.testing.assert_allclose(P.get_x(), 1.0, atol=1e-6)
+
+
+def test_graph_iterations_equal_direct_launches(case, monkeypatch):
+    """The steady iterations run as one cached CUDA graph each; the same
+    kernels launched one by one give the same history bit for bit."""
+    size, loc, nl, R, O = case
+    g1 = D.group_cg(R, 200, 1e-9)
+    g2 = D.group_cg(R, 200, 1e-9)  # the cached graph again
+    monkeypatch.setenv("HPCGB200_DIST_GRAPH", "0")
+    d = D.group_cg(R, 200, 1e-9)
+    assert g1["niters"] == g2["niters"] == d["niters"] > 1
+    assert np.array_equal(g1["hist"], d["hist"]) and np.array_equal(g2["hist"], d["hist"])
 
 
 def test_one_rank_equals_single_rank_problem(oracle_libs):
