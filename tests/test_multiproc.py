@@ -81,3 +81,21 @@ def test_reference_arm_runs_on_rank_zero_only():
     assert r.returncode == 0, r.stderr
     lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1 and lines[0]["impl"] == "reference"
+
+
+def test_decomposed_bench_model_and_launch_count():
+    """bench.py's decomposed line: the HPCG flop model of the GLOBAL grid, and
+    the kernels one rank launches per CG iteration."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from rochpcg_b200 import hpcg_model
+
+    (f, _), dims = bench.dist_model(256, (2, 2, 1))
+    assert dims[0] == (512, 512, 256) and dims[3] == (64, 64, 32)
+    want, _ = hpcg_model(dims, [bench.stencil_nnz(d) for d in dims])
+    assert f == want
+
+    class FakeRank:
+        levels = [{"nblocks": 8}] * 4
+    # 3 levels with restriction/prolongation: (15) + 3 + 1 + (3 + 7 + 7); coarsest (15); CG 7
+    assert bench.dist_launches_per_iter(FakeRank()) == 3 * (15 + 4 + 17) + 15 + 7
