@@ -531,6 +531,13 @@ int hpcgb200_benchmark_report(hpcgb200_benchmark_result* result, char* json, siz
  * (host only). */
 int hpcgb200_dist_shape(int size, int* npx, int* npy, int* npz);
 
+/* src/GenerateGeometry.cpp:49-169 (host only; the C++ GenerateGeometry):
+ * out[13] = {npx, npy, npz, ipx, ipy, ipz, gnx, gny, gnz, gix0, giy0, giz0,
+ * npartz} of `rank` (npx*npy*npz <= 0 or > size: hpcgb200_dist_shape; pz > 0:
+ * process planes below pz hold zl points in z, the others zu). */
+int hpcgb200_geometry(int size, int rank, int pz, int zl, int zu, int nx, int ny, int nz, int npx, int npy, int npz,
+                      long long* out);
+
 /* src/SetupHalo.cpp:135-651 on the host (no device needed): the halo plan of
  * `rank` for a local brick nx*ny*nz (npx/npy/npz <= 0: hpcgb200_dist_shape).
  * hpcgb200_halo_plan_info fills info[16] = {m, externals, neighbours,

@@ -98,6 +98,8 @@ def ref_lib(rows: bool = False):
         L.hpcgref_optimal_shape.argtypes = [ctypes.c_int, _c_int_p, _c_int_p, _c_int_p]
         L.hpcgref_optimal_shape.restype = None
         L.hpcgref_rank_problem.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p] * 5
+        L.hpcgref_geometry.argtypes = [ctypes.c_int] * 11 + [ctypes.c_void_p]
+        L.hpcgref_geometry.restype = None
         _ref_libs[so] = L
     return _ref_libs[so]
 
@@ -108,6 +110,13 @@ def ref_optimal_shape(size: int) -> tuple[int, int, int]:
     x, y, z = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     L.hpcgref_optimal_shape(size, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z))
     return x.value, y.value, z.value
+
+
+def ref_geometry(size, rank, pz, zl, zu, nx, ny, nz, npx=0, npy=0, npz=0) -> list[int]:
+    """The reference's GenerateGeometry (src/GenerateGeometry.cpp)."""
+    out = np.zeros(13, np.int64)
+    ref_lib().hpcgref_geometry(size, rank, pz, zl, zu, nx, ny, nz, npx, npy, npz, _ptr(out))
+    return [int(v) for v in out]
 
 
 def ref_rank_problem(size: int, rank: int, nx: int, ny: int, nz: int) -> dict:

@@ -318,6 +318,18 @@ void hpcgref_optimal_shape(int size, int* npx, int* npy, int* npz)
     *npx = x, *npy = y, *npz = z;
 }
 
+// The reference's GenerateGeometry (src/GenerateGeometry.cpp): out[13] =
+// {npx, npy, npz, ipx, ipy, ipz, gnx, gny, gnz, gix0, giy0, giz0, npartz}.
+void hpcgref_geometry(int size, int rank, int pz, int zl, int zu, int nx, int ny, int nz, int npx, int npy, int npz,
+                      long long* out)
+{
+    Geometry g;
+    GenerateGeometry(size, rank, 1, pz, zl, zu, nx, ny, nz, npx, npy, npz, &g);
+    const long long v[13] = {g.npx, g.npy, g.npz, g.ipx, g.ipy, g.ipz, g.gnx, g.gny, g.gnz, g.gix0, g.giy0, g.giz0,
+                             g.npartz};
+    std::memcpy(out, v, sizeof(v));
+}
+
 // Rank `rank` of a `size`-rank run with local brick nx*ny*nz, as the
 // reference generates it (src/GenerateGeometry.cpp + src/GenerateProblem_ref.cpp
 // with the geometry's global offsets): per natural row its GLOBAL column ids

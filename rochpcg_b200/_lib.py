@@ -101,6 +101,7 @@ SIGNATURES = {
     "hpcgb200_problem_time_op": (_i, [_vp, _cp, _i, _vp]),
     # domain decomposition
     "hpcgb200_dist_shape": (_i, [_i, _vp, _vp, _vp]),
+    "hpcgb200_geometry": (_i, [_i] * 11 + [_vp]),
     "hpcgb200_halo_plan_create": (_i, [_i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     "hpcgb200_halo_plan_info": (_i, [_vp, _vp]),
     "hpcgb200_halo_plan_copy": (_i, [_vp, _cp, _vp, _sz]),

@@ -724,6 +724,19 @@ extern "C" int hpcgb200_dist_shape(int size, int* npx, int* npy, int* npz)
     return 0;
 }
 
+extern "C" int hpcgb200_geometry(int size, int rank, int pz, int zl, int zu, int nx, int ny, int nz, int npx, int npy,
+                                 int npz, long long* out)
+{
+    if(!out || size < 1 || rank < 0 || rank >= size) return hb::record_error(HPCGB200_ERR_ARG, "bad argument");
+    Geometry g{};
+    GenerateGeometry(size, rank, 1, pz, zl, zu, nx, ny, nz, npx, npy, npz, &g);
+    const long long v[13] = {g.npx, g.npy, g.npz, g.ipx, g.ipy, g.ipz, g.gnx, g.gny, g.gnz, g.gix0, g.giy0, g.giz0,
+                             g.npartz};
+    std::memcpy(out, v, sizeof(v));
+    DeleteGeometry(g);
+    return 0;
+}
+
 extern "C" int hpcgb200_halo_plan_create(int nx, int ny, int nz, int size, int rank, int npx, int npy, int npz,
                                          hpcgb200_halo_plan** out)
 {

@@ -1,41 +1,91 @@
-// Problem construction: src/GenerateGeometry.cpp:49-169 (single rank),
+// Problem construction: src/GenerateGeometry.cpp:49-169,
 // src/GenerateProblem.cpp:375-489, src/SetupHalo.cpp:294-327 (single rank),
 // src/GenerateCoarseProblem.cpp:98-184 and the deleters of
 // src/SparseMatrix.hpp:264-330 / src/MGData.hpp:101-120.
 #include <cstring>
+#include <string>
 
+#include "dist.hpp"
 #include "hpcg_b200.h"
 #include "internal.hpp"
 
 using namespace hpcg_b200;
 
+// The process grid (the given one when it fits in size ranks, else the
+// least-surface split of size), this rank's coordinates and its brick's
+// global offsets; with pz > 0 the process planes below z-index pz hold nz =
+// zl points, the others zu (the reference's two z zones).
 void GenerateGeometry(int size, int rank, int numThreads, int pz, local_int_t zl, local_int_t zu, local_int_t nx,
                       local_int_t ny, local_int_t nz, int npx, int npy, int npz, Geometry* geom)
 {
-    // One rank (the tier fixes a single GPU): a 1x1x1 process grid.
-    (void)npx;
-    (void)npy;
-    (void)npz;
-    (void)zl;
-    (void)zu;
-    (void)pz;
+    if(npx * npy * npz <= 0 || npx * npy * npz > size) optimal_shape(size, npx, npy, npz);
     geom->size = size;
     geom->rank = rank;
     geom->numThreads = numThreads;
     geom->nx = nx;
     geom->ny = ny;
     geom->nz = nz;
-    geom->npx = geom->npy = geom->npz = 1;
-    geom->pz = 0;
-    geom->npartz = 1;
-    geom->partz_ids = new int[1]{1};
-    geom->partz_nz = new local_int_t[1]{nz};
-    geom->ipx = geom->ipy = geom->ipz = 0;
-    geom->gnx = nx;
-    geom->gny = ny;
-    geom->gnz = nz;
-    geom->gix0 = geom->giy0 = geom->giz0 = 0;
+    geom->npx = npx;
+    geom->npy = npy;
+    geom->npz = npz;
+    geom->pz = pz;
+    if(pz == 0)
+    {
+        geom->npartz = 1;
+        geom->partz_ids = new int[1]{npz};
+        geom->partz_nz = new local_int_t[1]{nz};
+    }
+    else
+    {
+        geom->npartz = 2;
+        geom->partz_ids = new int[2]{pz, npz};
+        geom->partz_nz = new local_int_t[2]{zl, zu};
+    }
+    geom->ipz = rank / (npx * npy);
+    geom->ipy = (rank - geom->ipz * npx * npy) / npx;
+    geom->ipx = rank % npx;
+    geom->gnx = (global_int_t)npx * nx;
+    geom->gny = (global_int_t)npy * ny;
+    // z extent and offset over the zones: zone i spans process planes
+    // [partz_ids[i-1], partz_ids[i]) with partz_nz[i] points each
+    global_int_t gnz = 0, giz0 = 0;
+    int lo = 0;
+    bool placed = false;
+    for(int i = 0; i < geom->npartz; ++i)
+    {
+        const int hi = geom->partz_ids[i];
+        gnz += (global_int_t)geom->partz_nz[i] * (hi - lo);
+        if(!placed)
+        {
+            if(geom->ipz < hi)
+            {
+                giz0 += (global_int_t)(geom->ipz - lo) * geom->partz_nz[i];
+                placed = true;
+            }
+            else
+                giz0 += (global_int_t)(hi - lo) * geom->partz_nz[i];
+        }
+        lo = hi;
+    }
+    geom->gnz = gnz;
+    geom->gix0 = (global_int_t)geom->ipx * nx;
+    geom->giy0 = (global_int_t)geom->ipy * ny;
+    geom->giz0 = giz0;
 }
+
+namespace {
+
+// The C++ operator layer holds one rank; a decomposed problem is built and
+// solved through hpcgb200_dist_* (its own halo plan and exchange).
+void require_one_rank(const SparseMatrix& A, const char* what)
+{
+    if(A.geom && A.geom->size > 1)
+        throw Error(HPCGB200_ERR_ARG, std::string(what) + ": a geometry of " + std::to_string(A.geom->size) +
+                                          " ranks; the C++ operator layer holds one rank, build decomposed problems "
+                                          "with hpcgb200_dist_create (include/hpcg_b200.h)");
+}
+
+}  // namespace
 
 void DeleteGeometry(Geometry& geom)
 {
@@ -57,6 +107,7 @@ void InitializeSparseMatrix(SparseMatrix& A, Geometry* geom)
 
 void GenerateProblem(SparseMatrix& A, Vector* b, Vector* x, Vector* xexact)
 {
+    require_one_rank(A, "GenerateProblem");
     ensure_runtime();
     cudaStream_t s = rt().stream;
     const local_int_t nx = A.geom->nx, ny = A.geom->ny, nz = A.geom->nz;
@@ -123,7 +174,9 @@ void GenerateCoarseProblem(const SparseMatrix& Af)
     check(hpcgb200_f2c_operator(nxf, nyf, nzf, f2c, c2f, rt().stream));
 
     Geometry* geomc = new Geometry;
-    GenerateGeometry(Af.geom->size, Af.geom->rank, Af.geom->numThreads, 0, 0, 0, nxc, nyc, nzc, 1, 1, 1, geomc);
+    GenerateGeometry(Af.geom->size, Af.geom->rank, Af.geom->numThreads, Af.geom->pz,
+                     Af.geom->pz > 0 ? Af.geom->partz_nz[0] / 2 : 0, Af.geom->pz > 0 ? Af.geom->partz_nz[1] / 2 : 0, nxc,
+                     nyc, nzc, Af.geom->npx, Af.geom->npy, Af.geom->npz, geomc);
     SparseMatrix* Ac = new SparseMatrix;
     InitializeSparseMatrix(*Ac, geomc);
     GenerateProblem(*Ac, nullptr, nullptr, nullptr);

@@ -248,3 +248,28 @@ def test_gloo_ranks_exchange_halos_with_the_library_plan(world, loc):
     res = sorted(q.get(timeout=5) for _ in range(world))
     assert all(ok for _, ok, _ in res), res
     assert all(n > 0 for _, _, n in res)
+
+
+@pytest.mark.parametrize("size", [1, 2, 3, 4, 6, 8, 12, 16, 27, 30])
+def test_cpp_geometry_matches_reference(size, oracle_libs):
+    """The C++ GenerateGeometry (process grid, coordinates, global offsets,
+    the two-zone z split) against the reference's own, every rank."""
+    import ctypes
+
+    if not _ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference source tree)")
+    from rochpcg_b200 import load
+
+    L = load()
+    # process grids of exactly `size` ranks (the given one, the computed one, a
+    # row of ranks); a z split (pz > 0) needs more than pz process planes
+    grids = [(0, 0, 0), D.shape(size), (size, 1, 1), (1, 1, size)]
+    for grid in grids:
+        npz = grid[2] if grid[0] else D.shape(size)[2]
+        for pz, zl, zu in [(0, 0, 0)] + ([(1, 6, 10)] if npz > 1 else []):
+            for rank in range(size):
+                out = np.zeros(13, np.int64)
+                assert L.hpcgb200_geometry(size, rank, pz, zl, zu, 8, 6, 4, *grid,
+                                           out.ctypes.data_as(ctypes.c_void_p)) == 0
+                want = oracle_libs.ref_geometry(size, rank, pz, zl, zu, 8, 6, 4, *grid)
+                assert list(out) == want, (size, rank, pz, grid)
