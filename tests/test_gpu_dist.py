@@ -25,23 +25,33 @@ from rochpcg_b200 import dist as D
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(2, (16, 16, 16), 4), (4, (16, 8, 16), 4), (8, (8, 16, 8), 4), (3, (16, 8, 8), 4), (12, (8, 8, 8), 3)]
+# (ranks, brick, levels, process grid or None for the reference's own): every
+# neighbour direction alone and together, bricks with odd coarse levels
+# (24x16x8 -> 3x2x1), up to 12 ranks
+CASES = [(2, (16, 16, 16), 4, None), (4, (16, 8, 16), 4, None), (8, (8, 16, 8), 4, None), (3, (16, 8, 8), 4, None),
+         (12, (8, 8, 8), 3, None), (2, (16, 16, 16), 4, (1, 2, 1)), (2, (16, 16, 16), 4, (1, 1, 2)),
+         (4, (24, 16, 8), 4, (1, 2, 2)), (6, (8, 8, 8), 3, (1, 2, 3))]
 
 
-def _ranks(size, loc, nlevels):
-    return [D.DistProblem(*loc, size, r, nlevels=nlevels) for r in range(size)]
+def _ranks(size, loc, nlevels, grid=None):
+    return [D.DistProblem(*loc, size, r, nlevels=nlevels, grid=grid) for r in range(size)]
 
 
 def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-@pytest.fixture(scope="module", params=CASES, ids=lambda c: f"{c[0]}ranks-{c[1][0]}x{c[1][1]}x{c[1][2]}")
+def _case_id(c):
+    grid = "" if c[3] is None else "-grid" + "x".join(map(str, c[3]))
+    return f"{c[0]}ranks-{c[1][0]}x{c[1][1]}x{c[1][2]}{grid}"
+
+
+@pytest.fixture(scope="module", params=CASES, ids=_case_id)
 def case(request, oracle_libs):
-    size, loc, nl = request.param
+    size, loc, nl, grid = request.param
     torch.cuda.set_device(0)
-    R = _ranks(size, loc, nl)
-    O = oracle_libs.DistOracle(size, *loc, nlevels=nl)
+    R = _ranks(size, loc, nl, grid)
+    O = oracle_libs.DistOracle(size, *loc, nlevels=nl, grid=grid)
     yield size, loc, nl, R, O
     for r in R:
         r.close()
@@ -49,7 +59,7 @@ def case(request, oracle_libs):
 
 def test_setup_bit_exact(case):
     size, loc, nl, R, O = case
-    assert R[0].grid == D.shape(size)
+    assert R[0].grid[0] * R[0].grid[1] * R[0].grid[2] == size
     for rank, P in enumerate(R):
         for l in range(nl):
             assert P.levels[l]["m"] == O.info[rank][l]["m"] and P.levels[l]["next"] == O.info[rank][l]["next"]
