@@ -7,6 +7,9 @@
 //
 // Row-wise results are bit-identical to the reference kernels (same fma
 // order); reductions use a fixed-shape deterministic tree.
+#include <algorithm>
+#include <vector>
+
 #include "ops64.cuh"
 
 namespace hb {
@@ -73,6 +76,7 @@ __global__ void __launch_bounds__(kBS) k_symgs_sweep(int m, int ncols, int size,
 // only the slots before the diagonal, only columns of earlier colours.  The
 // reference multiplies by __drcp_rn(a_ii); inv_diag = 1/a_ii is the same
 // correctly rounded value, read coalesced instead of from the diagonal slot.
+template <int GHI>
 __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset, const int* __restrict__ ell_col,
                                                     const double* __restrict__ ell_val,
                                                     const int* __restrict__ diag_idx,
@@ -86,8 +90,8 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
     if(offset > 0)
     {
         const int diag = diag_idx[row];
-        sum = ell_row_sum(m, row, ell_col, ell_val, x, sum, -1.0, 0, diag,
-                          [offset](int col) { return col >= 0 && col < offset; });
+        sum = ell_row_sum<0, GHI>(m, row, ell_col, ell_val, x, sum, -1.0, 0, diag,
+                                  [offset](int col) { return col >= 0 && col < offset; });
     }
     const double v = sum * inv_diag[row];
     x[row] = v;
@@ -95,6 +99,7 @@ __global__ void __launch_bounds__(kBS) k_symgs_fwd0(int m, int size, int offset,
 }
 
 // src/ComputeSYMGS.cpp:297-341 (kernel_backward_sweep_0).
+template <int GLO>
 __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset, const int* __restrict__ ell_col,
                                                     const double* __restrict__ ell_val,
                                                     const int* __restrict__ diag_idx, const double* __restrict__ diag,
@@ -105,8 +110,8 @@ __global__ void __launch_bounds__(kBS) k_symgs_bwd0(int m, int size, int offset,
     if(gid >= size) return;
     const int row = gid + offset;
     const int d = diag_idx[row];
-    const double sum = ell_row_sum(m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, d + 1, kWidth,
-                                   [offset, m](int col) { return col >= offset && col < m; });
+    const double sum = ell_row_sum<GLO, 3>(m, row, ell_col, ell_val, x, __dmul_rn(x[row], diag[row]), -1.0, d + 1,
+                                           kWidth, [offset, m](int col) { return col >= offset && col < m; });
     const double v = sum * inv_diag[row];
     x[row] = v;
     pro.add(row, v);
@@ -255,21 +260,102 @@ int launch_sweep_color(int m, int ncols, int size, int offset, const int* ell_co
 
 int launch_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                       const double* ell_val, const int* diag_idx, const double* diag, const double* inv_diag,
-                      const double* r, double* x, cudaStream_t s, Prolong<double> pro)
+                      const double* r, double* x, cudaStream_t s, Prolong<double> pro, const ZgGroups* zg)
 {
     for(int i = 0; i < nblocks; ++i)
     {
         if(sizes[i] <= 0) continue;
-        k_symgs_fwd0<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx,
-                                                                inv_diag, r, x, i > ublocks ? pro : Prolong<double>{});
+        const dim3 g((sizes[i] + kBS - 1) / kBS);
+        const Prolong<double> pv = i > ublocks ? pro : Prolong<double>{};
+        switch(zg ? zg[i].fhi : 3)
+        {
+        case 0:
+            k_symgs_fwd0<0><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, inv_diag, r, x, pv);
+            break;
+        case 1:
+            k_symgs_fwd0<1><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, inv_diag, r, x, pv);
+            break;
+        case 2:
+            k_symgs_fwd0<2><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, inv_diag, r, x, pv);
+            break;
+        default:
+            k_symgs_fwd0<3><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, inv_diag, r, x, pv);
+        }
         HB_LAUNCHED();
     }
     for(int i = ublocks; i >= 0; --i)
     {
         if(sizes[i] <= 0) continue;
-        k_symgs_bwd0<<<(sizes[i] + kBS - 1) / kBS, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx,
-                                                                diag, inv_diag, x, pro);
+        const dim3 g((sizes[i] + kBS - 1) / kBS);
+        switch(zg ? zg[i].blo : 0)
+        {
+        case 3:
+            k_symgs_bwd0<3><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, diag, inv_diag, x,
+                                              pro);
+            break;
+        case 2:
+            k_symgs_bwd0<2><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, diag, inv_diag, x,
+                                              pro);
+            break;
+        case 1:
+            k_symgs_bwd0<1><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, diag, inv_diag, x,
+                                              pro);
+            break;
+        default:
+            k_symgs_bwd0<0><<<g, kBS, 0, s>>>(m, sizes[i], offsets[i], ell_col, ell_val, diag_idx, diag, inv_diag, x,
+                                              pro);
+        }
         HB_LAUNCHED();
+    }
+    return 0;
+}
+
+__global__ void k_diag_bounds(int lo, int hi, const int* __restrict__ diag_idx, int* __restrict__ out)
+{
+    int mn = kWidth, mx = 0;
+    for(int i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += gridDim.x * blockDim.x)
+    {
+        const int d = diag_idx[i];
+        mn = min(mn, d);
+        mx = max(mx, d);
+    }
+    for(int o = 16; o > 0; o >>= 1)
+    {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if((threadIdx.x & 31) == 0)
+    {
+        atomicMin(out, mn);
+        atomicMax(out + 1, mx);
+    }
+}
+
+int zero_guess_groups(int m, int nblocks, const int* offsets, const int* diag_idx, ZgGroups* zg, cudaStream_t s)
+{
+    if(nblocks <= 0) return 0;
+    int* d = nullptr;
+    HB_CUDA(cudaMallocAsync(&d, sizeof(int) * 2 * nblocks, s));
+    std::vector<int> init(2 * nblocks), h(2 * nblocks);
+    for(int c = 0; c < nblocks; ++c) init[2 * c] = kWidth, init[2 * c + 1] = 0;
+    HB_CUDA(cudaMemcpyAsync(d, init.data(), sizeof(int) * 2 * nblocks, cudaMemcpyHostToDevice, s));
+    for(int c = 0; c < nblocks; ++c)
+    {
+        const int lo = offsets[c], hi = offsets[c + 1];
+        if(hi <= lo) continue;
+        const int blocks = std::min((hi - lo + kBS - 1) / kBS, kReduceBlocks);
+        k_diag_bounds<<<blocks, kBS, 0, s>>>(lo, hi, diag_idx, d + 2 * c);
+        HB_LAUNCHED();
+    }
+    HB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(int) * 2 * nblocks, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    HB_CUDA(cudaFreeAsync(d, s));
+    (void)m;
+    for(int c = 0; c < nblocks; ++c)
+    {
+        const int dmin = h[2 * c], dmax = h[2 * c + 1];
+        zg[c].fhi = (dmax + 8) / 9;                      // groups holding slots [0, dmax)
+        zg[c].blo = dmin >= kWidth ? 0 : (dmin + 1) / 9; // first group holding slot dmin + 1
     }
     return 0;
 }

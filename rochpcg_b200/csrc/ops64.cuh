@@ -41,14 +41,21 @@ ColorChunks make_chunks(int m, int ncolors, const int* offsets);
 // diagonal) with a branch measured slower (256^3 zero-guess SymGS 1.312 vs
 // 1.288 ms), the branch keeping the loads of the next group from starting
 // while the current one's fmas wait.
-template <typename ColPred>
+//
+// [GLO, GHI) bounds the groups at compile time: a caller that knows every row
+// of its launch needs only some groups (the zero-guess sweeps of a colour, from
+// the colour's extreme diagonal positions) issues no instructions for the
+// others; the sum is the same, since the groups left out hold no slot of the
+// range.
+template <int GLO = 0, int GHI = kWidth / 9, typename ColPred>
 __device__ __forceinline__ double ell_row_sum(int m, int row, const int* __restrict__ ell_col,
                                               const double* __restrict__ ell_val, const double* x, double sum,
                                               double s, int p_lo, int p_hi, ColPred use_col)
 {
     constexpr int G = 9;
+    static_assert(kWidth == 3 * G && 0 <= GLO && GLO <= GHI && GHI <= 3, "group range");
 #pragma unroll
-    for(int g = 0; g < kWidth; g += G)
+    for(int g = GLO * G; g < GHI * G; g += G)
     {
         int col[G];
         double v[G], xv[G];
@@ -89,9 +96,21 @@ int launch_symgs(int m, int nblocks, int ublocks, const int* sizes, const int* o
 // decomposed problem's sweeps; launch_symgs uses ncols = m).
 int launch_sweep_color(int m, int ncols, int size, int offset, const int* ell_col, const double* ell_val,
                        const double* inv_diag, const double* r, double* x, cudaStream_t s);
+// Groups of 9 ELL slots a colour's zero-guess passes need: the forward pass
+// groups [0, fhi) (slots before the diagonal), the backward pass [blo, 3).
+struct ZgGroups
+{
+    int fhi = 3;
+    int blo = 0;
+};
+// zg (one entry per colour, optional) narrows each colour's group range.
 int launch_symgs_zero(int m, int nblocks, int ublocks, const int* sizes, const int* offsets, const int* ell_col,
                       const double* ell_val, const int* diag_idx, const double* diag, const double* inv_diag,
-                      const double* r, double* x, cudaStream_t s, Prolong<double> pro = {});
+                      const double* r, double* x, cudaStream_t s, Prolong<double> pro = {},
+                      const ZgGroups* zg = nullptr);
+// The group ranges of colours [0, nblocks) from their rows' diagonal slots
+// (synchronizes the stream).
+int zero_guess_groups(int m, int nblocks, const int* offsets, const int* diag_idx, ZgGroups* zg, cudaStream_t s);
 // pro_f[inj_c[ic]] = inj_f[ic]: coarse permuted row -> injected fine permuted row.
 int launch_prolong_map(int nc, const int* inj_f, const int* inj_c, int* pro_f, cudaStream_t s);
 int launch_restrict(int nc, const int* inj_f, const int* inj_c, int mf, const int* ell_col, const double* ell_val,

@@ -393,7 +393,7 @@ void symgs_zero(Group& G, int l, const std::vector<double*>& rs, const std::vect
     each(G, [&](hpcgb200_dist* d, int i) {
         const SparseMatrix& A = *d->L[l].A;
         return hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind,
-                                     A.ell_val, A.diag_idx, opt(A)->diag, A.inv_diag, rs[i], xs[i], G.s);
+                                     A.ell_val, A.diag_idx, opt(A)->diag, A.inv_diag, rs[i], xs[i], G.s, {}, zg_of(A));
     });
 }
 

@@ -100,6 +100,8 @@ struct LevelOpt
     int jpl_blocks = 0;                // the reference's nblocks (2 per JPL round)
     std::vector<int> round_sizes;      // the reference's per-round sizes[]
     hb::ColorChunks cc{};              // colour-interleaved SpMV map
+    hb::ZgGroups zg[HPCGB200_MAX_COLORS];  // per colour: slot groups the zero-guess passes need
+    bool zg_ok = false;
 
     // FP32 / implicit-stencil data
     bool stencil_ok = false;
@@ -151,6 +153,11 @@ struct MGOpt
 bool fused_prolongation();
 
 inline LevelOpt* opt(const SparseMatrix& A) { return static_cast<LevelOpt*>(A.optimizationData); }
+inline const hb::ZgGroups* zg_of(const SparseMatrix& A)
+{
+    const LevelOpt* o = opt(A);
+    return o && o->zg_ok ? o->zg : nullptr;
+}
 inline MGOpt* mgopt(const SparseMatrix& A) { return A.mgData ? static_cast<MGOpt*>(A.mgData->optimizationData) : nullptr; }
 
 // Operators on raw FP32 level data (mixed V-cycle), defined in operators.cpp.

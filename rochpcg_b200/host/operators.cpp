@@ -51,7 +51,7 @@ int ComputeSYMGSZeroGuess(const SparseMatrix& A, const Vector& r, Vector& x)
     return guarded([&] {
         return hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind,
                                      A.ell_val, A.diag_idx, opt(A)->diag, A.inv_diag, r.d_values, x.d_values,
-                                     rt().stream);
+                                     rt().stream, {}, zg_of(A));
     });
 }
 
@@ -113,7 +113,7 @@ int mg64_ell(const SparseMatrix& A, const Vector& r, Vector& x, hb::Prolong<doub
     const int m = A.localNumberOfRows;
     auto zero_guess = [&](hb::Prolong<double> p) {
         return hb::launch_symgs_zero(m, A.nblocks, A.ublocks, A.sizes, A.offsets, A.ell_col_ind, A.ell_val,
-                                     A.diag_idx, opt(A)->diag, A.inv_diag, r.d_values, x.d_values, s, p);
+                                     A.diag_idx, opt(A)->diag, A.inv_diag, r.d_values, x.d_values, s, p, zg_of(A));
     };
     auto full = [&](hb::Prolong<double> p) {
         ExchangeHalo(A, x);
@@ -225,7 +225,8 @@ int mg64_stencil(const SparseMatrix& A, const double* r, double* x, cudaStream_t
     if(vec) HB_RETURN_IF(hb::launch64v_symgs_zero(o->st, o->diag, A.inv_diag, r, x, s, pz));
     else
         HB_RETURN_IF(hb::launch_symgs_zero(A.localNumberOfRows, A.nblocks, A.ublocks, A.sizes, A.offsets,
-                                           A.ell_col_ind, A.ell_val, A.diag_idx, o->diag, A.inv_diag, r, x, s, pz));
+                                           A.ell_col_ind, A.ell_val, A.diag_idx, o->diag, A.inv_diag, r, x, s, pz,
+                                           zg_of(A)));
     if(!A.mgData) return 0;
     const MGOpt* mo = mgopt(A);
     const int nc = A.Ac->localNumberOfRows;

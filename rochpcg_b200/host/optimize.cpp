@@ -59,6 +59,8 @@ static void optimize_level(SparseMatrix& A)
     A.inv_diag = dalloc<double>(m);
     o->diag = dalloc<double>(m);
     check(hpcgb200_extract_diagonal(m, A.ell_col_ind, A.ell_val, A.diag_idx, A.inv_diag, o->diag, s));
+    check(hb::zero_guess_groups(m, A.nblocks, A.offsets, A.diag_idx, o->zg, s));
+    o->zg_ok = true;
     o->cc = hb::make_chunks(m, A.nblocks, A.offsets);
 
     // -- FP32 implicit stencil (mixed path): verify before enabling
