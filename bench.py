@@ -325,7 +325,7 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (HPCG generator)", "impl": "reference",
         "config": {"workload": f"HPCG {nx}^3 FP64 MG-PCG (4 levels), generated b, x0=0", "grid": [nx, nx, nx],
-                   "mg_levels": 4, "parallelism": "replicas"},
+                   "mg_levels": 4, "parallelism": "one CPU process (rank 0), OpenMP threads"},
         "cpu_baseline": {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample,
                          **cpu_facts()},
         "e2e": {"value": gflops, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
