@@ -274,9 +274,10 @@ def host_threads():
 
 
 def cpu_baseline(args):
-    """configs[0] (32^3, 50 CG_ref iterations, generated b, x0 = 0) is the
-    primary CPU figure, repeated for about 10 s; a 128^3 x 10-iteration sample
-    shows the reference at a size whose working set leaves the caches."""
+    """The reference's CPU-runnable case (32^3, 50 CG_ref iterations, generated
+    b, x0 = 0) is the primary CPU figure, repeated for about 10 s; a 128^3 x
+    10-iteration sample shows the reference at a size whose working set leaves
+    the caches."""
     facts = cpu_facts()
     out = {"unit": "GFLOP/s", "cores": host_threads(), "kind": "reference", **facts}
     try:
