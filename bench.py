@@ -548,6 +548,13 @@ def run_ours(args):
         ref_errors = dict(checker.errors)
         checker.close()
 
+    # ---- the decomposed path on this GPU: 8 ranks of 64^3 (global 128^3)
+    # driven from this process (device-copy exchange), checked against the
+    # exact solution; a correctness record, not a multi-GPU measurement
+    decomposed = None
+    if rank == 0 and world == 1:
+        decomposed = decomposed_check()
+
     # ---- CPU baseline: the reference's CG_ref on host cores (rank 0, N=1),
     # after the checker has exited so that nothing else uses the host cores
     cpu = None
@@ -582,7 +589,7 @@ def run_ours(args):
             "roofline": roofline, "kernels": extra_kernels, "fp64_stencil": stencil, "cpu_baseline": cpu,
             "mixed": mixed,
             "learned": learned, "largest": largest,
-            "gpu_launches": launches, "clocks": clocks,
+            "gpu_launches": launches, "clocks": clocks, "decomposed_check": decomposed,
         }
         attach_ref_residuals(line, ref_values, ref_errors)
         line["ref_spmv_check"] = ("every solve's final x checked on the host with the reference's ComputeSPMV_ref "
@@ -886,6 +893,25 @@ def run_profile_case(case: str) -> int:
 
 
 # ------------------------------------------------------------ decomposed solve
+
+def decomposed_check(nranks: int = 8, n: int = 64) -> dict:
+    """The decomposed solve with every rank in this process on one GPU: the
+    global 2n x 2n x 2n problem's generated b, x = 1 expected."""
+    from rochpcg_b200 import dist as D
+
+    R = [D.DistProblem(n, n, n, nranks, r) for r in range(nranks)]
+    try:
+        D.group_cg(R, 500, 1e-9)  # captures the steady-iteration graph
+        r = D.group_cg(R, 500, 1e-9)
+        err = max(float(np.max(np.abs(P.get_x() - 1.0))) for P in R)
+        g = R[0].grid
+        return {"ranks": nranks, "local_grid": [n, n, n], "process_grid": list(g),
+                "global_grid": [g[0] * n, g[1] * n, g[2] * n], "iterations": r["niters"],
+                "rel_residual": r["normr"] / r["normr0"], "max_abs_x_minus_1": err, "seconds": r["seconds"],
+                "exchange": "device copies between the ranks' buffers (one GPU)"}
+    finally:
+        for P in R:
+            P.close()
 
 def dist_launches_per_iter(P) -> int:
     """Our kernels per CG iteration of one rank of the decomposed solve (NCCL's
