@@ -480,6 +480,8 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     ensure_runtime();
     Hierarchy H;
     // ---- set-up phase (src/main.cpp:188-215)
+    TracePhases trace;
+    trace.phase("hpcg:setup");
     sync();
     double t = wall();
     H.geom = new Geometry;
@@ -505,6 +507,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     R.postsmoother_steps = H.A.mgData->numberOfPostsmootherSteps;
 
     // ---- CheckProblem on every level (src/main.cpp:218-246)
+    trace.phase("hpcg:CheckProblem");
     if(verify)
     {
         cur = &H.A;
@@ -515,6 +518,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     }
 
     // ---- reference SpMV+MG timing (src/main.cpp:275-306)
+    trace.phase("hpcg:reference SpMV+MG timing");
     const int numberOfCalls = quickPath ? 1 : 10;
     if(verify)
     {
@@ -534,6 +538,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     }
 
     // ---- reference CG: the residual reduction of 50 iterations (src/main.cpp:312-341)
+    trace.phase("hpcg:reference CG");
     const int refMaxIters = 50;
     R.ref_max_iters = refMaxIters;
     double refTolerance = P.tol;
@@ -551,6 +556,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     R.ref_tolerance = refTolerance;
 
     // ---- OptimizeProblem (src/main.cpp:343-356)
+    trace.phase("hpcg:OptimizeProblem");
     sync();
     t = wall();
     check(OptimizeProblem(H.A, H.data, H.b, H.x, H.xexact));
@@ -559,6 +565,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     R.optimize_problem_bytes = optimize_problem_bytes(numberOfMgLevels, R.rows);
 
     // ---- validation (src/main.cpp:370-386)
+    trace.phase("hpcg:TestCG + TestSymmetry");
     if(verify)
     {
         TestCGData tc{};
@@ -577,6 +584,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     }
 
     // ---- optimized CG set-up: iterations to reach the reference residual (src/main.cpp:400-445)
+    trace.phase("hpcg:optimized CG set-up");
     int optMaxIters = 10 * refMaxIters;
     int optNiters = refMaxIters;
     double opt_worst_time = 0.0;
@@ -600,6 +608,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     R.opt_worst_time = opt_worst_time;
 
     // ---- timed CG sets (src/main.cpp:472-530)
+    trace.phase("hpcg:timed CG sets");
     const double total_runtime = P.running_time;
     const int numberOfCgSets = int(total_runtime / opt_worst_time) + 1;
     optMaxIters = optNiters;
@@ -620,6 +629,7 @@ int run_protocol(const hpcgb200_benchmark_params& P, hpcgb200_benchmark_result& 
     R.cg_sets = actualCgSets;
 
     // ---- TestNorms (src/main.cpp:532-556)
+    trace.phase("hpcg:TestNorms");
     TestNormsData tn{};
     tn.samples = actualCgSets;
     tn.values = scaled_residual.data();

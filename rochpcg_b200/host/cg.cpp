@@ -272,6 +272,7 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
            double* seconds, double* phase_seconds)
 {
     const bool timed = phase_seconds != nullptr;
+    TraceRange trace("hpcg:CG");
     try
     {
         ensure_runtime();

@@ -230,6 +230,7 @@ void each(Group& G, F&& f)
 // Send buffers are packed (on G.s); the external tails of xs[i] receive.
 void exchange_begin(Group& G, int l, const std::vector<double*>& xs)
 {
+    TraceRange trace("hpcg:ExchangeHalo");
     if(G.use_nccl)
     {
         hpcgb200_dist* d = G.R[0];
@@ -294,6 +295,7 @@ void pack(Group& G, int l, const std::vector<double*>& xs)
 // Sum of slot `k` of every rank's scalars, left in every rank's slot.
 void allreduce(Group& G, int k)
 {
+    TraceRange trace("hpcg:Allreduce");
     if(G.use_nccl)
     {
         hpcgb200_dist* d = G.R[0];
@@ -492,6 +494,7 @@ cudaGraphExec_t steady_graph(Group& G, bool precond, F&& body)
 void cg(Group& G, int max_iter, double tol, bool precond, int& niters, double& normr, double& normr0, double* hist,
         double* seconds)
 {
+    TraceRange trace("hpcg:CG (decomposed)");
     const auto rs = vecs(G, [](hpcgb200_dist* d) { return d->r; });
     const auto zs = vecs(G, [](hpcgb200_dist* d) { return d->z; });
     const auto ps = vecs(G, [](hpcgb200_dist* d) { return d->p; });
@@ -576,6 +579,7 @@ T* upload(const std::vector<T>& v, cudaStream_t s)
 
 void setup_level(hpcgb200_dist* D, int l, const DistGeom& g, int* d_status)
 {
+    TraceRange trace("hpcg:SetupHalo");
     cudaStream_t s = rt().stream;
     DistLevel& Lv = D->L[l];
     Lv.A = D->local->levels[l];

@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../csrc/cg.cuh"
 #include "../csrc/learned.cuh"
 #include "../csrc/mixed.cuh"
@@ -33,6 +35,33 @@ inline void check(int rc)
     if(rc != 0) throw_last(rc);
 }
 #define HB_HOST_CUDA(call) ::hpcg_b200::check_cuda((call), #call)
+
+// NVTX ranges (the reference's roctx ranges: set-up, optimization, CG, halo
+// exchange, allreduce, benchmark phases) for profilers such as Nsight; with
+// no tool attached they cost nothing.
+struct TraceRange
+{
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
+
+// Consecutive phases of one function: phase() closes the previous range.
+struct TracePhases
+{
+    bool open = false;
+    void phase(const char* name)
+    {
+        if(open) nvtxRangePop();
+        nvtxRangePushA(name);
+        open = true;
+    }
+    ~TracePhases()
+    {
+        if(open) nvtxRangePop();
+    }
+};
 
 struct Runtime
 {

@@ -113,6 +113,8 @@ extern "C" int hpcgb200_problem_create_ex(int nx, int ny, int nz, int nlevels, i
     auto* P = new hpcgb200_problem;
     const int rc = guarded([&] {
         g_keep_generated = (flags & HPCGB200_FLAG_KEEP_GENERATED) != 0;
+        TracePhases trace;
+        trace.phase("hpcg:GenerateProblem");
         const auto t0 = std::chrono::steady_clock::now();
         P->geom = new Geometry;
         GenerateGeometry(1, 0, 1, 0, 0, 0, nx, ny, nz, 1, 1, 1, P->geom);
@@ -129,6 +131,7 @@ extern "C" int hpcgb200_problem_create_ex(int nx, int ny, int nz, int nlevels, i
         }
         HB_HOST_CUDA(cudaStreamSynchronize(rt().stream));
         const auto t1 = std::chrono::steady_clock::now();
+        trace.phase("hpcg:OptimizeProblem");
         int r = OptimizeProblem(P->A, P->data, P->b, P->x, P->xexact);
         if(r) return r;
         HB_HOST_CUDA(cudaStreamSynchronize(rt().stream));
