@@ -65,3 +65,21 @@ def test_bench_reference_arm_schema():
     assert d["impl"] == "reference"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "reference"
+
+
+def test_solve_cli_arguments():
+    """python -m rochpcg_b200.solve: the reference's grid arguments plus the
+    solver flags (host-only parsing)."""
+    import pytest
+    from rochpcg_b200.solve import parse_args
+
+    a = parse_args(["64", "32", "16", "--precision=mixed", "--rhs=normal:9999", "--tol=1e-8"])
+    assert a["dims"] == (64, 32, 16) and a["precision"] == "mixed" and a["rhs"] == ("normal", 9999)
+    assert a["tol"] == 1e-8 and a["smoother"] == "symgs"
+    a = parse_args(["--nx=96", "--smoother=learned"])
+    assert a["dims"] == (96, 96, 96) and a["smoother"] == "learned" and a["rhs"] == ("ones", None)
+    assert parse_args([])["dims"] == (128, 128, 128)
+    for bad in (["--precision=fp16"], ["--rhs=uniform"], ["--smoother=jacobi"], ["--bogus=1"],
+                ["--precision=fp64_stencil", "--smoother=learned"]):
+        with pytest.raises(ValueError):
+            parse_args(bad)
