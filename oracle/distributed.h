@@ -56,6 +56,19 @@ void od_mg(od_problem* P, double** rs, double** xs);                           /
 void od_cg(od_problem* P, int max_iter, double tol, int precond, double** bs, double** xs, int* niters,
            double* normr, double* normr0, double* hist);
 
+/* The REFERENCE (natural-order `_ref`) path over the same decomposition
+ * (oracle/distributed_ref.c): vectors hold every rank's rows rank after rank,
+ * each rank's in natural order.  src/test_rochpcg.cpp:262-271 runs its CG_ref
+ * for 50 iterations to fix the tolerance of the optimized CG. */
+typedef struct odr_problem odr_problem;
+odr_problem* odr_create(int size, int npx, int npy, int npz, int nx, int ny, int nz, int nlevels);
+void odr_destroy(odr_problem* P);
+void odr_spmv(const odr_problem* P, int level, const double* x, double* y);  /* ComputeSPMV_ref.cpp:48-75 */
+void odr_symgs(odr_problem* P, int level, const double* r, double* x);      /* ComputeSYMGS_ref.cpp:51-111 */
+void odr_mg(odr_problem* P, const double* r, double* x);                    /* ComputeMG_ref.cpp:38-66 */
+void odr_cg(odr_problem* P, int max_iter, double tol, int precond, int* niters, double* normr, double* normr0,
+            double* hist);                                                   /* CG_ref.cpp:86-170 */
+
 #ifdef __cplusplus
 }
 #endif

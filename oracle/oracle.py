@@ -565,6 +565,74 @@ class DistOracle:
         return {"niters": it.value, "normr": nr.value, "normr0": nr0.value, "hist": hist[:it.value + 1], "x": xs}
 
 
+def _dist_ref_lib():
+    L = _dist_lib()
+    if not getattr(L, "_odr_ready", False):
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.odr_create.argtypes = [ci] * 8
+        L.odr_create.restype = vp
+        L.odr_destroy.argtypes = [vp]
+        L.odr_spmv.argtypes = [vp, ci, vp, vp]
+        L.odr_symgs.argtypes = [vp, ci, vp, vp]
+        L.odr_mg.argtypes = [vp, vp, vp]
+        L.odr_cg.argtypes = [vp, ci, ctypes.c_double, ci, _c_int_p, _c_dbl_p, _c_dbl_p, vp]
+        for name in ("odr_destroy", "odr_spmv", "odr_symgs", "odr_mg", "odr_cg"):
+            getattr(L, name).restype = None
+        L._odr_ready = True
+    return L
+
+
+class DistRefOracle:
+    """The reference's natural-order `_ref` path over a decomposition
+    (oracle/distributed_ref.c): vectors hold every rank's rows, rank after
+    rank, each in natural order.  `cg(50, 0.0)` gives the tolerance that
+    src/test_rochpcg.cpp:262-271 fixes before it runs the optimized CG."""
+
+    def __init__(self, size: int, nx: int, ny: int, nz: int, nlevels: int = 4, grid=None):
+        self.L = _dist_ref_lib()
+        npx, npy, npz = grid if grid else (0, 0, 0)
+        self.h = self.L.odr_create(size, npx, npy, npz, nx, ny, nz, nlevels)
+        if not self.h:
+            raise ValueError("odr_create: process grid does not match size, or a level is empty")
+        self.size, self.m = size, nx * ny * nz
+        self.dims = [(nx >> l, ny >> l, nz >> l) for l in range(nlevels)]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.odr_destroy(self.h)
+            self.h = None
+
+    def rows(self, level: int = 0) -> int:
+        nx, ny, nz = self.dims[level]
+        return self.size * nx * ny * nz
+
+    def spmv(self, level: int, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.rows(level))
+        self.L.odr_spmv(self.h, level, _ptr(x), _ptr(y))
+        return y
+
+    def symgs(self, level: int, r: np.ndarray, x: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.array(x, np.float64)
+        self.L.odr_symgs(self.h, level, _ptr(r), _ptr(x))
+        return x
+
+    def mg(self, r: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        x = np.zeros(self.rows(0))
+        self.L.odr_mg(self.h, _ptr(r), _ptr(x))
+        return x
+
+    def cg(self, max_iter: int, tol: float, precond: bool = True) -> dict:
+        hist = np.zeros(max_iter + 1)
+        it = ctypes.c_int()
+        nr, nr0 = ctypes.c_double(), ctypes.c_double()
+        self.L.odr_cg(self.h, max_iter, tol, 1 if precond else 0, ctypes.byref(it), ctypes.byref(nr),
+                      ctypes.byref(nr0), _ptr(hist))
+        return {"niters": it.value, "normr": nr.value, "normr0": nr0.value, "hist": hist[:it.value + 1]}
+
+
 def bf16(a: np.ndarray) -> np.ndarray:
     """fp32 -> bf16 (round to nearest even) -> fp32, vectorised like oc_bf16."""
     u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)

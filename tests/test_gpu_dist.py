@@ -15,7 +15,10 @@ waits for another), checked against the multi-rank oracle
   history bit for bit;
 * one rank with a one-rank NCCL communicator (its allreduce captured in the
   graph) gives the group result bit for bit (the allreduce of one rank is the
-  identity).
+  identity);
+* the reference's own multi-rank test: on 2 and 4 ranks of 16^3 ... 128^3 the
+  decomposed CG reaches the tolerance of 50 multi-rank CG_ref iterations within
+  src/test_rochpcg.cpp's iteration bound.
 """
 import numpy as np
 import pytest
@@ -254,3 +257,32 @@ def test_decomposed_solution_checked_by_the_global_operator():
         G.close()
         for P in R:
             P.close()
+
+
+# (ranks, cubic brick edge): src/test_rochpcg.cpp's multi-rank cases up to
+# 128^3 per rank, plus (2, 32), which it holds to its default bound of 50
+REF_BOUND_CASES = [(2, 16), (4, 16), (2, 32), (4, 32), (2, 48), (4, 48), (2, 64), (4, 64), (2, 80), (4, 80),
+                   (2, 128), (4, 128)]
+
+
+@pytest.mark.parametrize("size,n", REF_BOUND_CASES, ids=lambda v: str(v))
+def test_reference_multi_rank_iteration_bounds(oracle_libs, size, n):
+    """src/test_rochpcg.cpp:262-311 on `size` ranks of n^3: 50 CG_ref
+    iterations over the decomposition (the natural-order multi-rank
+    restatement) fix the tolerance; the decomposed CUDA CG must reach it within
+    check_niter's bound (src/test_rochpcg.cpp:88-119), from the same initial
+    residual."""
+    from niter_bounds import check_niter
+
+    ref = oracle_libs.DistRefOracle(size, n, n, n).cg(50, 0.0)
+    tol = ref["normr"] / ref["normr0"]
+    torch.cuda.set_device(0)
+    R = _ranks(size, (n, n, n), 4)
+    try:
+        got = D.group_cg(R, 500, tol)
+    finally:
+        for P in R:
+            P.close()
+    np.testing.assert_allclose(got["normr0"], ref["normr0"], rtol=1e-14)
+    assert got["normr"] / got["normr0"] <= tol
+    assert got["niters"] <= check_niter(size, (n, n, n)), (got["niters"], tol)
