@@ -3,12 +3,21 @@
 // neighbours are gathered with all loads issued before the ordered adds (an
 // absent neighbour contributes -0.0f, which leaves any sum unchanged, so the
 // rounding sequence is exactly the ELL sweep's).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <array>
+#include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <mutex>
 #include <type_traits>
 #include <utility>
+#include <vector>
 
 #include "mixed.cuh"
+#include "tma.cuh"
 
 namespace hb {
 
@@ -737,6 +746,303 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, con
         }
     }
     pro.add4(b.row0, out);
+}
+
+// ------------------------------------------------------------ TMA-staged FP32 colour passes
+// The FP32 colour passes of the V-cycle on large levels with the canonical
+// colouring -- the full sweep (kv_sweep) and the zero-guess forward and
+// backward passes (kv_fwd0, kv_bwd0) -- with their neighbourhoods staged by
+// TMA.  A CTA of 8 x 16 x 2 threads takes a 32 x 16 x 2 tile of its colour's
+// brick (four x-adjacent rows per thread).  One thread loads, with one tiled
+// TMA box per colour the pass reads (every other colour for the sweep, the
+// earlier ones forward, the later ones backward), the part of that colour's
+// brick the tile's neighbourhoods cover: the tile itself, grown by one brick
+// column along x (4 floats: a box starts and spans in 16-byte units), one line
+// along y and one plane along z on the axes where that colour's parity
+// differs, on the side the launching colour's parity gives.  The boxes
+// complete on one mbarrier (zero fill outside the grid); every thread then
+// adds its rows' neighbours out of shared memory in the ELL slot order, -0.0f
+// for the absent ones, with the per-row prologue and epilogue of the kernel it
+// replaces -- the same bits.
+constexpr int kTmaX = 32, kTmaY = 16, kTmaZ = 2;
+constexpr int kTmaThreads = (kTmaX / 4) * kTmaY * kTmaZ;
+
+enum : int
+{
+    kTmaSweep = 0,  // x = (r + sum of all neighbours) / a_ii            (kv_sweep)
+    kTmaFwd0 = 1,   // x = (r + sum of the earlier colours) / a_ii         (kv_fwd0)
+    kTmaBwd0 = 2    // x = (x a_ii + sum of the later colours) / a_ii      (kv_bwd0)
+};
+
+__host__ __device__ constexpr int tma_sel(int kind) { return kind == kTmaSweep ? kOff : (kind == kTmaFwd0 ? kBefore : kAfter); }
+
+struct TmaTile
+{
+    int u;                   // colour of the staged brick
+    int bx, by, bz;          // box (floats, lines, planes)
+    int sx, sy, sz;          // box start = tile origin - (sx, sy, sz)
+    int off;                 // shared-memory offset (floats, multiple of 32: 128-byte aligned)
+};
+
+struct TmaPlan
+{
+    int nt;                  // staged colours
+    TmaTile t[7];            // in colour order
+    int total;               // shared-memory floats
+    unsigned bytes;          // bytes the boxes deliver
+    int tile[27];            // per ELL slot: staged tile (-1: not read by this pass)
+    int ax[27], ay[27], az[27];  // slot's position in its tile relative to the row's (4 tx, ty, tz)
+};
+
+__host__ __device__ constexpr int canon_parity(int colour)
+{
+    int p = 0;
+    while(p < 7 && canon_colour(p) != colour) ++p;
+    return p;
+}
+
+// floor(a / 2) for a >= -2
+__host__ __device__ constexpr int half_floor(int a) { return (a + 2) / 2 - 1; }
+
+// colour u is read by a pass of kind `kind` of colour v
+__host__ __device__ constexpr bool tma_reads(int kind, int v, int u)
+{
+    return u != v && (kind == kTmaSweep || (kind == kTmaFwd0 ? u < v : u > v));
+}
+
+__host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
+{
+    TmaPlan P{};
+    const int px = (cls >> 2) & 1, py = (cls >> 1) & 1, pz = cls & 1;
+    const int v = canon_colour(cls);
+    int idx[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    int i = 0, off = 0;
+    unsigned bytes = 0;
+    for(int u = 0; u < 8; ++u)
+    {
+        if(!tma_reads(kind, v, u)) continue;
+        const int d = cls ^ canon_parity(u);
+        const int dx = (d >> 2) & 1, dy = (d >> 1) & 1, dz = d & 1;
+        TmaTile t{};
+        t.u = u;
+        t.bx = kTmaX + 4 * dx;
+        t.by = kTmaY + dy;
+        t.bz = kTmaZ + dz;
+        t.sx = (dx && !px) ? 4 : 0;
+        t.sy = (dy && !py) ? 1 : 0;
+        t.sz = (dz && !pz) ? 1 : 0;
+        t.off = off;
+        off += (t.bx * t.by * t.bz + 31) / 32 * 32;
+        bytes += (unsigned)(t.bx * t.by * t.bz) * 4u;
+        idx[u] = i;
+        P.t[i++] = t;
+    }
+    P.nt = i;
+    P.total = off;
+    P.bytes = bytes;
+    const KvSlots k = kv_slots(cls);
+    for(int j = 0; j < 27; ++j)
+    {
+        P.tile[j] = -1;
+        if(!(tma_sel(kind) == kBefore ? j < k.dp : (tma_sel(kind) == kAfter ? j > k.dp : j != k.dp))) continue;
+        const int u = canon_colour(cls ^ (((k.dx[j] & 1) << 2) | ((k.dy[j] & 1) << 1) | (k.dz[j] & 1)));
+        const int ti = idx[u];
+        P.tile[j] = ti;
+        if(ti < 0) continue;
+        P.ax[j] = half_floor(px + k.dx[j]) + P.t[ti].sx;
+        P.ay[j] = half_floor(py + k.dy[j]) + P.t[ti].sy;
+        P.az[j] = half_floor(pz + k.dz[j]) + P.t[ti].sz;
+    }
+    return P;
+}
+
+template <int kCls, int kKind>
+struct TmaTab
+{
+    static constexpr TmaPlan p = tma_plan(kCls, kKind);
+};
+
+// Every slot a pass reads lies inside its staged tile, and every slot of the
+// pass's selection has a tile (checked at compile time for all eight classes
+// and the three kinds, with the largest thread position).
+__host__ __device__ constexpr bool tma_plan_ok(int cls, int kind)
+{
+    const TmaPlan P = tma_plan(cls, kind);
+    const KvSlots k = kv_slots(cls);
+    for(int j = 0; j < 27; ++j)
+    {
+        const bool want = tma_sel(kind) == kBefore ? j < k.dp : (tma_sel(kind) == kAfter ? j > k.dp : j != k.dp);
+        if(want != (P.tile[j] >= 0)) return false;
+        if(P.tile[j] < 0) continue;
+        const TmaTile& t = P.t[P.tile[j]];
+        const int lo = P.ax[j] - (P.ax[j] & 3), hi = 4 * (kTmaX / 4 - 1) + lo + ((P.ax[j] & 3) ? 8 : 4);
+        if(lo < 0 || hi > t.bx || P.ay[j] < 0 || P.ay[j] + kTmaY > t.by || P.az[j] < 0 || P.az[j] + kTmaZ > t.bz)
+            return false;
+    }
+    return P.total * 4 + 128 <= 48 * 1024;
+}
+
+__host__ __device__ constexpr bool tma_plans_ok()
+{
+    for(int cls = 0; cls < 8; ++cls)
+        for(int kind = 0; kind < 3; ++kind)
+            if(!tma_plan_ok(cls, kind)) return false;
+    return true;
+}
+static_assert(tma_plans_ok(), "TMA colour-pass tiles");
+
+struct NbMaps
+{
+    CUtensorMap m[7];        // the staged colours' x bricks, in colour order
+};
+
+template <int kCls, int kKind, int J>
+__device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4])
+{
+    using Tab = TmaTab<kCls, kKind>;
+    constexpr int ti = Tab::p.tile[J];
+    if constexpr(ti >= 0)
+    {
+        constexpr int bx = Tab::p.t[ti].bx, by = Tab::p.t[ti].by, off = Tab::p.t[ti].off;
+        constexpr int ax = Tab::p.ax[J], ay = Tab::p.ay[J], az = Tab::p.az[J];
+        constexpr int s = ax & 3;
+        const float* q = sm + off + ((tz + az) * by + ty + ay) * bx + 4 * tx + (ax - s);
+        float v[4];
+        const float4 a = *reinterpret_cast<const float4*>(q);
+        if constexpr(s == 0)
+        {
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        }
+        else
+        {
+            const float4 e = *reinterpret_cast<const float4*>(q + 4);
+            const float w[8] = {a.x, a.y, a.z, a.w, e.x, e.y, e.z, e.w};
+#pragma unroll
+            for(int r = 0; r < 4; ++r) v[r] = w[s + r];
+        }
+        constexpr unsigned bj = KvTab<kCls>::s.bm[J];
+        if(b.fast)
+        {
+#pragma unroll
+            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + v[r];
+        }
+        else
+        {
+#pragma unroll
+            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & bj) ? -0.0f : v[r]);
+        }
+    }
+}
+
+template <int kCls, int kKind, int... J>
+__device__ __forceinline__ void tma_slots(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4],
+                                          std::integer_sequence<int, J...>)
+{
+    (tma_slot<kCls, kKind, J>(sm, tx, ty, tz, b, sum), ...);
+}
+
+// One colour pass of kind kKind.  Sweep: r -> x (and z64, when given, the FP64
+// copy); forward zero-guess: r64 (when kFromDouble, storing its float copy in
+// r) or r -> x; backward zero-guess: x, diag -> x.  status (may be null) gets
+// 3 when the copies did not arrive in time; the tile's rows are then set to
+// NaN, so the solve ends as non-finite.
+template <int kCls, int kKind, bool kFromDouble>
+__global__ void __launch_bounds__(kTmaThreads, 4)
+    kv_pass_tma(const __grid_constant__ NbMaps nb, const ColorLaunch c, const float* __restrict__ inv_diag,
+                const float* __restrict__ diag, const double* __restrict__ r64, float* __restrict__ r,
+                float* __restrict__ x, double* __restrict__ z64, int* status)
+{
+    using Tab = TmaTab<kCls, kKind>;
+    extern __shared__ unsigned char sm_raw[];
+    __shared__ uint64_t mbar;
+    float* sm = reinterpret_cast<float*>(sm_raw + ((128u - (tma::smem_u32(sm_raw) & 127u)) & 127u));
+    const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+    const int x0 = blockIdx.x * kTmaX, y0 = blockIdx.y * kTmaY, z0 = blockIdx.z * kTmaZ;
+    pdl_begin();
+    const bool leader = tx == 0 && ty == 0 && tz == 0;
+    if constexpr(Tab::p.nt > 0)
+    {
+        if(leader)
+        {
+            constexpr TmaPlan P = Tab::p;
+            tma::mbar_init(&mbar, 1);
+            tma::mbar_arrive_expect_tx(&mbar, P.bytes);
+#pragma unroll
+            for(int i = 0; i < P.nt; ++i)
+                tma::load_3d(sm + P.t[i].off, &nb.m[i], x0 - P.t[i].sx, y0 - P.t[i].sy, z0 - P.t[i].sz, &mbar);
+        }
+    }
+    // the rows' own data and face bits while the boxes are in flight
+    const int kx0 = x0 + 4 * tx, ky = y0 + ty, kz = z0 + tz;
+    Rows4 b;
+    b.in = kx0 < c.bx && ky < c.by && kz < c.bz;  // bx % 4 == 0: all four rows or none
+    b.row0 = c.off + (kz * c.by + ky) * c.bx + kx0;
+    {
+        const int iy = 2 * ky + ((c.par >> 1) & 1), iz = 2 * kz + (c.par & 1);
+        unsigned any = 0;
+#pragma unroll
+        for(int q = 0; q < 4; ++q)
+        {
+            b.mask[q] = b.in ? face_mask(c, 2 * (kx0 + q) + ((c.par >> 2) & 1), iy, iz) : 0u;
+            any |= b.mask[q];
+        }
+        b.fast = __all_sync(0xffffffffu, any == 0u);
+    }
+    float sum[4], inv[4];
+    if(b.in)
+    {
+        if constexpr(kKind == kTmaBwd0)
+        {
+            float xv[4], dv[4];
+            Quad<float>::load(x + b.row0, xv);
+            Quad<float>::load(diag + b.row0, dv);
+#pragma unroll
+            for(int q = 0; q < 4; ++q) sum[q] = mul_rn(xv[q], dv[q]);
+        }
+        else if constexpr(kFromDouble)
+        {
+            double a[4];
+            Quad<double>::load(r64 + b.row0, a);
+#pragma unroll
+            for(int q = 0; q < 4; ++q) sum[q] = (float)a[q];
+            Quad<float>::store(r + b.row0, sum);
+        }
+        else
+        {
+            Quad<float>::load(r + b.row0, sum);
+        }
+        Quad<float>::load(inv_diag + b.row0, inv);
+    }
+    if constexpr(Tab::p.nt > 0)
+    {
+        __syncthreads();  // the barrier is initialised before anyone waits on it
+        if(!tma::mbar_wait(&mbar, 0))
+        {
+            if(leader && status) atomicExch(status, 3);
+            if(b.in)
+            {
+                const float q = __int_as_float(0x7fc00000);
+                const float nan[4] = {q, q, q, q};
+                Quad<float>::store(x + b.row0, nan);
+            }
+            tma::mbar_wait(&mbar, 0);  // the copies still in flight land before the CTA leaves
+            return;
+        }
+    }
+    if(!b.in) return;
+    tma_slots<kCls, kKind>(sm, tx, ty, tz, b, sum, std::make_integer_sequence<int, 27>{});
+    float out[4];
+#pragma unroll
+    for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
+    Quad<float>::store(x + b.row0, out);
+    if constexpr(kKind == kTmaSweep)
+    {
+        if(z64)
+        {
+            const double zo[4] = {(double)out[0], (double)out[1], (double)out[2], (double)out[3]};
+            Quad<double>::store(z64 + b.row0, zo);
+        }
+    }
 }
 
 // Restriction on the 4-row layout: the injected fine points are the parity-0
@@ -1544,6 +1850,113 @@ cudaError_t by_shape_restrict(const StencilLevel& Lf, F&& f)
     return Lf.m / 8 < kV4SmallRows ? cls(IntC<kV4GroupSmallOf<T>>{}) : cls(IntC<kV4GroupLarge>{});
 }
 
+// TMA maps of one FP32 vector of a level: map[u][d] covers colour u's brick
+// with the box a launching colour sees when its parity differs from u's by d.
+struct SweepMaps
+{
+    const float* x = nullptr;
+    int m = 0, nx = 0, ny = 0, nz = 0;
+    CUtensorMap map[8][8];
+};
+
+static int encode_brick_map(CUtensorMap* map, const float* base, int bx, int by, int bz, int boxx, int boxy, int boxz)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if(!encode)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        HB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if(q != cudaDriverEntryPointSuccess || !fn)
+            return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)bx, (cuuint64_t)by, (cuuint64_t)bz};
+    const cuuint64_t strides[2] = {(cuuint64_t)bx * 4, (cuuint64_t)bx * by * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)boxx, (cuuint32_t)boxy, (cuuint32_t)boxz};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if(r != CUDA_SUCCESS) return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
+// Maps of x on level L, built once per (vector, level) and kept (a V-cycle
+// sweeps the same few vectors).
+static const SweepMaps* sweep_maps(const StencilLevel& L, const float* x)
+{
+    static std::mutex mu;
+    static std::vector<std::unique_ptr<SweepMaps>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    for(const auto& e : cache)
+        if(e->x == x && e->m == L.m && e->nx == L.nx && e->ny == L.ny && e->nz == L.nz) return e.get();
+    auto e = std::make_unique<SweepMaps>();
+    e->x = x;
+    e->m = L.m;
+    e->nx = L.nx;
+    e->ny = L.ny;
+    e->nz = L.nz;
+    for(int u = 0; u < 8; ++u)
+    {
+        const int bz = (L.nz - (L.par[u] & 1) + 1) / 2;
+        for(int d = 1; d < 8; ++d)
+            if(encode_brick_map(&e->map[u][d], x + L.offsets[u], L.bx[u], L.by[u], bz, kTmaX + 4 * ((d >> 2) & 1),
+                                kTmaY + ((d >> 1) & 1), kTmaZ + (d & 1)))
+                return nullptr;
+    }
+    if(cache.size() >= 64) cache.erase(cache.begin());
+    cache.push_back(std::move(e));
+    return cache.back().get();
+}
+
+// The TMA-staged colour passes serve large even levels with the canonical
+// colouring (HPCGB200_SWEEP_TMA=0 keeps the 4-row kernels everywhere).
+static bool sweep_tma_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("HPCGB200_SWEEP_TMA");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// Large even level with the canonical colouring, x 16-byte aligned, no fused
+// prolongation: the TMA-staged passes apply.
+static bool pass_tma_ok(const StencilLevel& L, const float* x, const Prolong<float>& pro)
+{
+    return sweep_tma_enabled() && vec4_ok(L) && L.canon && L.m / 8 >= kV4SmallRows && !pro.xf &&
+           (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
+}
+
+template <int C, int K, bool D>
+static cudaError_t launch_pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M,
+                                   const float* inv_diag32, const float* diag32, const double* r64, float* r, float* x,
+                                   double* z64, cudaStream_t s)
+{
+    NbMaps nb;
+    for(int u = 0, i = 0; u < 8; ++u)
+        if(tma_reads(K, c.v, u)) nb.m[i++] = M.map[u][L.par[c.v] ^ L.par[u]];
+    const dim3 grid((unsigned)((c.bx + kTmaX - 1) / kTmaX), (unsigned)((c.by + kTmaY - 1) / kTmaY),
+                    (unsigned)((c.bz + kTmaZ - 1) / kTmaZ));
+    const size_t smem = (size_t)TmaTab<C, K>::p.total * 4 + 128;
+    return launch_pdl_smem(kv_pass_tma<C, K, D>, grid, dim3(kTmaX / 4, kTmaY, kTmaZ), smem, s, nb, c, inv_diag32,
+                           diag32, r64, r, x, z64, L.status);
+}
+
+// One TMA-staged pass of kind K over colour c (canonical colouring: the
+// class is a compile-time constant).
+template <int K, bool D>
+static cudaError_t pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M, const float* inv_diag32,
+                            const float* diag32, const double* r64, float* r, float* x, double* z64, cudaStream_t s)
+{
+    return by_class(L, c.par, [&](auto kc) {
+        constexpr int C = decltype(kc)::value;
+        if constexpr(C < 0) return cudaErrorInvalidValue;  // L.canon holds on this path
+        else return launch_pass_tma<C, K, D>(L, c, M, inv_diag32, diag32, r64, r, x, z64, s);
+    });
+}
+
 // The colour n-1 is final after the forward sweep, the others after the
 // backward sweep (n-2..0): those passes carry the fused prolongation `pro`.
 int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float* inv_diag32, const double* r64,
@@ -1552,13 +1965,21 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     const int n = L.ncolors;
     const dim3 t(32, 8), t4(kV4X, kV4Y);
     const bool vec = vec4_ok(L);
+    const bool tma = pass_tma_ok(L, x, pro);
+    const SweepMaps* maps = tma ? sweep_maps(L, x) : nullptr;
+    if(tma && !maps) return HPCGB200_ERR_CUDA;
     for(int v = 0; v < n; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const dim3 g = brick_grid(c);
         const Prolong<float> pv = v == n - 1 ? pro : Prolong<float>{};
-        if(vec)
+        if(maps)
+        {
+            HB_CUDA((r64 ? pass_tma<kTmaFwd0, true>(L, c, *maps, inv_diag32, nullptr, r64, r32, x, nullptr, s)
+                         : pass_tma<kTmaFwd0, false>(L, c, *maps, inv_diag32, nullptr, nullptr, r32, x, nullptr, s)));
+        }
+        else if(vec)
         {
             HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
                 constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
@@ -1584,7 +2005,11 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
-        if(vec)
+        if(maps)
+        {
+            HB_CUDA((pass_tma<kTmaBwd0, false>(L, c, *maps, inv_diag32, diag32, nullptr, nullptr, x, nullptr, s)));
+        }
+        else if(vec)
         {
             HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
                 constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
@@ -1603,10 +2028,16 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
 {
     const int n = L.ncolors;
     const bool vec = vec4_ok(L);
+    const bool tma = pass_tma_ok(L, x, pro);
+    const SweepMaps* maps = tma ? sweep_maps(L, x) : nullptr;
+    if(tma && !maps) return HPCGB200_ERR_CUDA;
     auto sweep = [&](int v, double* z, Prolong<float> pv) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
-        if(vec)
+        if(maps)
+            HB_CUDA((pass_tma<kTmaSweep, false>(L, c, *maps, inv_diag32, nullptr, nullptr, const_cast<float*>(r), x,
+                                                z, s)));
+        else if(vec)
         {
             HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
                 constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
