@@ -769,12 +769,16 @@ constexpr int kTmaThreads = (kTmaX / 4) * kTmaY * kTmaZ;
 
 enum : int
 {
-    kTmaSweep = 0,  // x = (r + sum of all neighbours) / a_ii            (kv_sweep)
-    kTmaFwd0 = 1,   // x = (r + sum of the earlier colours) / a_ii         (kv_fwd0)
-    kTmaBwd0 = 2    // x = (x a_ii + sum of the later colours) / a_ii      (kv_bwd0)
+    kTmaSweep = 0,    // x = (r + sum of all neighbours) / a_ii            (kv_sweep)
+    kTmaFwd0 = 1,     // x = (r + sum of the earlier colours) / a_ii         (kv_fwd0)
+    kTmaBwd0 = 2,     // x = (x a_ii + sum of the later colours) / a_ii      (kv_bwd0)
+    kTmaRestrict = 3  // rc[inj_c] = r - A x on the parity-0 colour         (kv_restrict)
 };
 
-__host__ __device__ constexpr int tma_sel(int kind) { return kind == kTmaSweep ? kOff : (kind == kTmaFwd0 ? kBefore : kAfter); }
+__host__ __device__ constexpr int tma_sel(int kind)
+{
+    return (kind == kTmaSweep || kind == kTmaRestrict) ? kOff : (kind == kTmaFwd0 ? kBefore : kAfter);
+}
 
 struct TmaTile
 {
@@ -807,7 +811,7 @@ __host__ __device__ constexpr int half_floor(int a) { return (a + 2) / 2 - 1; }
 // colour u is read by a pass of kind `kind` of colour v
 __host__ __device__ constexpr bool tma_reads(int kind, int v, int u)
 {
-    return u != v && (kind == kTmaSweep || (kind == kTmaFwd0 ? u < v : u > v));
+    return u != v && (tma_sel(kind) == kOff || (kind == kTmaFwd0 ? u < v : u > v));
 }
 
 __host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
@@ -885,7 +889,7 @@ __host__ __device__ constexpr bool tma_plan_ok(int cls, int kind)
 __host__ __device__ constexpr bool tma_plans_ok()
 {
     for(int cls = 0; cls < 8; ++cls)
-        for(int kind = 0; kind < 3; ++kind)
+        for(int kind = 0; kind < 4; ++kind)
             if(!tma_plan_ok(cls, kind)) return false;
     return true;
 }
@@ -896,12 +900,20 @@ struct NbMaps
     CUtensorMap m[7];        // the staged colours' x bricks, in colour order
 };
 
+// Slot J of the rows' ELL walk; the restriction's diagonal slot is
+// fma(-a_ii, x_i, sum) with the row's own xo and dg.
 template <int kCls, int kKind, int J>
-__device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4])
+__device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4],
+                                         const float (&xo)[4], const float (&dg)[4])
 {
     using Tab = TmaTab<kCls, kKind>;
     constexpr int ti = Tab::p.tile[J];
-    if constexpr(ti >= 0)
+    if constexpr(kKind == kTmaRestrict && J == KvTab<kCls>::s.dp)
+    {
+#pragma unroll
+        for(int r = 0; r < 4; ++r) sum[r] = fma_rn(-dg[r], xo[r], sum[r]);
+    }
+    else if constexpr(ti >= 0)
     {
         constexpr int bx = Tab::p.t[ti].bx, by = Tab::p.t[ti].by, off = Tab::p.t[ti].off;
         constexpr int ax = Tab::p.ax[J], ay = Tab::p.ay[J], az = Tab::p.az[J];
@@ -936,21 +948,23 @@ __device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz
 
 template <int kCls, int kKind, int... J>
 __device__ __forceinline__ void tma_slots(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4],
-                                          std::integer_sequence<int, J...>)
+                                          const float (&xo)[4], const float (&dg)[4], std::integer_sequence<int, J...>)
 {
-    (tma_slot<kCls, kKind, J>(sm, tx, ty, tz, b, sum), ...);
+    (tma_slot<kCls, kKind, J>(sm, tx, ty, tz, b, sum, xo, dg), ...);
 }
 
 // One colour pass of kind kKind.  Sweep: r -> x (and z64, when given, the FP64
 // copy); forward zero-guess: r64 (when kFromDouble, storing its float copy in
-// r) or r -> x; backward zero-guess: x, diag -> x.  status (may be null) gets
-// 3 when the copies did not arrive in time; the tile's rows are then set to
-// NaN, so the solve ends as non-finite.
+// r) or r -> x; backward zero-guess: x, diag -> x; restriction: r, x, diag ->
+// rc[inj_c] (x is only read).  status (may be null) gets 3 when the copies did
+// not arrive in time; the tile's outputs are then set to NaN, so the solve
+// ends as non-finite.
 template <int kCls, int kKind, bool kFromDouble>
 __global__ void __launch_bounds__(kTmaThreads, 4)
     kv_pass_tma(const __grid_constant__ NbMaps nb, const ColorLaunch c, const float* __restrict__ inv_diag,
                 const float* __restrict__ diag, const double* __restrict__ r64, float* __restrict__ r,
-                float* __restrict__ x, double* __restrict__ z64, int* status)
+                float* __restrict__ x, double* __restrict__ z64, const int* __restrict__ inj_c,
+                float* __restrict__ rc, int* status)
 {
     using Tab = TmaTab<kCls, kKind>;
     extern __shared__ unsigned char sm_raw[];
@@ -988,10 +1002,16 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
         }
         b.fast = __all_sync(0xffffffffu, any == 0u);
     }
-    float sum[4], inv[4];
+    float sum[4], inv[4], xo[4] = {}, dg[4] = {};
     if(b.in)
     {
-        if constexpr(kKind == kTmaBwd0)
+        if constexpr(kKind == kTmaRestrict)
+        {
+            Quad<float>::load(r + b.row0, sum);
+            Quad<float>::load(x + b.row0, xo);
+            Quad<float>::load(diag + b.row0, dg);
+        }
+        else if constexpr(kKind == kTmaBwd0)
         {
             float xv[4], dv[4];
             Quad<float>::load(x + b.row0, xv);
@@ -1011,7 +1031,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
         {
             Quad<float>::load(r + b.row0, sum);
         }
-        Quad<float>::load(inv_diag + b.row0, inv);
+        if constexpr(kKind != kTmaRestrict) Quad<float>::load(inv_diag + b.row0, inv);
     }
     if constexpr(Tab::p.nt > 0)
     {
@@ -1022,15 +1042,35 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
             if(b.in)
             {
                 const float q = __int_as_float(0x7fc00000);
-                const float nan[4] = {q, q, q, q};
-                Quad<float>::store(x + b.row0, nan);
+                if constexpr(kKind == kTmaRestrict)
+                {
+                    const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
+                    rc[ic.x] = q;
+                    rc[ic.y] = q;
+                    rc[ic.z] = q;
+                    rc[ic.w] = q;
+                }
+                else
+                {
+                    const float nan[4] = {q, q, q, q};
+                    Quad<float>::store(x + b.row0, nan);
+                }
             }
             tma::mbar_wait(&mbar, 0);  // the copies still in flight land before the CTA leaves
             return;
         }
     }
     if(!b.in) return;
-    tma_slots<kCls, kKind>(sm, tx, ty, tz, b, sum, std::make_integer_sequence<int, 27>{});
+    tma_slots<kCls, kKind>(sm, tx, ty, tz, b, sum, xo, dg, std::make_integer_sequence<int, 27>{});
+    if constexpr(kKind == kTmaRestrict)
+    {
+        const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
+        rc[ic.x] = sum[0];
+        rc[ic.y] = sum[1];
+        rc[ic.z] = sum[2];
+        rc[ic.w] = sum[3];
+        return;
+    }
     float out[4];
 #pragma unroll
     for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
@@ -1932,7 +1972,7 @@ static bool pass_tma_ok(const StencilLevel& L, const float* x, const Prolong<flo
 template <int C, int K, bool D>
 static cudaError_t launch_pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M,
                                    const float* inv_diag32, const float* diag32, const double* r64, float* r, float* x,
-                                   double* z64, cudaStream_t s)
+                                   double* z64, const int* inj_c, float* rc, cudaStream_t s)
 {
     NbMaps nb;
     for(int u = 0, i = 0; u < 8; ++u)
@@ -1941,19 +1981,20 @@ static cudaError_t launch_pass_tma(const StencilLevel& L, const ColorLaunch& c, 
                     (unsigned)((c.bz + kTmaZ - 1) / kTmaZ));
     const size_t smem = (size_t)TmaTab<C, K>::p.total * 4 + 128;
     return launch_pdl_smem(kv_pass_tma<C, K, D>, grid, dim3(kTmaX / 4, kTmaY, kTmaZ), smem, s, nb, c, inv_diag32,
-                           diag32, r64, r, x, z64, L.status);
+                           diag32, r64, r, x, z64, inj_c, rc, L.status);
 }
 
 // One TMA-staged pass of kind K over colour c (canonical colouring: the
 // class is a compile-time constant).
 template <int K, bool D>
 static cudaError_t pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M, const float* inv_diag32,
-                            const float* diag32, const double* r64, float* r, float* x, double* z64, cudaStream_t s)
+                            const float* diag32, const double* r64, float* r, float* x, double* z64, cudaStream_t s,
+                            const int* inj_c = nullptr, float* rc = nullptr)
 {
     return by_class(L, c.par, [&](auto kc) {
         constexpr int C = decltype(kc)::value;
         if constexpr(C < 0) return cudaErrorInvalidValue;  // L.canon holds on this path
-        else return launch_pass_tma<C, K, D>(L, c, M, inv_diag32, diag32, r64, r, x, z64, s);
+        else return launch_pass_tma<C, K, D>(L, c, M, inv_diag32, diag32, r64, r, x, z64, inj_c, rc, s);
     });
 }
 
@@ -2062,7 +2103,13 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
                       const float* rf, const float* xf, float* rc, cudaStream_t s)
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
-    if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
+    const SweepMaps* maps = pass_tma_ok(Lf, xf, {}) && nc == c.bx * c.by * c.bz ? sweep_maps(Lf, xf) : nullptr;
+    if(maps)
+    {
+        HB_CUDA((pass_tma<kTmaRestrict, false>(Lf, c, *maps, nullptr, diag32, nullptr, const_cast<float*>(rf),
+                                                const_cast<float*>(xf), nullptr, s, inj_c, rc)));
+    }
+    else if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
     {
         HB_CUDA(by_shape_restrict<float>(Lf, [&](auto kg, auto kc) {
             constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
