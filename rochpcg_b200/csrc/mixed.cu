@@ -748,24 +748,32 @@ __global__ void __launch_bounds__(kV4X * kV4Y) kv_sweep(const ColorLaunch c, con
     pro.add4(b.row0, out);
 }
 
-// ------------------------------------------------------------ TMA-staged FP32 colour passes
-// The FP32 colour passes of the V-cycle on large levels with the canonical
-// colouring -- the full sweep (kv_sweep) and the zero-guess forward and
-// backward passes (kv_fwd0, kv_bwd0) -- with their neighbourhoods staged by
-// TMA.  A CTA of 8 x 16 x 2 threads takes a 32 x 16 x 2 tile of its colour's
-// brick (four x-adjacent rows per thread).  One thread loads, with one tiled
-// TMA box per colour the pass reads (every other colour for the sweep, the
-// earlier ones forward, the later ones backward), the part of that colour's
-// brick the tile's neighbourhoods cover: the tile itself, grown by one brick
-// column along x (4 floats: a box starts and spans in 16-byte units), one line
-// along y and one plane along z on the axes where that colour's parity
-// differs, on the side the launching colour's parity gives.  The boxes
-// complete on one mbarrier (zero fill outside the grid); every thread then
-// adds its rows' neighbours out of shared memory in the ELL slot order, -0.0f
-// for the absent ones, with the per-row prologue and epilogue of the kernel it
-// replaces -- the same bits.
-constexpr int kTmaX = 32, kTmaY = 16, kTmaZ = 2;
-constexpr int kTmaThreads = (kTmaX / 4) * kTmaY * kTmaZ;
+// ------------------------------------------------------------ TMA-staged colour passes
+// The colour passes of the FP32 (mixed) and FP64 (stencil) V-cycles on large
+// levels with the canonical colouring -- the full sweep (kv_sweep), the
+// zero-guess forward and backward passes (kv_fwd0, kv_bwd0) and the
+// restriction (kv_restrict) -- with their neighbourhoods staged by TMA.  A CTA
+// of 8 x TY x 2 threads takes a 32 x TY x 2 tile of its colour's brick (four
+// x-adjacent rows per thread; TY = 16 for float, 8 for double).  One thread
+// loads, with one tiled TMA box per colour the pass reads (every other colour
+// for the sweep and the restriction, the earlier ones forward, the later ones
+// backward), the part of that colour's brick the tile's neighbourhoods cover:
+// the tile itself, grown by one brick column along x (4 elements: a box
+// starts and spans in 16-byte units), one line along y and one plane along z
+// on the axes where that colour's parity differs, on the side the launching
+// colour's parity gives.  The boxes complete on one mbarrier (zero fill
+// outside the grid); every thread then adds its rows' neighbours out of shared
+// memory in the ELL slot order, -0 for the absent ones, with the per-row
+// prologue and epilogue of the kernel it replaces -- the same bits.
+constexpr int kTmaX = 32, kTmaZ = 2;
+template <typename T>
+constexpr int kTmaYOf = sizeof(T) == 4 ? 16 : 8;
+template <typename T>
+constexpr int kTmaThreadsOf = (kTmaX / 4) * kTmaYOf<T> * kTmaZ;
+// resident CTAs per SM the register budget is sized for (shared memory allows
+// 4-5 of the float tiles' up to 41 KB and the double tiles' up to 43 KB)
+template <typename T>
+constexpr int kTmaMinBlocksOf = sizeof(T) == 4 ? 4 : 5;
 
 enum : int
 {
@@ -783,16 +791,16 @@ __host__ __device__ constexpr int tma_sel(int kind)
 struct TmaTile
 {
     int u;                   // colour of the staged brick
-    int bx, by, bz;          // box (floats, lines, planes)
+    int bx, by, bz;          // box (elements, lines, planes)
     int sx, sy, sz;          // box start = tile origin - (sx, sy, sz)
-    int off;                 // shared-memory offset (floats, multiple of 32: 128-byte aligned)
+    int off;                 // shared-memory offset (elements; a multiple of 128 bytes)
 };
 
 struct TmaPlan
 {
     int nt;                  // staged colours
     TmaTile t[7];            // in colour order
-    int total;               // shared-memory floats
+    int total;               // shared-memory elements
     unsigned bytes;          // bytes the boxes deliver
     int tile[27];            // per ELL slot: staged tile (-1: not read by this pass)
     int ax[27], ay[27], az[27];  // slot's position in its tile relative to the row's (4 tx, ty, tz)
@@ -814,11 +822,18 @@ __host__ __device__ constexpr bool tma_reads(int kind, int v, int u)
     return u != v && (tma_sel(kind) == kOff || (kind == kTmaFwd0 ? u < v : u > v));
 }
 
-__host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
+__host__ __device__ constexpr bool tma_selected(int kind, int j, int dp)
+{
+    return tma_sel(kind) == kBefore ? j < dp : (tma_sel(kind) == kAfter ? j > dp : j != dp);
+}
+
+// ty: tile lines; esize: element bytes
+__host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind, int ty, int esize)
 {
     TmaPlan P{};
     const int px = (cls >> 2) & 1, py = (cls >> 1) & 1, pz = cls & 1;
     const int v = canon_colour(cls);
+    const int align = 128 / esize;
     int idx[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
     int i = 0, off = 0;
     unsigned bytes = 0;
@@ -830,14 +845,14 @@ __host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
         TmaTile t{};
         t.u = u;
         t.bx = kTmaX + 4 * dx;
-        t.by = kTmaY + dy;
+        t.by = ty + dy;
         t.bz = kTmaZ + dz;
         t.sx = (dx && !px) ? 4 : 0;
         t.sy = (dy && !py) ? 1 : 0;
         t.sz = (dz && !pz) ? 1 : 0;
         t.off = off;
-        off += (t.bx * t.by * t.bz + 31) / 32 * 32;
-        bytes += (unsigned)(t.bx * t.by * t.bz) * 4u;
+        off += (t.bx * t.by * t.bz + align - 1) / align * align;
+        bytes += (unsigned)(t.bx * t.by * t.bz * esize);
         idx[u] = i;
         P.t[i++] = t;
     }
@@ -848,7 +863,7 @@ __host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
     for(int j = 0; j < 27; ++j)
     {
         P.tile[j] = -1;
-        if(!(tma_sel(kind) == kBefore ? j < k.dp : (tma_sel(kind) == kAfter ? j > k.dp : j != k.dp))) continue;
+        if(!tma_selected(kind, j, k.dp)) continue;
         const int u = canon_colour(cls ^ (((k.dx[j] & 1) << 2) | ((k.dy[j] & 1) << 1) | (k.dz[j] & 1)));
         const int ti = idx[u];
         P.tile[j] = ti;
@@ -860,53 +875,88 @@ __host__ __device__ constexpr TmaPlan tma_plan(int cls, int kind)
     return P;
 }
 
-template <int kCls, int kKind>
+template <typename T, int kCls, int kKind>
 struct TmaTab
 {
-    static constexpr TmaPlan p = tma_plan(kCls, kKind);
+    static constexpr TmaPlan p = tma_plan(kCls, kKind, kTmaYOf<T>, (int)sizeof(T));
 };
 
-// Every slot a pass reads lies inside its staged tile, and every slot of the
-// pass's selection has a tile (checked at compile time for all eight classes
-// and the three kinds, with the largest thread position).
-__host__ __device__ constexpr bool tma_plan_ok(int cls, int kind)
+// Every slot a pass reads lies inside its staged tile, every slot of the
+// pass's selection has a tile, and the tiles fit the default dynamic shared
+// memory (checked at compile time for every class, kind and element size,
+// with the largest thread position).
+__host__ __device__ constexpr bool tma_plan_ok(int cls, int kind, int ty, int esize)
 {
-    const TmaPlan P = tma_plan(cls, kind);
+    const TmaPlan P = tma_plan(cls, kind, ty, esize);
     const KvSlots k = kv_slots(cls);
     for(int j = 0; j < 27; ++j)
     {
-        const bool want = tma_sel(kind) == kBefore ? j < k.dp : (tma_sel(kind) == kAfter ? j > k.dp : j != k.dp);
-        if(want != (P.tile[j] >= 0)) return false;
+        if(tma_selected(kind, j, k.dp) != (P.tile[j] >= 0)) return false;
         if(P.tile[j] < 0) continue;
         const TmaTile& t = P.t[P.tile[j]];
         const int lo = P.ax[j] - (P.ax[j] & 3), hi = 4 * (kTmaX / 4 - 1) + lo + ((P.ax[j] & 3) ? 8 : 4);
-        if(lo < 0 || hi > t.bx || P.ay[j] < 0 || P.ay[j] + kTmaY > t.by || P.az[j] < 0 || P.az[j] + kTmaZ > t.bz)
+        if(lo < 0 || hi > t.bx || P.ay[j] < 0 || P.ay[j] + ty > t.by || P.az[j] < 0 || P.az[j] + kTmaZ > t.bz)
             return false;
     }
-    return P.total * 4 + 128 <= 48 * 1024;
+    return P.total * esize + 128 <= 48 * 1024;
 }
 
 __host__ __device__ constexpr bool tma_plans_ok()
 {
     for(int cls = 0; cls < 8; ++cls)
         for(int kind = 0; kind < 4; ++kind)
-            if(!tma_plan_ok(cls, kind)) return false;
+            if(!tma_plan_ok(cls, kind, kTmaYOf<float>, 4) || !tma_plan_ok(cls, kind, kTmaYOf<double>, 8)) return false;
     return true;
 }
 static_assert(tma_plans_ok(), "TMA colour-pass tiles");
 
 struct NbMaps
 {
-    CUtensorMap m[7];        // the staged colours' x bricks, in colour order
+    CUtensorMap m[7];        // the staged colours' bricks of x, in colour order
 };
+
+// Four consecutive elements starting s (0..3) past a 4-aligned position of
+// shared memory: float4 loads for float, double2 loads for double.
+template <int kS>
+__device__ __forceinline__ void sm_quad(const float* q, float (&v)[4])
+{
+    const float4 a = *reinterpret_cast<const float4*>(q);
+    if constexpr(kS == 0)
+    {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    else
+    {
+        const float4 e = *reinterpret_cast<const float4*>(q + 4);
+        const float w[8] = {a.x, a.y, a.z, a.w, e.x, e.y, e.z, e.w};
+#pragma unroll
+        for(int r = 0; r < 4; ++r) v[r] = w[kS + r];
+    }
+}
+
+template <int kS>
+__device__ __forceinline__ void sm_quad(const double* q, double (&v)[4])
+{
+    constexpr int p0 = kS / 2, p1 = (kS + 3) / 2;  // double2 pairs covering [kS, kS + 4)
+    double w[8];
+#pragma unroll
+    for(int p = p0; p <= p1; ++p)
+    {
+        const double2 a = *reinterpret_cast<const double2*>(q + 2 * p);
+        w[2 * p] = a.x;
+        w[2 * p + 1] = a.y;
+    }
+#pragma unroll
+    for(int r = 0; r < 4; ++r) v[r] = w[kS + r];
+}
 
 // Slot J of the rows' ELL walk; the restriction's diagonal slot is
 // fma(-a_ii, x_i, sum) with the row's own xo and dg.
-template <int kCls, int kKind, int J>
-__device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4],
-                                         const float (&xo)[4], const float (&dg)[4])
+template <typename T, int kCls, int kKind, int J>
+__device__ __forceinline__ void tma_slot(const T* sm, int tx, int ty, int tz, const Rows4& b, T (&sum)[4],
+                                         const T (&xo)[4], const T (&dg)[4])
 {
-    using Tab = TmaTab<kCls, kKind>;
+    using Tab = TmaTab<T, kCls, kKind>;
     constexpr int ti = Tab::p.tile[J];
     if constexpr(kKind == kTmaRestrict && J == KvTab<kCls>::s.dp)
     {
@@ -918,20 +968,8 @@ __device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz
         constexpr int bx = Tab::p.t[ti].bx, by = Tab::p.t[ti].by, off = Tab::p.t[ti].off;
         constexpr int ax = Tab::p.ax[J], ay = Tab::p.ay[J], az = Tab::p.az[J];
         constexpr int s = ax & 3;
-        const float* q = sm + off + ((tz + az) * by + ty + ay) * bx + 4 * tx + (ax - s);
-        float v[4];
-        const float4 a = *reinterpret_cast<const float4*>(q);
-        if constexpr(s == 0)
-        {
-            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-        }
-        else
-        {
-            const float4 e = *reinterpret_cast<const float4*>(q + 4);
-            const float w[8] = {a.x, a.y, a.z, a.w, e.x, e.y, e.z, e.w};
-#pragma unroll
-            for(int r = 0; r < 4; ++r) v[r] = w[s + r];
-        }
+        T v[4];
+        sm_quad<s>(sm + off + ((tz + az) * by + ty + ay) * bx + 4 * tx + (ax - s), v);
         constexpr unsigned bj = KvTab<kCls>::s.bm[J];
         if(b.fast)
         {
@@ -941,37 +979,36 @@ __device__ __forceinline__ void tma_slot(const float* sm, int tx, int ty, int tz
         else
         {
 #pragma unroll
-            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & bj) ? -0.0f : v[r]);
+            for(int r = 0; r < 4; ++r) sum[r] = sum[r] + ((b.mask[r] & bj) ? T(-0.0) : v[r]);
         }
     }
 }
 
-template <int kCls, int kKind, int... J>
-__device__ __forceinline__ void tma_slots(const float* sm, int tx, int ty, int tz, const Rows4& b, float (&sum)[4],
-                                          const float (&xo)[4], const float (&dg)[4], std::integer_sequence<int, J...>)
+template <typename T, int kCls, int kKind, int... J>
+__device__ __forceinline__ void tma_slots(const T* sm, int tx, int ty, int tz, const Rows4& b, T (&sum)[4],
+                                          const T (&xo)[4], const T (&dg)[4], std::integer_sequence<int, J...>)
 {
-    (tma_slot<kCls, kKind, J>(sm, tx, ty, tz, b, sum, xo, dg), ...);
+    (tma_slot<T, kCls, kKind, J>(sm, tx, ty, tz, b, sum, xo, dg), ...);
 }
 
-// One colour pass of kind kKind.  Sweep: r -> x (and z64, when given, the FP64
-// copy); forward zero-guess: r64 (when kFromDouble, storing its float copy in
-// r) or r -> x; backward zero-guess: x, diag -> x; restriction: r, x, diag ->
-// rc[inj_c] (x is only read).  status (may be null) gets 3 when the copies did
-// not arrive in time; the tile's outputs are then set to NaN, so the solve
-// ends as non-finite.
-template <int kCls, int kKind, bool kFromDouble>
-__global__ void __launch_bounds__(kTmaThreads, 4)
-    kv_pass_tma(const __grid_constant__ NbMaps nb, const ColorLaunch c, const float* __restrict__ inv_diag,
-                const float* __restrict__ diag, const double* __restrict__ r64, float* __restrict__ r,
-                float* __restrict__ x, double* __restrict__ z64, const int* __restrict__ inj_c,
-                float* __restrict__ rc, int* status)
+// One colour pass of kind kKind.  Sweep: r -> x (and, FP32, z64 when given:
+// the FP64 copy); forward zero-guess: r -> x, or for FP32 with kFromDouble
+// r64 -> x storing the float copy of r64 in r; backward zero-guess: x, diag ->
+// x; restriction: r, x, diag -> rc[inj_c] (x is only read).  status (may be
+// null) gets 3 when the copies did not arrive in time; the tile's outputs are
+// then set to NaN, so the solve ends as non-finite.
+template <typename T, int kCls, int kKind, bool kFromDouble>
+__global__ void __launch_bounds__(kTmaThreadsOf<T>, kTmaMinBlocksOf<T>)
+    kv_pass_tma(const __grid_constant__ NbMaps nb, const ColorLaunch c, const T* __restrict__ inv_diag,
+                const T* __restrict__ diag, const double* __restrict__ r64, T* __restrict__ r, T* __restrict__ x,
+                double* __restrict__ z64, const int* __restrict__ inj_c, T* __restrict__ rc, int* status)
 {
-    using Tab = TmaTab<kCls, kKind>;
+    using Tab = TmaTab<T, kCls, kKind>;
     extern __shared__ unsigned char sm_raw[];
     __shared__ uint64_t mbar;
-    float* sm = reinterpret_cast<float*>(sm_raw + ((128u - (tma::smem_u32(sm_raw) & 127u)) & 127u));
+    T* sm = reinterpret_cast<T*>(sm_raw + ((128u - (tma::smem_u32(sm_raw) & 127u)) & 127u));
     const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-    const int x0 = blockIdx.x * kTmaX, y0 = blockIdx.y * kTmaY, z0 = blockIdx.z * kTmaZ;
+    const int x0 = blockIdx.x * kTmaX, y0 = blockIdx.y * kTmaYOf<T>, z0 = blockIdx.z * kTmaZ;
     pdl_begin();
     const bool leader = tx == 0 && ty == 0 && tz == 0;
     if constexpr(Tab::p.nt > 0)
@@ -1002,20 +1039,20 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
         }
         b.fast = __all_sync(0xffffffffu, any == 0u);
     }
-    float sum[4], inv[4], xo[4] = {}, dg[4] = {};
+    T sum[4], inv[4], xo[4] = {}, dg[4] = {};
     if(b.in)
     {
         if constexpr(kKind == kTmaRestrict)
         {
-            Quad<float>::load(r + b.row0, sum);
-            Quad<float>::load(x + b.row0, xo);
-            Quad<float>::load(diag + b.row0, dg);
+            Quad<T>::load(r + b.row0, sum);
+            Quad<T>::load(x + b.row0, xo);
+            Quad<T>::load(diag + b.row0, dg);
         }
         else if constexpr(kKind == kTmaBwd0)
         {
-            float xv[4], dv[4];
-            Quad<float>::load(x + b.row0, xv);
-            Quad<float>::load(diag + b.row0, dv);
+            T xv[4], dv[4];
+            Quad<T>::load(x + b.row0, xv);
+            Quad<T>::load(diag + b.row0, dv);
 #pragma unroll
             for(int q = 0; q < 4; ++q) sum[q] = mul_rn(xv[q], dv[q]);
         }
@@ -1024,14 +1061,14 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
             double a[4];
             Quad<double>::load(r64 + b.row0, a);
 #pragma unroll
-            for(int q = 0; q < 4; ++q) sum[q] = (float)a[q];
-            Quad<float>::store(r + b.row0, sum);
+            for(int q = 0; q < 4; ++q) sum[q] = (T)a[q];
+            Quad<T>::store(r + b.row0, sum);
         }
         else
         {
-            Quad<float>::load(r + b.row0, sum);
+            Quad<T>::load(r + b.row0, sum);
         }
-        if constexpr(kKind != kTmaRestrict) Quad<float>::load(inv_diag + b.row0, inv);
+        if constexpr(kKind != kTmaRestrict) Quad<T>::load(inv_diag + b.row0, inv);
     }
     if constexpr(Tab::p.nt > 0)
     {
@@ -1041,7 +1078,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
             if(leader && status) atomicExch(status, 3);
             if(b.in)
             {
-                const float q = __int_as_float(0x7fc00000);
+                const T q = (T)__int_as_float(0x7fc00000);
                 if constexpr(kKind == kTmaRestrict)
                 {
                     const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
@@ -1052,8 +1089,8 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
                 }
                 else
                 {
-                    const float nan[4] = {q, q, q, q};
-                    Quad<float>::store(x + b.row0, nan);
+                    const T nan[4] = {q, q, q, q};
+                    Quad<T>::store(x + b.row0, nan);
                 }
             }
             tma::mbar_wait(&mbar, 0);  // the copies still in flight land before the CTA leaves
@@ -1061,7 +1098,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
         }
     }
     if(!b.in) return;
-    tma_slots<kCls, kKind>(sm, tx, ty, tz, b, sum, xo, dg, std::make_integer_sequence<int, 27>{});
+    tma_slots<T, kCls, kKind>(sm, tx, ty, tz, b, sum, xo, dg, std::make_integer_sequence<int, 27>{});
     if constexpr(kKind == kTmaRestrict)
     {
         const int4 ic = *reinterpret_cast<const int4*>(inj_c + (b.row0 - c.off));
@@ -1071,11 +1108,11 @@ __global__ void __launch_bounds__(kTmaThreads, 4)
         rc[ic.w] = sum[3];
         return;
     }
-    float out[4];
+    T out[4];
 #pragma unroll
     for(int q = 0; q < 4; ++q) out[q] = sum[q] * inv[q];
-    Quad<float>::store(x + b.row0, out);
-    if constexpr(kKind == kTmaSweep)
+    Quad<T>::store(x + b.row0, out);
+    if constexpr(kKind == kTmaSweep && sizeof(T) == 4)
     {
         if(z64)
         {
@@ -1890,16 +1927,17 @@ cudaError_t by_shape_restrict(const StencilLevel& Lf, F&& f)
     return Lf.m / 8 < kV4SmallRows ? cls(IntC<kV4GroupSmallOf<T>>{}) : cls(IntC<kV4GroupLarge>{});
 }
 
-// TMA maps of one FP32 vector of a level: map[u][d] covers colour u's brick
-// with the box a launching colour sees when its parity differs from u's by d.
+// TMA maps of one vector of a level: map[u][d] covers colour u's brick with
+// the box a launching colour sees when its parity differs from u's by d.
 struct SweepMaps
 {
-    const float* x = nullptr;
-    int m = 0, nx = 0, ny = 0, nz = 0;
+    const void* x = nullptr;
+    int esize = 0, m = 0, nx = 0, ny = 0, nz = 0;
     CUtensorMap map[8][8];
 };
 
-static int encode_brick_map(CUtensorMap* map, const float* base, int bx, int by, int bz, int boxx, int boxy, int boxz)
+static int encode_brick_map(CUtensorMap* map, const void* base, int esize, int bx, int by, int bz, int boxx, int boxy,
+                            int boxz)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if(!encode)
@@ -1912,27 +1950,32 @@ static int encode_brick_map(CUtensorMap* map, const float* base, int bx, int by,
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
     const cuuint64_t dims[3] = {(cuuint64_t)bx, (cuuint64_t)by, (cuuint64_t)bz};
-    const cuuint64_t strides[2] = {(cuuint64_t)bx * 4, (cuuint64_t)bx * by * 4};
+    const cuuint64_t strides[2] = {(cuuint64_t)bx * esize, (cuuint64_t)bx * by * esize};
     const cuuint32_t box[3] = {(cuuint32_t)boxx, (cuuint32_t)boxy, (cuuint32_t)boxz};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
-                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = encode(map, esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                              const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if(r != CUDA_SUCCESS) return record_error(HPCGB200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return 0;
 }
 
 // Maps of x on level L, built once per (vector, level) and kept (a V-cycle
 // sweeps the same few vectors).
-static const SweepMaps* sweep_maps(const StencilLevel& L, const float* x)
+template <typename T>
+static const SweepMaps* sweep_maps(const StencilLevel& L, const T* x)
 {
     static std::mutex mu;
     static std::vector<std::unique_ptr<SweepMaps>> cache;
     std::lock_guard<std::mutex> lock(mu);
+    const int es = (int)sizeof(T);
     for(const auto& e : cache)
-        if(e->x == x && e->m == L.m && e->nx == L.nx && e->ny == L.ny && e->nz == L.nz) return e.get();
+        if(e->x == x && e->esize == es && e->m == L.m && e->nx == L.nx && e->ny == L.ny && e->nz == L.nz)
+            return e.get();
     auto e = std::make_unique<SweepMaps>();
     e->x = x;
+    e->esize = es;
     e->m = L.m;
     e->nx = L.nx;
     e->ny = L.ny;
@@ -1941,8 +1984,8 @@ static const SweepMaps* sweep_maps(const StencilLevel& L, const float* x)
     {
         const int bz = (L.nz - (L.par[u] & 1) + 1) / 2;
         for(int d = 1; d < 8; ++d)
-            if(encode_brick_map(&e->map[u][d], x + L.offsets[u], L.bx[u], L.by[u], bz, kTmaX + 4 * ((d >> 2) & 1),
-                                kTmaY + ((d >> 1) & 1), kTmaZ + (d & 1)))
+            if(encode_brick_map(&e->map[u][d], x + L.offsets[u], es, L.bx[u], L.by[u], bz, kTmaX + 4 * ((d >> 2) & 1),
+                                kTmaYOf<T> + ((d >> 1) & 1), kTmaZ + (d & 1)))
                 return nullptr;
     }
     if(cache.size() >= 64) cache.erase(cache.begin());
@@ -1963,38 +2006,39 @@ static bool sweep_tma_enabled()
 
 // Large even level with the canonical colouring, x 16-byte aligned, no fused
 // prolongation: the TMA-staged passes apply.
-static bool pass_tma_ok(const StencilLevel& L, const float* x, const Prolong<float>& pro)
+template <typename T>
+static bool pass_tma_ok(const StencilLevel& L, const T* x, const Prolong<T>& pro)
 {
     return sweep_tma_enabled() && vec4_ok(L) && L.canon && L.m / 8 >= kV4SmallRows && !pro.xf &&
            (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
 }
 
-template <int C, int K, bool D>
+template <typename T, int C, int K, bool D>
 static cudaError_t launch_pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M,
-                                   const float* inv_diag32, const float* diag32, const double* r64, float* r, float* x,
-                                   double* z64, const int* inj_c, float* rc, cudaStream_t s)
+                                   const T* inv_diag, const T* diag, const double* r64, T* r, T* x, double* z64,
+                                   const int* inj_c, T* rc, cudaStream_t s)
 {
     NbMaps nb;
     for(int u = 0, i = 0; u < 8; ++u)
         if(tma_reads(K, c.v, u)) nb.m[i++] = M.map[u][L.par[c.v] ^ L.par[u]];
-    const dim3 grid((unsigned)((c.bx + kTmaX - 1) / kTmaX), (unsigned)((c.by + kTmaY - 1) / kTmaY),
+    const dim3 grid((unsigned)((c.bx + kTmaX - 1) / kTmaX), (unsigned)((c.by + kTmaYOf<T> - 1) / kTmaYOf<T>),
                     (unsigned)((c.bz + kTmaZ - 1) / kTmaZ));
-    const size_t smem = (size_t)TmaTab<C, K>::p.total * 4 + 128;
-    return launch_pdl_smem(kv_pass_tma<C, K, D>, grid, dim3(kTmaX / 4, kTmaY, kTmaZ), smem, s, nb, c, inv_diag32,
-                           diag32, r64, r, x, z64, inj_c, rc, L.status);
+    const size_t smem = (size_t)TmaTab<T, C, K>::p.total * sizeof(T) + 128;
+    return launch_pdl_smem(kv_pass_tma<T, C, K, D>, grid, dim3(kTmaX / 4, kTmaYOf<T>, kTmaZ), smem, s, nb, c,
+                           inv_diag, diag, r64, r, x, z64, inj_c, rc, L.status);
 }
 
 // One TMA-staged pass of kind K over colour c (canonical colouring: the
 // class is a compile-time constant).
-template <int K, bool D>
-static cudaError_t pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M, const float* inv_diag32,
-                            const float* diag32, const double* r64, float* r, float* x, double* z64, cudaStream_t s,
-                            const int* inj_c = nullptr, float* rc = nullptr)
+template <typename T, int K, bool D = false>
+static cudaError_t pass_tma(const StencilLevel& L, const ColorLaunch& c, const SweepMaps& M, const T* inv_diag,
+                            const T* diag, const double* r64, T* r, T* x, double* z64, cudaStream_t s,
+                            const int* inj_c = nullptr, T* rc = nullptr)
 {
     return by_class(L, c.par, [&](auto kc) {
         constexpr int C = decltype(kc)::value;
         if constexpr(C < 0) return cudaErrorInvalidValue;  // L.canon holds on this path
-        else return launch_pass_tma<C, K, D>(L, c, M, inv_diag32, diag32, r64, r, x, z64, inj_c, rc, s);
+        else return launch_pass_tma<T, C, K, D>(L, c, M, inv_diag, diag, r64, r, x, z64, inj_c, rc, s);
     });
 }
 
@@ -2017,8 +2061,8 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         const Prolong<float> pv = v == n - 1 ? pro : Prolong<float>{};
         if(maps)
         {
-            HB_CUDA((r64 ? pass_tma<kTmaFwd0, true>(L, c, *maps, inv_diag32, nullptr, r64, r32, x, nullptr, s)
-                         : pass_tma<kTmaFwd0, false>(L, c, *maps, inv_diag32, nullptr, nullptr, r32, x, nullptr, s)));
+            HB_CUDA((r64 ? pass_tma<float, kTmaFwd0, true>(L, c, *maps, inv_diag32, nullptr, r64, r32, x, nullptr, s)
+                         : pass_tma<float, kTmaFwd0>(L, c, *maps, inv_diag32, nullptr, nullptr, r32, x, nullptr, s)));
         }
         else if(vec)
         {
@@ -2048,7 +2092,7 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
         const ColorLaunch c = color_launch(L, v);
         if(maps)
         {
-            HB_CUDA((pass_tma<kTmaBwd0, false>(L, c, *maps, inv_diag32, diag32, nullptr, nullptr, x, nullptr, s)));
+            HB_CUDA((pass_tma<float, kTmaBwd0>(L, c, *maps, inv_diag32, diag32, nullptr, nullptr, x, nullptr, s)));
         }
         else if(vec)
         {
@@ -2076,8 +2120,8 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
         if(maps)
-            HB_CUDA((pass_tma<kTmaSweep, false>(L, c, *maps, inv_diag32, nullptr, nullptr, const_cast<float*>(r), x,
-                                                z, s)));
+            HB_CUDA((pass_tma<float, kTmaSweep>(L, c, *maps, inv_diag32, nullptr, nullptr, const_cast<float*>(r), x, z,
+                                                s)));
         else if(vec)
         {
             HB_CUDA(by_shape<float>(L, c, [&](auto kg, auto kc) {
@@ -2106,7 +2150,7 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
     const SweepMaps* maps = pass_tma_ok(Lf, xf, {}) && nc == c.bx * c.by * c.bz ? sweep_maps(Lf, xf) : nullptr;
     if(maps)
     {
-        HB_CUDA((pass_tma<kTmaRestrict, false>(Lf, c, *maps, nullptr, diag32, nullptr, const_cast<float*>(rf),
+        HB_CUDA((pass_tma<float, kTmaRestrict>(Lf, c, *maps, nullptr, diag32, nullptr, const_cast<float*>(rf),
                                                 const_cast<float*>(xf), nullptr, s, inj_c, rc)));
     }
     else if(vec4_ok(Lf) && nc == c.bx * c.by * c.bz)
@@ -2149,11 +2193,19 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
     const dim3 t4(kV4X, kV4Y);
+    const SweepMaps* maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
+    if(pass_tma_ok(L, x, pro) && !maps) return HPCGB200_ERR_CUDA;
     for(int v = 0; v < L.ncolors; ++v)
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
         const Prolong<double> pv = v == L.ncolors - 1 ? pro : Prolong<double>{};
+        if(maps)
+        {
+            HB_CUDA((pass_tma<double, kTmaFwd0>(L, c, *maps, inv_diag, nullptr, nullptr, const_cast<double*>(r), x,
+                                                nullptr, s)));
+            continue;
+        }
         HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
             constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
             return launch_pdl(kv_fwd0<double, false, G, C>, brick_grid4(c), t4, s, c, L, inv_diag, nullptr,
@@ -2164,6 +2216,11 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
     {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) continue;
         const ColorLaunch c = color_launch(L, v);
+        if(maps)
+        {
+            HB_CUDA((pass_tma<double, kTmaBwd0>(L, c, *maps, inv_diag, diag, nullptr, nullptr, x, nullptr, s)));
+            continue;
+        }
         HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
             constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
             return launch_pdl(kv_bwd0<double, G, C>, brick_grid4(c), t4, s, c, L, diag, inv_diag, x, pro);
@@ -2176,9 +2233,17 @@ int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double*
                     Prolong<double> pro)
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
+    const SweepMaps* maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
+    if(pass_tma_ok(L, x, pro) && !maps) return HPCGB200_ERR_CUDA;
     auto sweep = [&](int v, Prolong<double> pv) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
         const ColorLaunch c = color_launch(L, v);
+        if(maps)
+        {
+            HB_CUDA((pass_tma<double, kTmaSweep>(L, c, *maps, inv_diag, nullptr, nullptr, const_cast<double*>(r), x,
+                                                 nullptr, s)));
+            return 0;
+        }
         HB_CUDA(by_shape<double>(L, c, [&](auto kg, auto kc) {
             constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
             return launch_pdl(kv_sweep<double, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, L, inv_diag, r, x,
@@ -2197,6 +2262,14 @@ int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const d
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
     if(!vec4_ok(Lf) || nc != c.bx * c.by * c.bz)
         return record_error(HPCGB200_ERR_ARG, "FP64 stencil restriction: colour bricks not 4-aligned");
+    if(pass_tma_ok(Lf, xf, Prolong<double>{}))
+    {
+        const SweepMaps* maps = sweep_maps(Lf, xf);
+        if(!maps) return HPCGB200_ERR_CUDA;
+        HB_CUDA((pass_tma<double, kTmaRestrict>(Lf, c, *maps, nullptr, diag, nullptr, const_cast<double*>(rf),
+                                                 const_cast<double*>(xf), nullptr, s, inj_c, rc)));
+        return 0;
+    }
     HB_CUDA(by_shape_restrict<double>(Lf, [&](auto kg, auto kc) {
         constexpr int G = decltype(kg)::value, C = decltype(kc)::value;
         return launch_pdl(kv_restrict<double, G, C>, brick_grid4(c), dim3(kV4X, kV4Y), s, c, Lf, inj_c, diag, rf, xf,
