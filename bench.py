@@ -72,7 +72,7 @@ def parse():
                     help="solves only: no e2e, operator timing, CPU baseline (profiling runs)")
     ap.add_argument("--mixed-only", action="store_true", help="only the mixed-vs-FP64 comparison")
     ap.add_argument("--profile-case", choices=["conv", "sweep128", "spmv128", "mixed128", "mixed192", "cg128",
-                                               "cgmixed192", "vcycle256", "mixed320", "net64"],
+                                               "cgmixed192", "vcycle256", "mixed320", "net64", "stencil192"],
                     help="run one small case for a profiler and exit (no JSON line)")
     ap.add_argument("--no-largest", action="store_true",
                     help="skip the largest workload (560x560x280, FP64 vs mixed vs learned, seed-7 and all-ones rhs)")
@@ -879,6 +879,10 @@ def run_profile_case(case: str) -> int:
             y = S.forward(r, (64, 64, 64), 1)
         torch.cuda.synchronize()
         print(json.dumps({"net64_norm": float(y.norm())}))
+    elif case == "stencil192":
+        # the FP64 stencil V-cycle at 192^3 (eager launches; its level-0 passes are the TMA-staged double kernels)
+        P = R.Problem(192)
+        print(json.dumps({"mg_stencil_ms": P.time_op("mg_stencil", 1)}))
     elif case == "mixed320":
         # one mixed V-cycle + one stencil SpMV at 320^3 (eager launches)
         P = R.Problem(320)
