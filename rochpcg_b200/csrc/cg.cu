@@ -72,19 +72,35 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_rtz(int n, const double* 
     }
 }
 
+// p = z (k == 1) or z + beta p; first, for k > 1, the previous iteration's
+// x += alpha p (src/CG.cpp:174), deferred to this pass, which reads that p
+// anyway (launch_cg_x_final applies the last one after the loop).
 template <typename Z>
 __global__ void __launch_bounds__(kBS) k_cg_update_p(int n, const Z* __restrict__ z, double* __restrict__ p,
-                                                     const CGState* __restrict__ st)
+                                                     double* __restrict__ x, const CGState* __restrict__ st)
 {
     const int i = blockIdx.x * kBS + threadIdx.x;
     if(i >= n) return;
     // first iteration, and the first one after the learned smoother fell
     // back: p = z (a restart: the old directions belong to the other
     // preconditioner)
-    const bool restart = st->k == 1 || (st->fallback_iter > 0 && st->k == st->fallback_iter + 1);
+    const int k = st->k;
+    const bool restart = k == 1 || (st->fallback_iter > 0 && k == st->fallback_iter + 1);
     const double zi = (double)z[i];
+    const double po = k > 1 ? p[i] : 0.0;
+    if(k > 1) x[i] = fma(st->alpha, po, x[i]);     // WAXPBY(1, x, alpha, p) of iteration k-1
     if(restart) p[i] = fma(0.0, zi, zi);            // WAXPBY(1, z, 0, z)
-    else p[i] = fma(st->beta, p[i], zi);           // WAXPBY(1, z, beta, p)
+    else p[i] = fma(st->beta, po, zi);             // WAXPBY(1, z, beta, p)
+}
+
+// The last iteration's x += alpha p (the deferred update of k_cg_update_p),
+// when the solve ran at least one iteration since its preamble.
+__global__ void __launch_bounds__(kBS) k_cg_x_final(int n, const double* __restrict__ p, double* __restrict__ x,
+                                                    const CGState* __restrict__ st)
+{
+    const int i = blockIdx.x * kBS + threadIdx.x;
+    if(i >= n || st->k <= 1) return;
+    x[i] = fma(st->alpha, p[i], x[i]);
 }
 
 // Ap = A p (one row per thread, colour-interleaved blocks as k_spmv) and
@@ -159,12 +175,11 @@ __global__ void __launch_bounds__(kBS) k_cg_pap_chunks(ColorChunks cc, const dou
     }
 }
 
+// r -= alpha Ap and ||r|| (x += alpha p runs in the next p update).
 template <typename Z>
-__global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const double* __restrict__ p,
-                                                                 const double* __restrict__ Ap,
-                                                                 double* __restrict__ r, double* __restrict__ x,
-                                                                 const Z* __restrict__ z, CGState* st,
-                                                                 ReduceScratch* ws)
+__global__ void __launch_bounds__(kReduceThreads) k_cg_update_r(int n, const double* __restrict__ Ap,
+                                                                double* __restrict__ r, const Z* __restrict__ z,
+                                                                CGState* st, ReduceScratch* ws)
 {
     __shared__ double red[32];
     const double alpha = st->alpha;
@@ -175,7 +190,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_update_xr(int n, const do
         const double v = fma(-alpha, Ap[i], r[i]);   // ComputeFusedWAXPBYDot(-alpha, Ap, r)
         r[i] = v;
         s = fma(v, v, s);
-        x[i] = fma(alpha, p[i], x[i]);               // WAXPBY(1, x, alpha, p)
         if(flex) sf = fma((double)z[i], v, sf);
     }
     double t1, t2;
@@ -263,10 +277,10 @@ template <typename Z>
 __global__ void __launch_bounds__(kBS) k_cg_step1_ell(int n, ColorChunks cc, const int* __restrict__ ell_col,
                                                       const double* __restrict__ ell_val, const double* __restrict__ r,
                                                       const Z* __restrict__ z, double* __restrict__ p,
-                                                      double* __restrict__ Ap, CGState* st, double* partial,
-                                                      unsigned int* ticket, GridBarrier* gb)
+                                                      double* __restrict__ x, double* __restrict__ Ap, CGState* st,
+                                                      double* partial, unsigned int* ticket, GridBarrier* gb)
 {
-    if(!step1_rz_p(n, r, z, p, st, partial, gb)) return;
+    if(!step1_rz_p(n, r, z, p, x, st, partial, gb)) return;
     double s = 0.0;
     for(int c = blockIdx.x; c < cc.nchunks(); c += gridDim.x)
     {
@@ -279,11 +293,10 @@ __global__ void __launch_bounds__(kBS) k_cg_step1_ell(int n, ColorChunks cc, con
     step1_alpha(s, st, partial, ticket);
 }
 
-// Step 2: the r/x update of k_cg_update_xr with the loop control in its last block.
+// Step 2: the r update of k_cg_update_r with the loop control in its last block.
 template <typename Z>
-__global__ void __launch_bounds__(kReduceThreads) k_cg_step2(int n, const double* __restrict__ p,
-                                                             const double* __restrict__ Ap, double* __restrict__ r,
-                                                             double* __restrict__ x, const Z* __restrict__ z,
+__global__ void __launch_bounds__(kReduceThreads) k_cg_step2(int n, const double* __restrict__ Ap,
+                                                             double* __restrict__ r, const Z* __restrict__ z,
                                                              CGState* st, ReduceScratch* ws, unsigned long long cond,
                                                              int watch_net)
 {
@@ -296,7 +309,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_cg_step2(int n, const double
         const double v = fma(-alpha, Ap[i], r[i]);
         r[i] = v;
         s = fma(v, v, s);
-        x[i] = fma(alpha, p[i], x[i]);
         if(flex) sf = fma((double)z[i], v, sf);
     }
     double t1, t2;
@@ -369,16 +381,23 @@ int launch_cg_rtz(int n, const double* r, const float* z, CGState* st, ReduceScr
     return rtz_impl(n, r, z, st, ws, s);
 }
 
-int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s)
+int launch_cg_update_p(int n, const double* z, double* p, double* x, const CGState* st, cudaStream_t s)
 {
-    k_cg_update_p<double><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
+    k_cg_update_p<double><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, x, st);
     HB_LAUNCHED();
     return 0;
 }
 
-int launch_cg_update_p(int n, const float* z, double* p, const CGState* st, cudaStream_t s)
+int launch_cg_update_p(int n, const float* z, double* p, double* x, const CGState* st, cudaStream_t s)
 {
-    k_cg_update_p<float><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, st);
+    k_cg_update_p<float><<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, z, p, x, st);
+    HB_LAUNCHED();
+    return 0;
+}
+
+int launch_cg_x_final(int n, const double* p, double* x, const CGState* st, cudaStream_t s)
+{
+    k_cg_x_final<<<(n + kBS - 1) / kBS, kBS, 0, s>>>(n, p, x, st);
     HB_LAUNCHED();
     return 0;
 }
@@ -401,67 +420,67 @@ int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const do
 }
 
 template <typename Z>
-static int update_xr_impl(int n, const double* p, const double* Ap, double* r, double* x, const Z* z, CGState* st,
-                          ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+static int update_r_impl(int n, const double* Ap, double* r, const Z* z, CGState* st, ReduceScratch* ws,
+                         unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    k_cg_update_xr<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws);
+    k_cg_update_r<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, Ap, r, z, st, ws);
     HB_LAUNCHED();
     k_cg_loop_control<<<1, 1, 0, s>>>(st, cond, watch_net);
     HB_LAUNCHED();
     return 0;
 }
 
-int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+int launch_cg_update_r(int n, const double* Ap, double* r, const double* z, CGState* st, ReduceScratch* ws,
+                       unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    return update_xr_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+    return update_r_impl(n, Ap, r, z, st, ws, cond, watch_net, s);
 }
 
-int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const float* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+int launch_cg_update_r(int n, const double* Ap, double* r, const float* z, CGState* st, ReduceScratch* ws,
+                       unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    return update_xr_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+    return update_r_impl(n, Ap, r, z, st, ws, cond, watch_net, s);
 }
 
 // ---- two-kernel CG step
 template <typename Z>
 static int step1_ell_impl(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
-                          const Z* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
-                          cudaStream_t s)
+                          const Z* z, double* p, double* x, double* Ap, CGState* st, ReduceScratch* ws,
+                          GridBarrier* gb, cudaStream_t s)
 {
     static const int grid = resident_grid(k_cg_step1_ell<Z>, kBS, kReduceBlocks);
     if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "CG step: no resident grid");
-    HB_CUDA(launch_coop(k_cg_step1_ell<Z>, grid, kBS, s, n, cc, ell_col, ell_val, r, z, p, Ap, st, ws->partial,
+    HB_CUDA(launch_coop(k_cg_step1_ell<Z>, grid, kBS, s, n, cc, ell_col, ell_val, r, z, p, x, Ap, st, ws->partial,
                         &ws->ticket, gb));
     return 0;
 }
 
 int launch_cg_step1_ell(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
-                        const double* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
-                        cudaStream_t s)
+                        const double* z, double* p, double* x, double* Ap, CGState* st, ReduceScratch* ws,
+                        GridBarrier* gb, cudaStream_t s)
 {
-    return step1_ell_impl(n, cc, ell_col, ell_val, r, z, p, Ap, st, ws, gb, s);
+    return step1_ell_impl(n, cc, ell_col, ell_val, r, z, p, x, Ap, st, ws, gb, s);
 }
 
 template <typename Z>
-static int step2_impl(int n, const double* p, const double* Ap, double* r, double* x, const Z* z, CGState* st,
-                      ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+static int step2_impl(int n, const double* Ap, double* r, const Z* z, CGState* st, ReduceScratch* ws,
+                      unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    k_cg_step2<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, Ap, r, x, z, st, ws, cond, watch_net);
+    k_cg_step2<Z><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, Ap, r, z, st, ws, cond, watch_net);
     HB_LAUNCHED();
     return 0;
 }
 
-int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const double* z, CGState* st,
-                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+int launch_cg_step2(int n, const double* Ap, double* r, const double* z, CGState* st, ReduceScratch* ws,
+                    unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    return step2_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+    return step2_impl(n, Ap, r, z, st, ws, cond, watch_net, s);
 }
 
-int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const float* z, CGState* st,
-                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s)
+int launch_cg_step2(int n, const double* Ap, double* r, const float* z, CGState* st, ReduceScratch* ws,
+                    unsigned long long cond, int watch_net, cudaStream_t s)
 {
-    return step2_impl(n, p, Ap, r, x, z, st, ws, cond, watch_net, s);
+    return step2_impl(n, Ap, r, z, st, ws, cond, watch_net, s);
 }
 
 int launch_cg_timer(CGState* st, int phase, cudaStream_t s)

@@ -51,7 +51,8 @@ __device__ __forceinline__ void step_rows(long long n, long long& lo, long long&
 // when a barrier timed out.
 template <typename Z>
 __device__ __forceinline__ bool step1_rz_p(long long n, const double* __restrict__ r, const Z* __restrict__ z,
-                                           double* __restrict__ p, CGState* st, double* partial, GridBarrier* gb)
+                                           double* __restrict__ p, double* __restrict__ x, CGState* st,
+                                           double* partial, GridBarrier* gb)
 {
     __shared__ double red[32];
     __shared__ double sh_beta;
@@ -60,7 +61,7 @@ __device__ __forceinline__ bool step1_rz_p(long long n, const double* __restrict
     step_rows(n, lo, hi);
     const int k = st->k;
     const bool restart = k == 1 || (st->fallback_iter > 0 && k == st->fallback_iter + 1);
-    const double old_rtz = st->rtz, rtz_flex = st->rtz_flex;
+    const double old_rtz = st->rtz, rtz_flex = st->rtz_flex, alpha_prev = st->alpha;
     const bool flex = st->flexible != 0;
     double s = 0.0;
     for(long long i = lo + tid; i < hi; i += blockDim.x) s = fma((double)z[i], r[i], s);
@@ -86,7 +87,9 @@ __device__ __forceinline__ bool step1_rz_p(long long n, const double* __restrict
     for(long long i = lo + tid; i < hi; i += blockDim.x)
     {
         const double zi = (double)z[i];
-        __stcg(p + i, restart ? fma(0.0, zi, zi) : fma(beta, __ldcg(p + i), zi));
+        const double po = k > 1 ? __ldcg(p + i) : 0.0;
+        if(k > 1) x[i] = fma(alpha_prev, po, x[i]);  // iteration k-1's x += alpha p, deferred
+        __stcg(p + i, restart ? fma(0.0, zi, zi) : fma(beta, po, zi));
     }
     return grid_barrier(gb, gridDim.x, &st->status);
 }
@@ -146,9 +149,13 @@ int launch_cg_residual0(int n, const double* b, const double* Ap, double* r, CGS
 // the FP32 V-cycles' output directly (every value widened exactly).
 int launch_cg_rtz(int n, const double* r, const double* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
 int launch_cg_rtz(int n, const double* r, const float* z, CGState* st, ReduceScratch* ws, cudaStream_t s);
-// p = z (k == 1) or p = z + beta p.
-int launch_cg_update_p(int n, const double* z, double* p, const CGState* st, cudaStream_t s);
-int launch_cg_update_p(int n, const float* z, double* p, const CGState* st, cudaStream_t s);
+// p = z (k == 1) or p = z + beta p; for k > 1 first the previous iteration's
+// x += alpha p (deferred from the r update to this pass, which reads that p
+// anyway: one read of p per iteration fewer).  launch_cg_x_final applies the
+// last iteration's update after the loop.
+int launch_cg_update_p(int n, const double* z, double* p, double* x, const CGState* st, cudaStream_t s);
+int launch_cg_update_p(int n, const float* z, double* p, double* x, const CGState* st, cudaStream_t s);
+int launch_cg_x_final(int n, const double* p, double* x, const CGState* st, cudaStream_t s);
 // Ap = A p and alpha = rtz / (p.Ap); `partial` holds cc.nchunks() per-block
 // sums, `ticket` must start at zero and is left at zero.
 int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* p,
@@ -158,30 +165,30 @@ int launch_cg_spmv_pap(int m, const ColorChunks& cc, const int* ell_col, const d
 // so a solve whose SpMV runs elsewhere keeps the ELL solve's scalars bit for bit.
 int launch_cg_pap_chunks(int m, const ColorChunks& cc, const double* p, const double* Ap, CGState* st,
                          double* partial, unsigned int* ticket, cudaStream_t s);
-// r -= alpha Ap, normr = ||r||, x += alpha p, history; then (own 1-thread
-// kernel) k++ and the loop condition (k <= max_iter && normr/normr0 > tol)
-// written to `cond` (a graph conditional handle; 0 = none).  While the
-// learned smoother is active (net == 1) an iteration that does not reduce
-// normr marks it failed (net = 2); with watch_net the loop then also ends.
-int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const double* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
-int launch_cg_update_xr(int n, const double* p, const double* Ap, double* r, double* x, const float* z,
-                        CGState* st, ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+// r -= alpha Ap, normr = ||r||, history; then (own 1-thread kernel) k++ and
+// the loop condition (k <= max_iter && normr/normr0 > tol) written to `cond`
+// (a graph conditional handle; 0 = none).  While the learned smoother is
+// active (net == 1) an iteration that does not reduce normr marks it failed
+// (net = 2); with watch_net the loop then also ends.
+int launch_cg_update_r(int n, const double* Ap, double* r, const double* z, CGState* st, ReduceScratch* ws,
+                       unsigned long long cond, int watch_net, cudaStream_t s);
+int launch_cg_update_r(int n, const double* Ap, double* r, const float* z, CGState* st, ReduceScratch* ws,
+                       unsigned long long cond, int watch_net, cudaStream_t s);
 
 // Two-kernel CG step (src/CG.cpp:148-184).  Step 1 (persistent, cooperative,
-// two bounded grid barriers): rtz = r.z and beta, p = z + beta p, Ap = A p
-// with pAp and alpha; it uses ws's partials and ticket (left at zero) and the
-// grid barrier gb (count zero before the launch, left at zero).  Step 2:
-// r -= alpha Ap, x += alpha p, normr, then the loop control (as
-// launch_cg_update_xr, in one kernel).  A barrier that times out sets
-// st->status.
+// two bounded grid barriers): rtz = r.z and beta, the previous iteration's
+// x += alpha p and p = z + beta p (as launch_cg_update_p), Ap = A p with pAp
+// and alpha; it uses ws's partials and ticket (left at zero) and the grid
+// barrier gb (count zero before the launch, left at zero).  Step 2:
+// r -= alpha Ap, normr, then the loop control (as launch_cg_update_r, in one
+// kernel).  A barrier that times out sets st->status.
 int launch_cg_step1_ell(int n, const ColorChunks& cc, const int* ell_col, const double* ell_val, const double* r,
-                        const double* z, double* p, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb,
-                        cudaStream_t s);
-int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const double* z, CGState* st,
-                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
-int launch_cg_step2(int n, const double* p, const double* Ap, double* r, double* x, const float* z, CGState* st,
-                    ReduceScratch* ws, unsigned long long cond, int watch_net, cudaStream_t s);
+                        const double* z, double* p, double* x, double* Ap, CGState* st, ReduceScratch* ws,
+                        GridBarrier* gb, cudaStream_t s);
+int launch_cg_step2(int n, const double* Ap, double* r, const double* z, CGState* st, ReduceScratch* ws,
+                    unsigned long long cond, int watch_net, cudaStream_t s);
+int launch_cg_step2(int n, const double* Ap, double* r, const float* z, CGState* st, ReduceScratch* ws,
+                    unsigned long long cond, int watch_net, cudaStream_t s);
 
 // One thread: adds the time since the previous stamp to phase_ns[phase]
 // (phase kPhaseStart only stamps).  Kernels on one stream run in order, so

@@ -1785,11 +1785,11 @@ __global__ void __launch_bounds__(kMThreads) k64_spmv_sep(const StencilLevel L, 
 template <typename Z>
 __global__ void __launch_bounds__(kMThreads) k_cg_step1_sep(const StencilLevel L, const double* __restrict__ diag,
                                                             const double* __restrict__ r, const Z* __restrict__ z,
-                                                            double* __restrict__ p, double* __restrict__ Ap,
-                                                            CGState* st, double* partial, unsigned int* ticket,
-                                                            GridBarrier* gb)
+                                                            double* __restrict__ p, double* __restrict__ x,
+                                                            double* __restrict__ Ap, CGState* st, double* partial,
+                                                            unsigned int* ticket, GridBarrier* gb)
 {
-    if(!step1_rz_p(L.m, r, z, p, st, partial, gb)) return;
+    if(!step1_rz_p(L.m, r, z, p, x, st, partial, gb)) return;
     const int tx = (L.nx + kMX - 1) / kMX, ty = (L.ny + kMY - 1) / kMY, tz = (L.nz + kSZ - 1) / kSZ;
     const int ntiles = tx * ty * tz;
     double s = 0.0;
@@ -2332,12 +2332,12 @@ int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x
 }
 
 int launch_cg_step1_sep(const StencilLevel& L, const double* diag, const double* r, const float* z, double* p,
-                        double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s)
+                        double* x, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s)
 {
     if(!canonical_colours(L)) return record_error(HPCGB200_ERR_ARG, "CG step: the level is not canonically coloured");
     static const int grid = resident_grid(k_cg_step1_sep<float>, kMThreads, kReduceBlocks);
     if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "CG step: no resident grid");
-    HB_CUDA(launch_coop(k_cg_step1_sep<float>, grid, kMThreads, s, L, diag, r, z, p, Ap, st, ws->partial,
+    HB_CUDA(launch_coop(k_cg_step1_sep<float>, grid, kMThreads, s, L, diag, r, z, p, x, Ap, st, ws->partial,
                         &ws->ticket, gb));
     return 0;
 }

@@ -107,7 +107,7 @@ size_t stencil_pap_partials(const StencilLevel& L);
 // Step 1 of the two-kernel CG step (launch_cg_step1_ell) with the separable
 // product, for the FP32 V-cycles' output z; canonical colouring only.
 int launch_cg_step1_sep(const StencilLevel& L, const double* diag, const double* r, const float* z, double* p,
-                        double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s);
+                        double* x, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s);
 int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, const double* p, double* Ap,
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s);
 

@@ -91,22 +91,21 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
     {
         LevelOpt* o = opt(A);
         if(z32)
-            HB_RETURN_IF(hb::launch_cg_step1_sep(o->st, o->diag, data.r.d_values, z32, data.p.d_values,
+            HB_RETURN_IF(hb::launch_cg_step1_sep(o->st, o->diag, data.r.d_values, z32, data.p.d_values, x.d_values,
                                                  data.Ap.d_values, st, rt().ws, o->step_barrier, s));
         else
             HB_RETURN_IF(hb::launch_cg_step1_ell(n, o->cc, A.ell_col_ind, A.ell_val, data.r.d_values,
-                                                 data.z.d_values, data.p.d_values, data.Ap.d_values, st, rt().ws,
-                                                 o->step_barrier, s));
-        return z32 ? hb::launch_cg_step2(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values, z32, st,
-                                         rt().ws, cond, watch, s)
-                   : hb::launch_cg_step2(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
-                                         data.z.d_values, st, rt().ws, cond, watch, s);
+                                                 data.z.d_values, data.p.d_values, x.d_values, data.Ap.d_values, st,
+                                                 rt().ws, o->step_barrier, s));
+        return z32 ? hb::launch_cg_step2(n, data.Ap.d_values, data.r.d_values, z32, st, rt().ws, cond, watch, s)
+                   : hb::launch_cg_step2(n, data.Ap.d_values, data.r.d_values, data.z.d_values, st, rt().ws, cond,
+                                         watch, s);
     }
     HB_RETURN_IF(z32 ? hb::launch_cg_rtz(n, data.r.d_values, z32, st, rt().ws, s)
                      : hb::launch_cg_rtz(n, data.r.d_values, data.z.d_values, st, rt().ws, s));
     HB_RETURN_IF(stamp(hb::kPhaseDot));
-    HB_RETURN_IF(z32 ? hb::launch_cg_update_p(n, z32, data.p.d_values, st, s)
-                     : hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, st, s));
+    HB_RETURN_IF(z32 ? hb::launch_cg_update_p(n, z32, data.p.d_values, x.d_values, st, s)
+                     : hb::launch_cg_update_p(n, data.z.d_values, data.p.d_values, x.d_values, st, s));
     HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
     if(prec == MGPrecision::FP64_STENCIL)
     {
@@ -131,11 +130,10 @@ static int capture_body(const SparseMatrix& A, CGData& data, Vector& x, bool pre
                                             o->spmv_partial, o->spmv_ticket, s));
     }
     HB_RETURN_IF(stamp(hb::kPhaseSpmv));
-    HB_RETURN_IF(z32 ? hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values, z32,
-                                               st, rt().ws, cond, watch, s)
-                     : hb::launch_cg_update_xr(n, data.p.d_values, data.Ap.d_values, data.r.d_values, x.d_values,
-                                               data.z.d_values, st, rt().ws, cond, watch, s));
-    // (the r/x update kernel launches the loop control after itself; its
+    HB_RETURN_IF(z32 ? hb::launch_cg_update_r(n, data.Ap.d_values, data.r.d_values, z32, st, rt().ws, cond, watch, s)
+                     : hb::launch_cg_update_r(n, data.Ap.d_values, data.r.d_values, data.z.d_values, st, rt().ws,
+                                              cond, watch, s));
+    // (the r update kernel launches the loop control after itself; its
     // stamp below also covers that one-thread kernel)
     HB_RETURN_IF(stamp(hb::kPhaseWaxpby));
     return 0;
@@ -400,6 +398,9 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
                 if(left < 1) break;
             }
         }
+        // the last iteration's x += alpha p (each iteration's update runs in
+        // the next iteration's p update)
+        check(hb::launch_cg_x_final(n, data.p.d_values, x.d_values, st, s));
         HB_HOST_CUDA(cudaEventRecord(e1, s));
         HB_HOST_CUDA(cudaMemcpyAsync(&h, st, offsetof(hb::CGState, hist), cudaMemcpyDeviceToHost, s));
         HB_HOST_CUDA(cudaStreamSynchronize(s));
