@@ -91,6 +91,8 @@ __device__ __forceinline__ bool step1_rz_p(long long n, const double* __restrict
         if(k > 1) x[i] = fma(alpha_prev, po, x[i]);  // iteration k-1's x += alpha p, deferred
         __stcg(p + i, restart ? fma(0.0, zi, zi) : fma(beta, po, zi));
     }
+    // the product after the next barrier may read p through TMA (the async proxy)
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     return grid_barrier(gb, gridDim.x, &st->status);
 }
 

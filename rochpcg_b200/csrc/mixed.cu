@@ -1631,34 +1631,74 @@ __device__ __forceinline__ void cp_async_wait()
 // with the diagonal staged too, measured 0.234 against 0.221 ms at 320^3.)
 constexpr int kSepRing = 4, kSepAhead = 3;
 
+// TMA staging of the planes (even grids with 4-aligned colour bricks): one
+// tiled box per colour brick of the plane's z parity, 36 x 3 x 1 doubles, so
+// a plane is four boxes issued by one thread and completing on the ring
+// slot's mbarrier instead of 396 eight-byte copies.  Shared layout: block
+// (py, px) of 3 lines x 36, the x-odd lines shifted by one (their box starts
+// two brick columns left of the tile: a box starts on 16 bytes); blocks are
+// padded to 112 doubles so that every box lands on a 128-byte boundary.
+constexpr int kSepTmaLine = 36, kSepTmaBlock = 112, kSepTmaPlane = 4 * kSepTmaBlock;
+constexpr unsigned kSepTmaBytes = 4 * 3 * kSepTmaLine * 8;  // the four boxes
+static_assert(kSepTmaBlock >= 3 * kSepTmaLine && (kSepTmaBlock * 8) % 128 == 0, "TMA plane blocks");
+
+struct SepMaps
+{
+    CUtensorMap m[8];  // the eight colour bricks of p (box 36 x 3 x 1)
+};
+
+// Shared slot of staged point (hx, hy) of the 66 x 6 plane: natural x = x0 + hx - 1, y = y0 + hy - 1.
+template <bool kTma>
+__host__ __device__ constexpr int sep_slot(int hx, int hy)
+{
+    if constexpr(!kTma) return plane_slot(hx, hy);
+    const int px = (hx + 1) & 1, py = (hy + 1) & 1;
+    return (py * 2 + px) * kSepTmaBlock + (hy >> 1) * kSepTmaLine + (hx >> 1) + px;
+}
+
+// The ring's mbarriers, initialised once per kernel before the first tile.
+__device__ __forceinline__ void sep_tma_init(uint64_t* bars)
+{
+    if(threadIdx.x == 0)
+        for(int i = 0; i < kSepRing; ++i) tma::mbar_init(&bars[i], 1);
+    __syncthreads();
+}
+
 // One tile (64 x 4 columns, kSZ planes) of the separable product; returns the
 // thread's running p.Ap sum.  Called by k64_spmv_sep (one tile per block) and
 // by the persistent CG step (a loop over tiles); the staging buffers are
-// reused from one tile to the next.
-template <bool kPap>
+// reused from one tile to the next.  kTma: planes staged by TMA boxes (maps,
+// bars, and the ring slots' phase bits in *phase, carried across tiles; bit
+// 31 records a wait that timed out).
+template <bool kPap, bool kTma = false>
 __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* __restrict__ diag,
                                            const double* __restrict__ p, double* __restrict__ Ap, int bx, int by,
-                                           int bz, double s)
+                                           int bz, double s, const SepMaps* maps = nullptr,
+                                           uint64_t* bars = nullptr, unsigned* phase = nullptr)
 {
-    __shared__ __align__(16) double xs[kSepRing][kPlane];  // staged planes with their one-point halo (66 x 6)
+    constexpr int kSlots = kTma ? kSepTmaPlane : kPlane;
+    __shared__ __align__(128) double xs[kSepRing][kSlots];  // staged planes with their one-point halo (66 x 6)
     __shared__ double sxs[kSPts];                           // x sums of the 64 x 6 points
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = bx * kMX, y0 = by * kMY, zb = bz * kSZ;  // zb even
     const int ze = zb + kSZ < L.nz ? zb + kSZ : L.nz;
 
-    // staged positions, as in the march
+    // staged positions, as in the march (eight-byte copies)
     int slot[kMLoads];
     bool inxy[kMLoads];
     CanonColumn col[kMLoads];
-#pragma unroll
-    for(int k = 0; k < kMLoads; ++k)
+    if constexpr(!kTma)
     {
-        const int e = tid + k * kMThreads;
-        const int hx = e % kPX, hy = e / kPX;
-        const int x = x0 + hx - 1, y = y0 + hy - 1;
-        slot[k] = e < kPlane ? plane_slot(hx, hy) : -1;
-        inxy[k] = e < kPlane && x >= 0 && x < L.nx && y >= 0 && y < L.ny;
-        col[k] = canon_column(L, inxy[k] ? x : 0, inxy[k] ? y : 0);
+#pragma unroll
+        for(int k = 0; k < kMLoads; ++k)
+        {
+            const int e = tid + k * kMThreads;
+            const int hx = e % kPX, hy = e / kPX;
+            const int x = x0 + hx - 1, y = y0 + hy - 1;
+            slot[k] = e < kPlane ? plane_slot(hx, hy) : -1;
+            inxy[k] = e < kPlane && x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+            col[k] = canon_column(L, inxy[k] ? x : 0, inxy[k] ? y : 0);
+        }
     }
     // x-sum positions: a warp takes one halo row and one x parity
     int sdst[kSPer], sm[kSPer], s0[kSPer], sp[kSPer];
@@ -1668,16 +1708,16 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
         const int e = tid + k * kMThreads;
         const int hy = e >> 6, lx = 2 * (e & 31) + ((e >> 5) & 1);
         sdst[k] = e < kSPts ? sx_slot(lx, hy) : -1;
-        sm[k] = plane_slot(lx, hy);
-        s0[k] = plane_slot(lx + 1, hy);
-        sp[k] = plane_slot(lx + 2, hy);
+        sm[k] = sep_slot<kTma>(lx, hy);
+        s0[k] = sep_slot<kTma>(lx + 1, hy);
+        sp[k] = sep_slot<kTma>(lx + 2, hy);
     }
     // own output column: warp -> (x parity, row), lane -> x
     const int px = warp & 1, ly = warp >> 1;
     const int lx = 2 * lane + px;
     const int x = x0 + lx, y = y0 + ly;
     const bool mine = x < L.nx && y < L.ny;
-    const int c = plane_slot(lx + 1, ly + 1);
+    const int c = sep_slot<kTma>(lx + 1, ly + 1);
     const int cm = sx_slot(lx, ly), c0 = sx_slot(lx, ly + 1), cp = sx_slot(lx, ly + 2);
     const CanonColumn own = canon_column(L, mine ? x : 0, mine ? y : 0);
 
@@ -1685,14 +1725,53 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
     auto issue = [&](int z, auto zq) {
         constexpr int q = decltype(zq)::value;  // z & 1
         double* dst = xs[(z + kSepRing) & (kSepRing - 1)];
-        const bool zin = z >= 0 && z < L.nz;
-#pragma unroll
-        for(int k = 0; k < kMLoads; ++k)
-            if(slot[k] >= 0)
+        if constexpr(kTma)
+        {
+            if(tid == 0)
             {
-                const bool v = inxy[k] && zin;
-                cp_async8(dst + slot[k], v ? p + canon_row<q>(col[k], z) : p, v);
+                uint64_t* bar = &bars[(z + kSepRing) & (kSepRing - 1)];
+                // p may have been written by other blocks of this kernel (the
+                // CG step's p update): order this thread's view of those
+                // generic-proxy writes before its async-proxy reads
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                tma::mbar_arrive_expect_tx(bar, kSepTmaBytes);
+#pragma unroll
+                for(int py = 0; py < 2; ++py)
+#pragma unroll
+                    for(int pxx = 0; pxx < 2; ++pxx)
+                    {
+                        const int v = (int)((0x01456327u >> (4 * ((pxx << 2) | (py << 1) | q))) & 15u);
+                        tma::load_3d(dst + (py * 2 + pxx) * kSepTmaBlock, &maps->m[v], x0 / 2 - 2 * pxx,
+                                     y0 / 2 - py, z >> 1, bar);
+                    }
             }
+        }
+        else
+        {
+            const bool zin = z >= 0 && z < L.nz;
+#pragma unroll
+            for(int k = 0; k < kMLoads; ++k)
+                if(slot[k] >= 0)
+                {
+                    const bool v = inxy[k] && zin;
+                    cp_async8(dst + slot[k], v ? p + canon_row<q>(col[k], z) : p, v);
+                }
+        }
+    };
+    // plane t is in its ring slot: this thread's copies (cp.async) or the
+    // slot's mbarrier phase (TMA)
+    auto landed = [&](int t) {
+        if constexpr(kTma)
+        {
+            const int sl = (t + kSepRing) & (kSepRing - 1);
+            const unsigned ph = (*phase >> sl) & 1u;
+            if(!tma::mbar_wait(&bars[sl], ph)) *phase |= 1u << 31;
+            *phase ^= 1u << sl;
+        }
+        else
+        {
+            cp_async_wait<kSepAhead>();
+        }
     };
     using Q0 = std::integral_constant<int, 0>;
     using Q1 = std::integral_constant<int, 1>;
@@ -1701,23 +1780,23 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
     double xo0 = 0.0, xo1 = 0.0;          // own x of planes t-1, t
     double dn = 0.0;                       // a_ii of the row plane finished at the next step
     issue(zb - 1, Q1{});
-    cp_async_commit();
+    if constexpr(!kTma) cp_async_commit();
     issue(zb, Q0{});
-    cp_async_commit();
+    if constexpr(!kTma) cp_async_commit();
     issue(zb + 1, Q1{});
-    cp_async_commit();
+    if constexpr(!kTma) cp_async_commit();
     // step t: plane t+3 goes out, plane t is summed, row plane t-1 (of
     // parity q = (t+1)&1 = (t+3)&1) is finished
     auto step = [&](int t, auto zq) {
         constexpr int q = decltype(zq)::value;
         if(t + kSepAhead <= ze) issue(t + kSepAhead, zq);  // its slot held plane t-1, read last step
-        cp_async_commit();
+        if constexpr(!kTma) cp_async_commit();
         const int zo = t - 1;
         const bool out = mine && zo >= zb;
         const double d = dn;
         dn = (mine && t >= zb && t < ze) ? diag[canon_row<q ^ 1>(own, t)] : 0.0;
-        cp_async_wait<kSepAhead>();  // this thread's copies of plane t have landed
-        __syncthreads();             // everyone's have
+        landed(t);
+        __syncthreads();             // everyone's copies of plane t have landed
         const double* xp = xs[(t + kSepRing) & (kSepRing - 1)];
 #pragma unroll
         for(int k = 0; k < kSPer; ++k)
@@ -1742,18 +1821,23 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
         step(t, Q0{});
         if(t + 1 <= ze) step(t + 1, Q1{});
     }
-    cp_async_wait<0>();
+    if constexpr(!kTma) cp_async_wait<0>();
     return s;
 }
 
-template <bool kPap>
+template <bool kPap, bool kTma>
 __global__ void __launch_bounds__(kMThreads) k64_spmv_sep(const StencilLevel L, const double* __restrict__ diag,
                                                           const double* __restrict__ p, double* __restrict__ Ap,
-                                                          CGState* st, double* partial, unsigned int* ticket)
+                                                          CGState* st, double* partial, unsigned int* ticket,
+                                                          const __grid_constant__ SepMaps maps)
 {
     __shared__ double red[32];
     __shared__ bool last;
-    double s = sep_tile<kPap>(L, diag, p, Ap, blockIdx.x, blockIdx.y, blockIdx.z, 0.0);
+    __shared__ uint64_t bars[kSepRing];
+    unsigned phase = 0;
+    if constexpr(kTma) sep_tma_init(bars);
+    double s = sep_tile<kPap, kTma>(L, diag, p, Ap, blockIdx.x, blockIdx.y, blockIdx.z, 0.0, &maps, bars, &phase);
+    if(kTma && (phase >> 31) && st && threadIdx.x == 0) atomicExch(&st->status, 3);
     if(!kPap) return;
     const int tid = threadIdx.x;
     s = block_sum(s, red);
@@ -1781,14 +1865,20 @@ __global__ void __launch_bounds__(kMThreads) k64_spmv_sep(const StencilLevel L, 
 
 // Step 1 of the two-kernel CG step with the separable product (canonical
 // colouring): r.z, beta, p update (the rows of n), then the tiles of the
-// product in a loop, p.Ap and alpha.  Persistent and cooperative.
-template <typename Z>
+// product in a loop, p.Ap and alpha.  Persistent and cooperative.  kTma: the
+// product's planes staged by TMA (the p update's stores are fenced for the
+// async proxy before the grid barrier that precedes them).
+template <typename Z, bool kTma>
 __global__ void __launch_bounds__(kMThreads) k_cg_step1_sep(const StencilLevel L, const double* __restrict__ diag,
                                                             const double* __restrict__ r, const Z* __restrict__ z,
                                                             double* __restrict__ p, double* __restrict__ x,
                                                             double* __restrict__ Ap, CGState* st, double* partial,
-                                                            unsigned int* ticket, GridBarrier* gb)
+                                                            unsigned int* ticket, GridBarrier* gb,
+                                                            const __grid_constant__ SepMaps maps)
 {
+    __shared__ uint64_t bars[kSepRing];
+    unsigned phase = 0;
+    if constexpr(kTma) sep_tma_init(bars);
     if(!step1_rz_p(L.m, r, z, p, x, st, partial, gb)) return;
     const int tx = (L.nx + kMX - 1) / kMX, ty = (L.ny + kMY - 1) / kMY, tz = (L.nz + kSZ - 1) / kSZ;
     const int ntiles = tx * ty * tz;
@@ -1797,8 +1887,9 @@ __global__ void __launch_bounds__(kMThreads) k_cg_step1_sep(const StencilLevel L
     {
         const int bz = tile / (tx * ty), rem = tile - bz * tx * ty;
         const int by = rem / tx, bx = rem - by * tx;
-        s = sep_tile<true>(L, diag, p, Ap, bx, by, bz, s);
+        s = sep_tile<true, kTma>(L, diag, p, Ap, bx, by, bz, s, &maps, bars, &phase);
     }
+    if(kTma && (phase >> 31) && threadIdx.x == 0) atomicExch(&st->status, 3);
     step1_alpha(s, st, partial, ticket);
 }
 
@@ -2321,10 +2412,49 @@ int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const doubl
     return 0;
 }
 
+// TMA maps of the eight colour bricks of one FP64 vector (box 36 x 3 x 1), for
+// the separable product's plane staging; built once per vector and kept.
+static const SepMaps* sep_maps(const StencilLevel& L, const double* v)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const double*, int>, std::unique_ptr<SepMaps>>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    for(const auto& e : cache)
+        if(e.first.first == v && e.first.second == L.m) return e.second.get();
+    auto M = std::make_unique<SepMaps>();
+    for(int u = 0; u < 8; ++u)
+    {
+        const int bz = (L.nz - (L.par[u] & 1) + 1) / 2;
+        if(encode_brick_map(&M->m[u], v + L.offsets[u], 8, L.bx[u], L.by[u], bz, kSepTmaLine, 3, 1)) return nullptr;
+    }
+    if(cache.size() >= 16) cache.erase(cache.begin());
+    cache.emplace_back(std::make_pair(v, L.m), std::move(M));
+    return cache.back().second.get();
+}
+
+// The separable product stages its planes by TMA on even grids with 4-aligned
+// colour bricks (HPCGB200_SEP_TMA=0: eight-byte asynchronous copies).
+static const SepMaps* sep_tma_maps(const StencilLevel& L, const double* v)
+{
+    static const bool on = [] {
+        const char* e = getenv("HPCGB200_SEP_TMA");
+        return !(e && e[0] == '0');
+    }();
+    if(!on || !vec4_ok(L) || (reinterpret_cast<uintptr_t>(v) & 15u)) return nullptr;
+    return sep_maps(L, v);
+}
+
 int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x, double* y, cudaStream_t s)
 {
     if(canonical_colours(L))
-        k64_spmv_sep<false><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
+    {
+        const SepMaps* M = sep_tma_maps(L, x);
+        if(M)
+            k64_spmv_sep<false, true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr, *M);
+        else
+            k64_spmv_sep<false, false><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr,
+                                                                          SepMaps{});
+    }
     else
         k64_spmv_tile<false><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr);
     HB_LAUNCHED();
@@ -2335,10 +2465,21 @@ int launch_cg_step1_sep(const StencilLevel& L, const double* diag, const double*
                         double* x, double* Ap, CGState* st, ReduceScratch* ws, GridBarrier* gb, cudaStream_t s)
 {
     if(!canonical_colours(L)) return record_error(HPCGB200_ERR_ARG, "CG step: the level is not canonically coloured");
-    static const int grid = resident_grid(k_cg_step1_sep<float>, kMThreads, kReduceBlocks);
+    // each staging runs its own resident grid (the TMA form holds fewer
+    // registers: 5 blocks per SM instead of 4); the r.z and p.Ap partitions
+    // follow the grid, so the two forms' CG scalars agree to rounding (with
+    // equal grids they agree bit for bit)
+    static const int grid_tma = resident_grid(k_cg_step1_sep<float, true>, kMThreads, kReduceBlocks);
+    static const int grid_cp = resident_grid(k_cg_step1_sep<float, false>, kMThreads, kReduceBlocks);
+    const SepMaps* M = sep_tma_maps(L, p);
+    const int grid = M ? grid_tma : grid_cp;
     if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "CG step: no resident grid");
-    HB_CUDA(launch_coop(k_cg_step1_sep<float>, grid, kMThreads, s, L, diag, r, z, p, x, Ap, st, ws->partial,
-                        &ws->ticket, gb));
+    if(M)
+        HB_CUDA(launch_coop(k_cg_step1_sep<float, true>, grid, kMThreads, s, L, diag, r, z, p, x, Ap, st, ws->partial,
+                            &ws->ticket, gb, *M));
+    else
+        HB_CUDA(launch_coop(k_cg_step1_sep<float, false>, grid, kMThreads, s, L, diag, r, z, p, x, Ap, st,
+                            ws->partial, &ws->ticket, gb, SepMaps{}));
     return 0;
 }
 
@@ -2346,7 +2487,13 @@ int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, cons
                                  CGState* st, double* partial, unsigned int* ticket, cudaStream_t s)
 {
     if(canonical_colours(L))
-        k64_spmv_sep<true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
+    {
+        const SepMaps* M = sep_tma_maps(L, p);
+        if(M) k64_spmv_sep<true, true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket, *M);
+        else
+            k64_spmv_sep<true, false><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket,
+                                                                         SepMaps{});
+    }
     else
         k64_spmv_tile<true><<<tile64_blocks(L), kT64Threads, 0, s>>>(L, diag, p, Ap, st, partial, ticket);
     HB_LAUNCHED();
