@@ -1668,8 +1668,8 @@ __device__ __forceinline__ void sep_tma_init(uint64_t* bars)
 // thread's running p.Ap sum.  Called by k64_spmv_sep (one tile per block) and
 // by the persistent CG step (a loop over tiles); the staging buffers are
 // reused from one tile to the next.  kTma: planes staged by TMA boxes (maps,
-// bars, and the ring slots' phase bits in *phase, carried across tiles; bit
-// 31 records a wait that timed out).
+// bars, and the ring slots' phase bits in *phase, carried across tiles with
+// the x-sum buffer toggle in bit 30; bit 31 records a wait that timed out).
 template <bool kPap, bool kTma = false>
 __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* __restrict__ diag,
                                            const double* __restrict__ p, double* __restrict__ Ap, int bx, int by,
@@ -1678,7 +1678,7 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
 {
     constexpr int kSlots = kTma ? kSepTmaPlane : kPlane;
     __shared__ __align__(128) double xs[kSepRing][kSlots];  // staged planes with their one-point halo (66 x 6)
-    __shared__ double sxs[kSPts];                           // x sums of the 64 x 6 points
+    __shared__ double sxs[kTma ? 2 : 1][kSPts];             // x sums of the 64 x 6 points
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = bx * kMX, y0 = by * kMY, zb = bz * kSZ;  // zb even
     const int ze = zb + kSZ < L.nz ? zb + kSZ : L.nz;
@@ -1796,16 +1796,24 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
         const double d = dn;
         dn = (mine && t >= zb && t < ze) ? diag[canon_row<q ^ 1>(own, t)] : 0.0;
         landed(t);
-        __syncthreads();             // everyone's copies of plane t have landed
+        // cp.async: everyone's copies of plane t have landed, and the x sums
+        // of the last step are read.  TMA: every thread has waited on the
+        // plane's mbarrier itself, and the x sums alternate between two
+        // buffers (bit 30 of *phase), so one barrier per plane suffices: the
+        // buffer written here was last read two steps ago, before the barrier
+        // of the last step.
+        if constexpr(!kTma) __syncthreads();
+        double* sx = sxs[kTma ? ((*phase >> 30) & 1u) : 0];
         const double* xp = xs[(t + kSepRing) & (kSepRing - 1)];
 #pragma unroll
         for(int k = 0; k < kSPer; ++k)
-            if(sdst[k] >= 0) sxs[sdst[k]] = (xp[sm[k]] + xp[s0[k]]) + xp[sp[k]];
+            if(sdst[k] >= 0) sx[sdst[k]] = (xp[sm[k]] + xp[s0[k]]) + xp[sp[k]];
         const double xn = xp[c];
         __syncthreads();  // x sums of plane t stored; plane t no longer read
+        if constexpr(kTma) *phase ^= 1u << 30;
         r0 = r1;
         r1 = r2;
-        r2 = (sxs[cm] + sxs[c0]) + sxs[cp];
+        r2 = (sx[cm] + sx[c0]) + sx[cp];
         xo0 = xo1;
         xo1 = xn;
         if(out)
