@@ -2421,14 +2421,24 @@ int launch64_spmv_stencil(const StencilLevel& L, const double* diag, const doubl
 }
 
 // TMA maps of the eight colour bricks of one FP64 vector (box 36 x 3 x 1), for
-// the separable product's plane staging; built once per vector and kept.
+// the separable product's plane staging; built once per (vector, grid) and
+// kept.  The key holds the grid's dimensions, not only its size: a freed
+// vector's address can come back for a grid of the same size and another
+// shape, whose bricks the old maps would mis-describe.
+struct SepMapsEntry
+{
+    const double* v;
+    int nx, ny, nz;
+    std::unique_ptr<SepMaps> maps;
+};
+
 static const SepMaps* sep_maps(const StencilLevel& L, const double* v)
 {
     static std::mutex mu;
-    static std::vector<std::pair<std::pair<const double*, int>, std::unique_ptr<SepMaps>>> cache;
+    static std::vector<SepMapsEntry> cache;
     std::lock_guard<std::mutex> lock(mu);
     for(const auto& e : cache)
-        if(e.first.first == v && e.first.second == L.m) return e.second.get();
+        if(e.v == v && e.nx == L.nx && e.ny == L.ny && e.nz == L.nz) return e.maps.get();
     auto M = std::make_unique<SepMaps>();
     for(int u = 0; u < 8; ++u)
     {
@@ -2436,8 +2446,8 @@ static const SepMaps* sep_maps(const StencilLevel& L, const double* v)
         if(encode_brick_map(&M->m[u], v + L.offsets[u], 8, L.bx[u], L.by[u], bz, kSepTmaLine, 3, 1)) return nullptr;
     }
     if(cache.size() >= 16) cache.erase(cache.begin());
-    cache.emplace_back(std::make_pair(v, L.m), std::move(M));
-    return cache.back().second.get();
+    cache.push_back(SepMapsEntry{v, L.nx, L.ny, L.nz, std::move(M)});
+    return cache.back().maps.get();
 }
 
 // The separable product stages its planes by TMA on even grids with 4-aligned
