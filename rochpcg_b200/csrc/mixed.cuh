@@ -45,7 +45,7 @@ struct StencilLevel
     int color_of_par[8];
     int canon;                 // slot tables equal the compile-time ones of the canonical colouring
     StencilTab tab[kMaxStencilColors];
-    int* status = nullptr;     // device word the staged sweeps set when their copies time out (may be null)
+    int* status = nullptr;     // device word the TMA-staged passes set (3) when their copies time out (may be null)
 };
 
 // Builds the level description from the grid and the colour of each parity

@@ -418,8 +418,20 @@ int run_cg(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, int 
             for(int k = restart_offset + h.niters + 1; k <= max_iter; ++k) hist[k] = 0.0;
         }
         if(h.status)
-            return hb::record_error(HPCGB200_ERR_DEVICE_STATUS, "CG: a grid barrier of the CG step timed out (%d)",
+            return hb::record_error(HPCGB200_ERR_DEVICE_STATUS,
+                                    "CG: a bounded device wait of the CG step timed out (status %d: 1 grid barrier, "
+                                    "3 TMA copies)",
                                     h.status);
+        for(const SparseMatrix* M = &A; M; M = M->Ac)
+        {
+            const LevelOpt* lo = opt(*M);
+            if(!lo || !lo->pass_status) continue;
+            int ps = 0;
+            HB_HOST_CUDA(cudaMemcpy(&ps, lo->pass_status, sizeof(int), cudaMemcpyDeviceToHost));
+            if(ps)
+                return hb::record_error(HPCGB200_ERR_DEVICE_STATUS,
+                                        "CG: the copies of a TMA-staged colour pass timed out (status %d)", ps);
+        }
         o->last_fallback_iter = restart_offset > 0 ? restart_offset : h.fallback_iter;
         if(prec == MGPrecision::LEARNED) check(smoother_status(*o->smoother, s));
         niters = restart_offset + h.niters;

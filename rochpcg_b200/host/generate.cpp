@@ -210,6 +210,7 @@ static void delete_level_opt(SparseMatrix& A)
     dfree(o->colors);
     dfree(o->diag32);
     dfree(o->inv_diag32);
+    dfree(o->pass_status);
     dfree(o->cg_state);
     dfree(o->step_barrier);
     dfree(o->r32);

@@ -137,6 +137,7 @@ struct LevelOpt
     hb::StencilLevel st{};
     float* diag32 = nullptr;
     float* inv_diag32 = nullptr;
+    int* pass_status = nullptr;        // set (3) by a TMA-staged colour pass whose copies timed out (device word)
 
     // level-0 solver state
     hb::CGState* cg_state = nullptr;

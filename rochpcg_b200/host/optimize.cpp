@@ -93,6 +93,10 @@ static void optimize_level(SparseMatrix& A)
     if(o->stencil_ok)
     {
         o->pm = hb::make_perm_map(o->st);
+        // the TMA-staged colour passes of this level set it when their copies time out
+        o->pass_status = dalloc<int>(1);
+        HB_HOST_CUDA(cudaMemsetAsync(o->pass_status, 0, sizeof(int), s));
+        o->st.status = o->pass_status;
         o->diag32 = dalloc<float>(m);
         o->inv_diag32 = dalloc<float>(m);
         check(hb::launch_diag32(m, o->diag, o->diag32, o->inv_diag32, s));
