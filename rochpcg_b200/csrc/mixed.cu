@@ -2063,16 +2063,16 @@ static int encode_brick_map(CUtensorMap* map, const void* base, int esize, int b
 // Maps of x on level L, built once per (vector, level) and kept (a V-cycle
 // sweeps the same few vectors).
 template <typename T>
-static const SweepMaps* sweep_maps(const StencilLevel& L, const T* x)
+static std::shared_ptr<const SweepMaps> sweep_maps(const StencilLevel& L, const T* x)
 {
     static std::mutex mu;
-    static std::vector<std::unique_ptr<SweepMaps>> cache;
+    static std::vector<std::shared_ptr<SweepMaps>> cache;
     std::lock_guard<std::mutex> lock(mu);
     const int es = (int)sizeof(T);
     for(const auto& e : cache)
         if(e->x == x && e->esize == es && e->m == L.m && e->nx == L.nx && e->ny == L.ny && e->nz == L.nz)
-            return e.get();
-    auto e = std::make_unique<SweepMaps>();
+            return e;
+    auto e = std::make_shared<SweepMaps>();
     e->x = x;
     e->esize = es;
     e->m = L.m;
@@ -2089,7 +2089,7 @@ static const SweepMaps* sweep_maps(const StencilLevel& L, const T* x)
     }
     if(cache.size() >= 64) cache.erase(cache.begin());
     cache.push_back(std::move(e));
-    return cache.back().get();
+    return cache.back();
 }
 
 // The TMA-staged colour passes serve large even levels with the canonical
@@ -2150,7 +2150,7 @@ int launch32_symgs_zero(const StencilLevel& L, const float* diag32, const float*
     const dim3 t(32, 8), t4(kV4X, kV4Y);
     const bool vec = vec4_ok(L);
     const bool tma = pass_tma_ok(L, x, pro);
-    const SweepMaps* maps = tma ? sweep_maps(L, x) : nullptr;
+    const std::shared_ptr<const SweepMaps> maps = tma ? sweep_maps(L, x) : nullptr;
     if(tma && !maps) return HPCGB200_ERR_CUDA;
     for(int v = 0; v < n; ++v)
     {
@@ -2213,7 +2213,7 @@ int launch32_symgs(const StencilLevel& L, const float* inv_diag32, const float* 
     const int n = L.ncolors;
     const bool vec = vec4_ok(L);
     const bool tma = pass_tma_ok(L, x, pro);
-    const SweepMaps* maps = tma ? sweep_maps(L, x) : nullptr;
+    const std::shared_ptr<const SweepMaps> maps = tma ? sweep_maps(L, x) : nullptr;
     if(tma && !maps) return HPCGB200_ERR_CUDA;
     auto sweep = [&](int v, double* z, Prolong<float> pv) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
@@ -2246,7 +2246,8 @@ int launch32_restrict(const StencilLevel& Lf, int nc, const int* inj_f, const in
                       const float* rf, const float* xf, float* rc, cudaStream_t s)
 {
     const ColorLaunch c = color_launch(Lf, Lf.color_of_par[0]);
-    const SweepMaps* maps = pass_tma_ok(Lf, xf, {}) && nc == c.bx * c.by * c.bz ? sweep_maps(Lf, xf) : nullptr;
+    const std::shared_ptr<const SweepMaps> maps =
+        pass_tma_ok(Lf, xf, {}) && nc == c.bx * c.by * c.bz ? sweep_maps(Lf, xf) : nullptr;
     if(maps)
     {
         HB_CUDA((pass_tma<float, kTmaRestrict>(Lf, c, *maps, nullptr, diag32, nullptr, const_cast<float*>(rf),
@@ -2292,7 +2293,7 @@ int launch64v_symgs_zero(const StencilLevel& L, const double* diag, const double
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
     const dim3 t4(kV4X, kV4Y);
-    const SweepMaps* maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
+    const std::shared_ptr<const SweepMaps> maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
     if(pass_tma_ok(L, x, pro) && !maps) return HPCGB200_ERR_CUDA;
     for(int v = 0; v < L.ncolors; ++v)
     {
@@ -2332,7 +2333,7 @@ int launch64v_symgs(const StencilLevel& L, const double* inv_diag, const double*
                     Prolong<double> pro)
 {
     if(!vec4_ok(L)) return record_error(HPCGB200_ERR_ARG, "FP64 stencil V-cycle: colour bricks not 4-aligned");
-    const SweepMaps* maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
+    const std::shared_ptr<const SweepMaps> maps = pass_tma_ok(L, x, pro) ? sweep_maps(L, x) : nullptr;
     if(pass_tma_ok(L, x, pro) && !maps) return HPCGB200_ERR_CUDA;
     auto sweep = [&](int v, Prolong<double> pv) -> int {
         if(L.offsets[v + 1] - L.offsets[v] <= 0) return 0;
@@ -2363,7 +2364,7 @@ int launch64v_restrict(const StencilLevel& Lf, int nc, const int* inj_c, const d
         return record_error(HPCGB200_ERR_ARG, "FP64 stencil restriction: colour bricks not 4-aligned");
     if(pass_tma_ok(Lf, xf, Prolong<double>{}))
     {
-        const SweepMaps* maps = sweep_maps(Lf, xf);
+        const std::shared_ptr<const SweepMaps> maps = sweep_maps(Lf, xf);
         if(!maps) return HPCGB200_ERR_CUDA;
         HB_CUDA((pass_tma<double, kTmaRestrict>(Lf, c, *maps, nullptr, diag, nullptr, const_cast<double*>(rf),
                                                  const_cast<double*>(xf), nullptr, s, inj_c, rc)));
@@ -2429,17 +2430,17 @@ struct SepMapsEntry
 {
     const double* v;
     int nx, ny, nz;
-    std::unique_ptr<SepMaps> maps;
+    std::shared_ptr<SepMaps> maps;
 };
 
-static const SepMaps* sep_maps(const StencilLevel& L, const double* v)
+static std::shared_ptr<const SepMaps> sep_maps(const StencilLevel& L, const double* v)
 {
     static std::mutex mu;
     static std::vector<SepMapsEntry> cache;
     std::lock_guard<std::mutex> lock(mu);
     for(const auto& e : cache)
-        if(e.v == v && e.nx == L.nx && e.ny == L.ny && e.nz == L.nz) return e.maps.get();
-    auto M = std::make_unique<SepMaps>();
+        if(e.v == v && e.nx == L.nx && e.ny == L.ny && e.nz == L.nz) return e.maps;
+    auto M = std::make_shared<SepMaps>();
     for(int u = 0; u < 8; ++u)
     {
         const int bz = (L.nz - (L.par[u] & 1) + 1) / 2;
@@ -2447,12 +2448,12 @@ static const SepMaps* sep_maps(const StencilLevel& L, const double* v)
     }
     if(cache.size() >= 16) cache.erase(cache.begin());
     cache.push_back(SepMapsEntry{v, L.nx, L.ny, L.nz, std::move(M)});
-    return cache.back().maps.get();
+    return cache.back().maps;
 }
 
 // The separable product stages its planes by TMA on even grids with 4-aligned
 // colour bricks (HPCGB200_SEP_TMA=0: eight-byte asynchronous copies).
-static const SepMaps* sep_tma_maps(const StencilLevel& L, const double* v)
+static std::shared_ptr<const SepMaps> sep_tma_maps(const StencilLevel& L, const double* v)
 {
     static const bool on = [] {
         const char* e = getenv("HPCGB200_SEP_TMA");
@@ -2466,7 +2467,7 @@ int launch64_spmv_sep(const StencilLevel& L, const double* diag, const double* x
 {
     if(canonical_colours(L))
     {
-        const SepMaps* M = sep_tma_maps(L, x);
+        const std::shared_ptr<const SepMaps> M = sep_tma_maps(L, x);
         if(M)
             k64_spmv_sep<false, true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, x, y, nullptr, nullptr, nullptr, *M);
         else
@@ -2489,7 +2490,7 @@ int launch_cg_step1_sep(const StencilLevel& L, const double* diag, const double*
     // equal grids they agree bit for bit)
     static const int grid_tma = resident_grid(k_cg_step1_sep<float, true>, kMThreads, kReduceBlocks);
     static const int grid_cp = resident_grid(k_cg_step1_sep<float, false>, kMThreads, kReduceBlocks);
-    const SepMaps* M = sep_tma_maps(L, p);
+    const std::shared_ptr<const SepMaps> M = sep_tma_maps(L, p);
     const int grid = M ? grid_tma : grid_cp;
     if(grid <= 0) return record_error(HPCGB200_ERR_CUDA, "CG step: no resident grid");
     if(M)
@@ -2506,7 +2507,7 @@ int launch64_cg_spmv_pap_stencil(const StencilLevel& L, const double* diag, cons
 {
     if(canonical_colours(L))
     {
-        const SepMaps* M = sep_tma_maps(L, p);
+        const std::shared_ptr<const SepMaps> M = sep_tma_maps(L, p);
         if(M) k64_spmv_sep<true, true><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket, *M);
         else
             k64_spmv_sep<true, false><<<sep_grid(L), kMThreads, 0, s>>>(L, diag, p, Ap, st, partial, ticket,
