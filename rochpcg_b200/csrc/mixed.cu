@@ -1765,7 +1765,9 @@ __device__ __forceinline__ double sep_tile(const StencilLevel& L, const double* 
         {
             const int sl = (t + kSepRing) & (kSepRing - 1);
             const unsigned ph = (*phase >> sl) & 1u;
-            if(!tma::mbar_wait(&bars[sl], ph)) *phase |= 1u << 31;
+            // after a time-out the remaining planes are not waited for (the
+            // solve is reported failed; each wait would run its full limit)
+            if(!(*phase >> 31) && !tma::mbar_wait(&bars[sl], ph)) *phase |= 1u << 31;
             *phase ^= 1u << sl;
         }
         else
