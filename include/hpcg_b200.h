@@ -53,6 +53,13 @@ extern "C" {
 const char* hpcgb200_last_error(void);
 /* Library version string. */
 const char* hpcgb200_version(void);
+/* Binds the library's runtime (stream, reduction scratch) to CUDA device
+ * `device` (< 0: the current device) -- the reference driver's --dev=
+ * (src/init.cpp:196-214 selects the HIP device for one rank).  Call it before
+ * any other entry point; once bound, a different device is refused
+ * (HPCGB200_ERR_ARG), the same one is a no-op.  HPCGB200_ERR_NO_DEVICE
+ * without a device, HPCGB200_ERR_ARG for an index out of range. */
+int hpcgb200_init(int device);
 /* Bytes of caller-provided scratch the reduction entry points need. */
 size_t hpcgb200_reduction_workspace_bytes(void);
 /* The first n values rand() returns after srand(seed) with glibc's

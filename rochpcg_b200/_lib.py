@@ -17,6 +17,7 @@ _cp = ctypes.c_char_p
 SIGNATURES = {
     "hpcgb200_last_error": (_cp, []),
     "hpcgb200_version": (_cp, []),
+    "hpcgb200_init": (_i, [_i]),
     "hpcgb200_reduction_workspace_bytes": (_sz, []),
     "hpcgb200_rand_sequence": (_i, [ctypes.c_uint, _i, _vp]),
     "hpcgb200_generate_problem": (_i, [_i, _i, _i, _ll, _ll, _ll, _ll, _ll, _ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

@@ -5,14 +5,21 @@ optimized CG set-up run, timed CG sets, TestNorms and the rating with
 convergence and optimisation overhead.  The report is a JSON document with the
 sections and field names of the reference's YAML report.
 
-    python -m rochpcg_b200.benchmark [nx ny nz rt] [--nx=N --ny=N --nz=N --rt=S --tol=T]
+    python -m rochpcg_b200.benchmark [nx ny nz rt] [--nx=N --ny=N --nz=N --rt=S --tol=T --dev=D]
+                                     [--pz= --zl= --zu= --npx= --npy= --npz=]
                                      [--mode=fp64|mixed|fp64_stencil] [--out=FILE]
 
 Arguments follow the reference driver (src/init.cpp:112-183): positional
 nx ny nz rt (values below 10 ignored), or --nx= ... --rt=; --tol=T skips the
-reference phases and uses T as the reference tolerance; a dimension below 16
-becomes the largest of the others, at least 16; rt = 0 (the default here) is
-the QuickPath: one timed CG set.
+reference phases and uses T as the reference tolerance; --dev=D runs on CUDA
+device D.  With no grid argument at all the grid (and, without --rt=, the
+run time) come from hpcg.dat in the working directory (src/ReadHpcgDat.cpp:
+two title lines, then nx ny nz, then the seconds, then npx npy npz).  A
+dimension below 16 becomes the largest of the others, at least 16; rt = 0
+(the default without hpcg.dat) is the QuickPath: one timed CG set.  The
+process-grid flags (--pz= --zl= --zu= --npx= --npy= --npz=) are read as the
+reference reads them; this driver runs one rank, so a grid of more than one
+rank is refused (the decomposed solve is rochpcg_b200.dist).
 """
 from __future__ import annotations
 
@@ -89,30 +96,82 @@ def run(nx: int, ny: int | None = None, nz: int | None = None, running_time: int
     return r.as_dict(), report(r, L)
 
 
-def parse_args(argv: list[str]) -> dict:
-    """src/init.cpp:112-183 for one rank, plus --mode= and --out=."""
-    ip = [0, 0, 0, 0]
-    for i in range(4):
-        try:
-            v = int(argv[i])
-            ip[i] = v if v >= 10 else 0
-        except (IndexError, ValueError):
-            ip[i] = 0
+_PREFIXES = ("--nx=", "--ny=", "--nz=", "--rt=", "--pz=", "--zl=", "--zu=", "--npx=", "--npy=", "--npz=", "--dev=")
+
+
+def _leading_int(text: str):
+    """The integer sscanf("%d") reads at the start of `text`, or None."""
+    text = text.lstrip()
+    n = 0
+    if n < len(text) and text[n] in "+-":
+        n += 1
+    while n < len(text) and text[n].isdigit():
+        n += 1
+    try:
+        return int(text[:n])
+    except ValueError:
+        return None
+
+
+def read_hpcg_dat(path: str = "hpcg.dat"):
+    """src/ReadHpcgDat.cpp:42-75: ([nx, ny, nz], seconds, [npx, npy, npz]) from
+    the file, or None when it cannot be opened.  Two title lines are skipped; a
+    dimension that is missing or below 16 becomes 16, a missing or negative time
+    30 minutes, a missing or non-positive process dimension 0 (unspecified)."""
+    try:
+        with open(path) as f:
+            lines = f.read().split("\n")
+    except OSError:
+        return None
+    body = lines[2:] + ["", "", ""]
+    dims_tok = body[0].split()
+    dims = []
+    for i in range(3):
+        v = _leading_int(dims_tok[i]) if i < len(dims_tok) else None
+        dims.append(v if v is not None and v >= 16 else 16)
+    t = _leading_int(body[1].split()[0]) if body[1].split() else None
+    seconds = t if t is not None and t >= 0 else 30 * 60
+    proc_tok = body[2].split()
+    procs = []
+    for i in range(3):
+        v = _leading_int(proc_tok[i]) if i < len(proc_tok) else None
+        procs.append(v if v is not None and v >= 1 else 0)
+    return dims, seconds, procs
+
+
+def parse_args(argv: list[str], dat_path: str = "hpcg.dat") -> dict:
+    """src/init.cpp:112-183 for one rank (hpcg.dat when no grid argument is
+    given), plus --mode= and --out=."""
+    ip = [0] * len(_PREFIXES)
+    for i in range(len(_PREFIXES)):
+        v = _leading_int(argv[i]) if i < len(argv) else None
+        ip[i] = v if v is not None and v >= 10 else 0
     verify, tol, mode, out = True, 0.0, MODE_FP64, None
     for a in argv:
-        for j, k in enumerate(("--nx=", "--ny=", "--nz=", "--rt=")):
+        for j, k in enumerate(_PREFIXES):
             if a.startswith(k):
-                try:
-                    ip[j] = int(a[len(k):])
-                except ValueError:
-                    ip[j] = 0
+                v = _leading_int(a[len(k):])
+                ip[j] = v if v is not None else 0
         if a.startswith("--tol="):
             tol, verify = float(a[6:]), False
         elif a.startswith("--mode="):
             mode = {"fp64": MODE_FP64, "mixed": MODE_MIXED, "fp64_stencil": MODE_FP64_STENCIL}[a[7:]]
         elif a.startswith("--out="):
             out = a[6:]
-    return dict(nx=ip[0], ny=ip[1], nz=ip[2], running_time=ip[3], verify=verify, tol=tol, mode=mode, out=out)
+    if not ip[0] and not ip[1] and not ip[2]:
+        dat = read_hpcg_dat(dat_path)
+        if dat is not None:
+            ip[0:3] = dat[0]
+            if not ip[3]:
+                ip[3] = dat[1]
+            ip[7:10] = dat[2]
+    # (the library applies the small-dimension rule, src/init.cpp:150-160)
+    npx, npy, npz = ip[7:10]
+    if max(npx, 1) * max(npy, 1) * max(npz, 1) > 1:
+        raise ValueError(f"process grid {npx}x{npy}x{npz}: this driver runs one rank (the decomposed solve is "
+                         "rochpcg_b200.dist)")
+    return dict(nx=ip[0], ny=ip[1], nz=ip[2], running_time=ip[3], verify=verify, tol=tol, mode=mode, out=out,
+                device=ip[10] if any(a.startswith("--dev=") for a in argv) else -1)
 
 
 def main(argv=None):
@@ -121,6 +180,8 @@ def main(argv=None):
     os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
     a = parse_args(sys.argv[1:] if argv is None else argv)
     out = a.pop("out")
+    L = load()
+    check(L, L.hpcgb200_init(a.pop("device")))
     res, rep = run(**a)
     text = json.dumps(rep, indent=1)
     if out is None:

@@ -67,6 +67,31 @@ int HPCG_B200_Init(int device)
     }
 }
 
+extern "C" int hpcgb200_init(int device)
+{
+    try
+    {
+        if(g_rt.initialized)
+        {
+            if(device >= 0 && device != g_rt.device)
+                return hb::record_error(HPCGB200_ERR_ARG, "the library runtime is bound to device %d already",
+                                        g_rt.device);
+            return 0;
+        }
+        int n = 0;
+        if(cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+            return hb::record_error(HPCGB200_ERR_NO_DEVICE, "no CUDA device visible");
+        if(device >= n) return hb::record_error(HPCGB200_ERR_ARG, "device %d out of range (%d visible)", device, n);
+        if(device >= 0) HB_HOST_CUDA(cudaSetDevice(device));
+        ensure_runtime();
+        return 0;
+    }
+    catch(const Error& e)
+    {
+        return report(e);
+    }
+}
+
 cudaStream_t HPCG_B200_Stream()
 {
     ensure_runtime();

@@ -4,6 +4,7 @@ JSON layout) against the restatement of src/ReportResults.cpp in
 oracle/report.py, and the driver's argument rules (src/init.cpp)."""
 import ctypes
 import math
+import os
 
 import numpy as np
 import pytest
@@ -138,3 +139,56 @@ def test_driver_arguments(argv, want):
                                        ((8, 24, 4), (24, 24, 24)), ((104, 16, 200), (104, 16, 200))])
 def test_small_dimension_rule(dims, want):
     assert OR.adjust_dims(*dims) == want
+
+
+def _dat(tmp_path, text):
+    p = tmp_path / "hpcg.dat"
+    p.write_text(text)
+    return str(p)
+
+
+def test_hpcg_dat_fallback(tmp_path):
+    """src/init.cpp:143-147 + src/ReadHpcgDat.cpp: with no grid argument the
+    grid and the seconds come from hpcg.dat; a nonzero --rt= wins over the
+    file's time (--rt=0 counts as not given, as in the reference); a grid
+    argument skips the file."""
+    dat = _dat(tmp_path, "HPCG benchmark input file\nsecond title line\n104 104 96\n60\n")
+    a = B.parse_args([], dat_path=dat)
+    assert (a["nx"], a["ny"], a["nz"], a["running_time"]) == (104, 104, 96, 60)
+    a = B.parse_args(["--rt=5", "--mode=mixed"], dat_path=dat)
+    assert (a["nx"], a["running_time"], a["mode"]) == (104, 5, MODE_MIXED)
+    assert B.parse_args(["--rt=0"], dat_path=dat)["running_time"] == 60
+    a = B.parse_args(["--nx=32"], dat_path=dat)
+    assert (a["nx"], a["ny"], a["running_time"]) == (32, 0, 0)
+    # missing file: nothing read
+    a = B.parse_args([], dat_path=str(tmp_path / "absent.dat"))
+    assert (a["nx"], a["ny"], a["nz"], a["running_time"]) == (0, 0, 0, 0)
+
+
+def test_hpcg_dat_defaults():
+    """Values below 16 (or absent) become 16, a missing or negative time 30
+    minutes, missing process dimensions 0."""
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "hpcg.dat")
+        with open(p, "w") as f:
+            f.write("t\nt\n8 200\n-5\n2 x\n")
+        dims, seconds, procs = B.read_hpcg_dat(p)
+        assert dims == [16, 200, 16] and seconds == 1800 and procs == [2, 0, 0]
+        with open(p, "w") as f:
+            f.write("only one line\n")
+        assert B.read_hpcg_dat(p) == ([16, 16, 16], 1800, [0, 0, 0])
+
+
+def test_device_and_process_grid_flags(tmp_path):
+    absent = str(tmp_path / "none.dat")
+    assert B.parse_args(["--nx=64", "--dev=3"], dat_path=absent)["device"] == 3
+    assert B.parse_args(["--nx=64"], dat_path=absent)["device"] == -1
+    # one rank: a process grid of one is accepted, a larger one refused
+    assert B.parse_args(["--nx=64", "--npx=1", "--npy=1", "--npz=1"], dat_path=absent)["nx"] == 64
+    with pytest.raises(ValueError):
+        B.parse_args(["--nx=64", "--npx=2"], dat_path=absent)
+    dat = _dat(tmp_path, "t\nt\n64 64 64\n0\n2 2 1\n")
+    with pytest.raises(ValueError):
+        B.parse_args([], dat_path=dat)

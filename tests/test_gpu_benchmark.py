@@ -161,3 +161,21 @@ def test_protocol_mixed_mode():
     assert res["tolerance_failures"] == 0 and res["opt_setup_niters"] <= 53
     assert res["valid"] == 1
     assert "Mixed precision" in rep["Final Summary"]
+
+
+def test_driver_command_line_with_device_and_hpcg_dat(tmp_path, monkeypatch):
+    """The driver as a user runs it: --dev=0 binds the runtime to device 0
+    (hpcgb200_init, src/init.cpp's --dev=), the grid comes from hpcg.dat in the
+    working directory, the report is written where --out= says."""
+    (tmp_path / "hpcg.dat").write_text("HPCG benchmark input file\ntitle\n32 32 32\n0\n")
+    monkeypatch.chdir(tmp_path)
+    out = tmp_path / "report.json"
+    assert B.main(["--dev=0", f"--out={out}"]) == 0
+    import json
+
+    rep = json.loads(out.read_text())
+    assert "HPCG result is VALID with a GFLOP/s rating of" in rep["Final Summary"]
+    L = R.load()
+    assert L.hpcgb200_init(0) == 0                 # the device it is bound to: a no-op
+    assert L.hpcgb200_init(1 << 20) == 1           # another device: refused
+    assert b"bound to device" in L.hpcgb200_last_error()
