@@ -142,6 +142,22 @@ def test_protocol_quickpath_valid(n, bound):
         assert res["ref_tolerance"] == pytest.approx(float(g["cg50_normr"]) / float(g["cg50_normr0"]), rel=1e-6)
 
 
+# src/test_rochpcg.cpp:65-77 sweeps these cubic sizes through the whole
+# protocol (the larger 256, 280 and 288 are covered by the bench's 256^3 run
+# and tests/test_gpu_cg.py); each must reach the reference residual within its
+# check_niter bound with every V&V test passing.
+@pytest.mark.parametrize("n", [16, 48, 80, 96, 104, 112, 120, 128])
+def test_protocol_sweep_of_the_reference_test(n):
+    from niter_bounds import check_niter
+
+    res, _ = B.run(n, n, n, running_time=0, verify=True)
+    assert res["check_problem_errors"] == 0 and res["ref_niters"] == 50
+    assert res["tolerance_failures"] == 0 and res["err_count"] == 0
+    assert res["opt_setup_niters"] <= check_niter(1, (n, n, n)), res["opt_setup_niters"]
+    assert res["testcg_count_fail"] == 0 and res["symmetry_count_fail"] == 0 and res["norms_pass"] == 1
+    assert res["valid"] == 1
+
+
 def test_protocol_with_given_tolerance_and_timed_sets():
     res, rep = B.run(32, 32, 32, running_time=1, verify=False, tol=1e-6)
     assert res["ref_tolerance"] == 1e-6 and res["ref_niters"] == 0
