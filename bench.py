@@ -463,7 +463,8 @@ def run_ours(args):
     true_rel = P.true_residual()
     fp64_tag = refcheck("fp64_256", grid, ("generated",), P.get_x()) if checker else None
     kpi = P.kernels_per_iteration(R.MODE_FP64)
-    launches = args.steps * (iters * kpi + 2)
+    # per solve: the preamble's SpMV and residual, the iterations, the last x update
+    launches = args.steps * (iters * kpi + 3)
 
     if args.lite:
         if rank == 0:
