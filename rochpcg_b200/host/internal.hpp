@@ -137,7 +137,8 @@ struct LevelOpt
     hb::StencilLevel st{};
     float* diag32 = nullptr;
     float* inv_diag32 = nullptr;
-    int* pass_status = nullptr;        // set (3) by a TMA-staged colour pass whose copies timed out (device word)
+    int* pass_status = nullptr;        // set (3) by a TMA-staged colour pass whose copies timed out (device word;
+                                       // never cleared: every later solve on the problem reports it)
 
     // level-0 solver state
     hb::CGState* cg_state = nullptr;
